@@ -1,0 +1,286 @@
+"""Benchmark: bzip2 compression throughput on B200 (plain form).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--size BYTES] [--impl ours|reference]
+
+Workload: the large Markov stream (order-1 Markov bytes, alphabet and
+Dirichlet concentration redrawn every 64 MiB, 2 % run starts of length
+4..300, 900,000-byte blocks, seed 0xB2C4), generated on the device.  A step
+compresses the whole stream to a complete .bz2 stream.
+  value  MB/s of input, input resident in HBM (bz2g_compress_device), output
+         stream delivered to host memory.
+  e2e    MB/s through bz2g_compress with the input in pinned host memory:
+         host->device copy of every byte and device->host copy of the stream
+         are inside the timed region.
+Under torchrun each rank compresses its own stream (weak scaling, no
+collective on the data path); times are the max over ranks.
+--impl reference times the reference path's CPU implementation (the oracle
+port of the reference semantics; the reference itself has no CPU compressor)
+on a bounded sample of the same workload with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "MB/s compressed on 1 B200: plain vs batched+learned at equal ratio; %HBM peak"
+WORKLOAD = "large Markov stream, 900k blocks (order-1 Markov, alphabet/alpha redrawn every 64 MiB, 2% runs)"
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(s[1]) for s in self.samples if len(s) > 2 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) > 2 and s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for k, nm in enumerate(names):
+                if len(s) > 5 + k and s[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.samples)}
+
+
+def dist_setup(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_sample_time(host, nbytes: int, threads: int):
+    import oracle
+    t = time.perf_counter()
+    out = oracle.compress(host[:nbytes], 9, 900000, threads=threads)
+    return time.perf_counter() - t, len(out)
+
+
+def run_reference(args):
+    """The reference path on the host cores (oracle port), bounded sample."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import bzip2gpu_b200.workloads as W
+    threads = os.cpu_count() or 1
+    sample = min(args.size, args.cpu_sample)
+    host = W.large_stream(sample, device=False)
+    for _ in range(args.warmup):
+        cpu_sample_time(host, min(sample, 8 << 20), threads)
+    times = []
+    for _ in range(args.steps):
+        dt, _ = cpu_sample_time(host, sample, threads)
+        times.append(dt)
+    tot = sum(times)
+    mbps = sample * len(times) / tot / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(mbps, 2), "unit": "MB/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(tot / len(times) * 1e3, 2), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample_bytes": sample, "block_bytes": 900000,
+                   "level": 9},
+        "cpu_baseline": {"value": round(mbps, 2), "unit": "MB/s", "cores": threads,
+                         "kind": "port",
+                         "sample": f"first {sample} bytes of the large Markov stream, "
+                                   f"{threads} threads, one block per thread"},
+        "e2e": {"value": round(mbps, 2), "unit": "MB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--size", type=int, default=10 << 30)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-sample", type=int, default=256 << 20)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--slab", type=int, default=0)
+    ap.add_argument("--workers", type=int, default=0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    world, rank, local = dist_setup(args.gpus)
+    import torch
+
+    import bzip2gpu_b200 as B
+    import bzip2gpu_b200.workloads as W
+
+    if args.slab or args.workers:
+        B.set_engine(args.slab, args.workers)
+    n = args.size
+    seed = 0xB2C4 + 7919 * rank
+    d_in = W.large_stream(n, seed=seed, device=True)
+    torch.cuda.synchronize()
+    B.set_timing(True)
+
+    # warm-up (also checks the output decodes: first 2 blocks' worth through libbz2)
+    for _ in range(args.warmup):
+        out = B.compress_device(d_in, 9)
+    ratio = len(out) / n
+
+    def timed(fn):
+        barrier(world)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res = None
+        for _ in range(args.steps):
+            res = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        barrier(world)
+        return e0.elapsed_time(e1) / 1e3, res
+
+    l0 = B.launch_count()
+    with Clocks(local) as clk:
+        dt, out = timed(lambda: B.compress_device(d_in, 9))
+    launches = (B.launch_count() - l0) // max(args.steps, 1)
+    stats = B.last_stats()
+    dt = max_over_ranks(dt, world)
+    value = n * world * args.steps / dt / 1e6
+
+    e2e = None
+    if not args.no_e2e:
+        h_in = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+        h_in.copy_(d_in)
+        del d_in
+        torch.cuda.synchronize()
+        B.compress(h_in, 9)  # warm the host path
+        dte, oute = timed(lambda: B.compress(h_in, 9))
+        dte = max_over_ranks(dte, world)
+        e2e = {"value": round(n * world * args.steps / dte / 1e6, 2), "unit": "MB/s",
+               "h2d_bytes_per_step": n, "d2h_bytes_per_step": len(oute)}
+        host_sample = h_in[: min(n, args.cpu_sample)].numpy()
+    else:
+        host_sample = d_in[: min(n, args.cpu_sample)].cpu().numpy()
+
+    peak, peak_kind = peaks()
+    mb = B.model_bytes(stats)
+    step_s = dt / args.steps
+    achieved = mb / step_s / 1e9
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": None,
+            "kernel": "whole pipeline (stage-boundary byte model)",
+            "peak_kind": peak_kind,
+            "model_bytes_per_step": int(mb)}
+
+    cpu = None
+    if rank == 0 and world == 1:
+        threads = os.cpu_count() or 1
+        sample = host_sample.size
+        cpu_dt, _ = cpu_sample_time(host_sample, sample, threads)
+        cpu = {"value": round(sample / cpu_dt / 1e6, 2), "unit": "MB/s", "cores": threads,
+               "kind": "port",
+               "sample": f"first {sample} bytes of the same stream, oracle port of the "
+                         f"reference path, {threads} threads"}
+
+    if rank == 0:
+        stage_ms = {k[3:]: round(v / args.steps if False else v, 1)
+                    for k, v in stats.items() if k.startswith("ms_")}
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": "MB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(step_s * 1e3, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded generator, device-generated)",
+            "config": {"workload": WORKLOAD, "bytes_per_rank": n, "block_bytes": 900000,
+                       "level": 9, "form": "plain", "l2": "input larger than L2",
+                       "blocks": int(stats["blocks"]), "ratio": round(ratio, 4)},
+            "e2e": e2e, "roofline": roof, "cpu_baseline": cpu,
+            "clocks": clk.summary(), "gpu_launches": int(launches),
+            "stats": {k: stats[k] for k in ("n", "m", "A", "s", "g", "bits")},
+            "stage_ms_sum_over_slabs_last_step": stage_ms,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,305 @@
+"""bzip2gpu-b200: the bzip2gpu compression path on NVIDIA B200 (sm_100a).
+
+Python view of the C-ABI in include/bz2g.h (libbz2gpu_b200.so, built in-tree by
+``python -m bzip2gpu_b200.build``).  Whole-stream calls take host bytes;
+per-stage calls take torch CUDA tensors as device memory and mirror the
+reference's operators (include/compression.h of SebastianBoteroLeonik/bzip2gpu):
+rle1_compress, fbwt, fmtf, make_symbols_table, rle2_compress,
+huffman_build_trees, huffman_encode, count_frequencies, bzip2_crc32.
+
+There is no CPU fallback: every call runs the CUDA library, and loading fails
+loudly when it has not been built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+__all__ = [
+    "Bz2gError", "lib", "lib_path", "compress", "compress_device", "compress_bound",
+    "set_engine", "rle1", "crc32", "bwt", "mtf", "symbols_table", "rle2", "huffman_build",
+    "huffman_encode", "count_frequencies", "gen_markov", "gen_uniform", "MAX_GROUPS",
+    "MAX_ALPHA",
+]
+
+MAX_GROUPS = 6
+MAX_ALPHA = 258
+_LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libbz2gpu_b200.so"
+_lib = None
+
+_c = ctypes
+_vp, _i, _u8p, _sz = _c.c_void_p, _c.c_int, _c.POINTER(_c.c_uint8), _c.c_size_t
+
+_SIGS = {
+    "bz2g_last_error": (_c.c_char_p, []),
+    "bz2g_version": (_i, []),
+    "bz2g_compress": (_i, [_vp, _sz, _i, _i, _c.POINTER(_u8p), _c.POINTER(_sz)]),
+    "bz2g_compress_device": (_i, [_vp, _sz, _i, _i, _c.POINTER(_u8p), _c.POINTER(_sz)]),
+    "bz2g_compress_into": (_i, [_vp, _sz, _i, _i, _vp, _sz, _c.POINTER(_sz)]),
+    "bz2g_compress_bound": (_sz, [_sz, _i]),
+    "bz2g_free": (None, [_vp]),
+    "bz2g_set_engine": (_i, [_i, _i]),
+    "bz2g_set_timing": (_i, [_i]),
+    "bz2g_last_stats": (_i, [_c.POINTER(_c.c_double), _i]),
+    "bz2g_launch_count": (_c.c_int64, []),
+    "bz2g_rle1_bound": (_sz, [_sz]),
+    "bz2g_rle1": (_i, [_vp, _i, _vp, _c.POINTER(_i), _vp]),
+    "bz2g_crc32": (_i, [_vp, _sz, _c.POINTER(_c.c_uint32), _vp]),
+    "bz2g_bwt": (_i, [_vp, _i, _vp, _vp]),
+    "bz2g_mtf": (_i, [_vp, _vp, _i, _vp, _c.POINTER(_i), _vp, _c.POINTER(_i), _vp]),
+    "bz2g_symbols_table": (_i, [_vp, _i, _vp, _c.POINTER(_i), _vp]),
+    "bz2g_rle2": (_i, [_vp, _i, _i, _vp, _vp, _vp]),
+    "bz2g_huffman_build": (_i, [_vp, _i, _i, _vp, _vp, _vp, _c.POINTER(_i), _c.POINTER(_i), _vp]),
+    "bz2g_huffman_encode": (_i, [_vp, _i, _vp, _vp, _vp, _i, _i, _vp, _c.POINTER(_c.c_int64), _vp]),
+    "bz2g_count_frequencies": (_i, [_vp, _i, _vp, _vp]),
+    "bz2g_gen_markov": (_i, [_c.c_uint64, _vp, _i, _c.c_double, _c.c_double, _i, _i, _vp,
+                             _c.c_int64, _i, _vp]),
+    "bz2g_gen_uniform": (_i, [_c.c_uint64, _vp, _c.c_int64, _i, _vp]),
+}
+
+
+class Bz2gError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"bz2g error {code}: {msg}")
+        self.code = code
+
+
+def lib_path() -> Path:
+    return _LIB_PATH
+
+
+def lib():
+    """The loaded native library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not _LIB_PATH.exists():
+            raise RuntimeError(f"native library missing: {_LIB_PATH} "
+                               "(build it with `python -m bzip2gpu_b200.build`)")
+        L = ctypes.CDLL(str(_LIB_PATH))
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise Bz2gError(rc, lib().bz2g_last_error().decode(errors="replace"))
+
+
+def _stream(stream) -> int | None:
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    return int(stream)
+
+
+def _ptr(t) -> int:
+    return t.data_ptr()
+
+
+# ------------------------------------------------------------ whole stream
+def _host_view(data) -> tuple[np.ndarray, int]:
+    a = np.frombuffer(data, dtype=np.uint8) if isinstance(data, (bytes, bytearray, memoryview)) \
+        else np.ascontiguousarray(data, dtype=np.uint8).reshape(-1)
+    return a, a.ctypes.data
+
+
+def compress(data, level: int = 9, block_bytes: int = 900000) -> bytes:
+    """Whole .bz2 stream of host bytes (bytes / numpy uint8 / pinned tensor)."""
+    if hasattr(data, "data_ptr") and not getattr(data, "is_cuda", False):
+        ptr, n, keep = data.data_ptr(), data.numel(), data
+    else:
+        keep, ptr = _host_view(data)
+        n = keep.size
+    out = _u8p()
+    ln = _sz()
+    _check(lib().bz2g_compress(ptr if n else None, n, level, block_bytes, ctypes.byref(out),
+                               ctypes.byref(ln)))
+    try:
+        return ctypes.string_at(out, ln.value)
+    finally:
+        lib().bz2g_free(out)
+
+
+def compress_device(d_in, level: int = 9, block_bytes: int = 900000) -> bytes:
+    """Whole .bz2 stream of a CUDA uint8 tensor."""
+    out = _u8p()
+    ln = _sz()
+    n = d_in.numel()
+    _check(lib().bz2g_compress_device(_ptr(d_in) if n else None, n, level, block_bytes,
+                                      ctypes.byref(out), ctypes.byref(ln)))
+    try:
+        return ctypes.string_at(out, ln.value)
+    finally:
+        lib().bz2g_free(out)
+
+
+def compress_bound(n: int, block_bytes: int = 900000) -> int:
+    return lib().bz2g_compress_bound(n, block_bytes)
+
+
+def set_engine(slab_blocks: int = 0, workers: int = 0) -> None:
+    _check(lib().bz2g_set_engine(slab_blocks, workers))
+
+
+def set_timing(on: bool) -> None:
+    _check(lib().bz2g_set_timing(int(on)))
+
+
+STAT_FIELDS = ("blocks", "n", "m", "A", "s", "g", "bits", "ms_rle1", "ms_bwt", "ms_mtf",
+               "ms_rle2", "ms_huffman", "ms_sizes", "ms_place")
+
+
+def last_stats() -> dict:
+    """Statistics of the last whole-stream call on this thread."""
+    buf = (ctypes.c_double * len(STAT_FIELDS))()
+    lib().bz2g_last_stats(buf, len(STAT_FIELDS))
+    return dict(zip(STAT_FIELDS, list(buf)))
+
+
+def launch_count() -> int:
+    return int(lib().bz2g_launch_count())
+
+
+def model_bytes(st: dict) -> float:
+    """Algorithmic HBM bytes of the stage-boundary model:
+    n + 10m + 28A + 14s + 5g + bits/8 (each stage reads its input once and
+    writes its output once; a doubling round costs 28 bytes per rotation still
+    in a non-singleton group)."""
+    return st["n"] + 10 * st["m"] + 28 * st["A"] + 14 * st["s"] + 5 * st["g"] + st["bits"] / 8
+
+
+# --------------------------------------------------------------- per stage
+def rle1(d_in, stream=None):
+    """rle1_compress: RLE1 (runs cut at 259) of a CUDA uint8 tensor."""
+    import torch
+    n = d_in.numel()
+    out = torch.empty(lib().bz2g_rle1_bound(n), dtype=torch.uint8, device=d_in.device)
+    m = _i()
+    _check(lib().bz2g_rle1(_ptr(d_in), n, _ptr(out), ctypes.byref(m), _stream(stream)))
+    return out[: m.value]
+
+
+def crc32(d_in, stream=None) -> int:
+    """bzip2_crc32 of a CUDA uint8 tensor."""
+    c = ctypes.c_uint32()
+    _check(lib().bz2g_crc32(_ptr(d_in), d_in.numel(), ctypes.byref(c), _stream(stream)))
+    return c.value
+
+
+def bwt(d_in, stream=None):
+    """fbwt: int32 suffix array of the cyclic rotations."""
+    import torch
+    m = d_in.numel()
+    sa = torch.empty(max(m, 1), dtype=torch.int32, device=d_in.device)
+    _check(lib().bz2g_bwt(_ptr(d_in), m, _ptr(sa), _stream(stream)))
+    return sa[:m]
+
+
+def mtf(d_orig, d_sa, stream=None):
+    """fmtf: (mtf values, origPtr, present[256] as uint8, nInUse)."""
+    import torch
+    m = d_orig.numel()
+    out = torch.empty(max(m, 1), dtype=torch.uint8, device=d_orig.device)
+    op = _i(-1)
+    nu = _i()
+    pres = np.zeros(256, np.uint8)
+    _check(lib().bz2g_mtf(_ptr(d_orig), _ptr(d_sa), m, _ptr(out), ctypes.byref(op),
+                          pres.ctypes.data, ctypes.byref(nu), _stream(stream)))
+    return out[:m], op.value, pres, nu.value
+
+
+def symbols_table(d_in, stream=None) -> np.ndarray:
+    """make_symbols_table: ascending present byte values."""
+    tbl = np.zeros(256, np.uint8)
+    cnt = _i()
+    _check(lib().bz2g_symbols_table(_ptr(d_in), d_in.numel(), tbl.ctypes.data, ctypes.byref(cnt),
+                                    _stream(stream)))
+    return tbl[: cnt.value].copy()
+
+
+def rle2(d_mtf, table_size: int, stream=None):
+    """rle2_compress: RUNA/RUNB symbols (int16 tensor holding uint16 values)."""
+    import torch
+    m = d_mtf.numel()
+    out = torch.zeros(m + 1, dtype=torch.int16, device=d_mtf.device)
+    ln = torch.zeros(1, dtype=torch.int32, device=d_mtf.device)
+    _check(lib().bz2g_rle2(_ptr(d_mtf), m, table_size, _ptr(out), _ptr(ln), _stream(stream)))
+    return out[: int(ln.item())]
+
+
+def huffman_build(d_syms, n_in_use: int, stream=None):
+    """huffman_build_trees: (len[6,258], code[6,258], selectors, n_groups)."""
+    s = d_syms.numel()
+    ln = np.full((MAX_GROUPS, MAX_ALPHA), 0, np.uint8)
+    code = np.zeros((MAX_GROUPS, MAX_ALPHA), np.int32)
+    sel = np.zeros(max((s + 49) // 50, 1), np.uint8)
+    ns = _i()
+    ng = _i()
+    _check(lib().bz2g_huffman_build(_ptr(d_syms), s, n_in_use, ln.ctypes.data, code.ctypes.data,
+                                    sel.ctypes.data, ctypes.byref(ns), ctypes.byref(ng),
+                                    _stream(stream)))
+    return ln, code, sel[: ns.value], ng.value
+
+
+def huffman_encode(d_syms, len_tab: np.ndarray, code_tab: np.ndarray, d_sel, n_groups: int,
+                   stream=None):
+    """huffman_encode: (words as uint32 numpy array, total bits)."""
+    import torch
+    s = d_syms.numel()
+    lt = np.ascontiguousarray(len_tab, dtype=np.uint8)
+    ct = np.ascontiguousarray(code_tab, dtype=np.int32)
+    words = torch.zeros((17 * s + 31) // 32 + 1, dtype=torch.int32, device=d_syms.device)
+    bits = ctypes.c_int64()
+    _check(lib().bz2g_huffman_encode(_ptr(d_syms), s, lt.ctypes.data, ct.ctypes.data, _ptr(d_sel),
+                                     d_sel.numel(), n_groups, _ptr(words), ctypes.byref(bits),
+                                     _stream(stream)))
+    nw = (bits.value + 31) // 32
+    return words[:nw].cpu().numpy().view(np.uint32), bits.value
+
+
+def count_frequencies(d_syms, stream=None) -> np.ndarray:
+    import torch
+    f = torch.zeros(MAX_ALPHA, dtype=torch.int32, device=d_syms.device)
+    _check(lib().bz2g_count_frequencies(_ptr(d_syms), d_syms.numel(), _ptr(f), _stream(stream)))
+    return f.cpu().numpy()
+
+
+# ------------------------------------------------------- synthetic inputs
+def gen_markov(n: int, seed: int, alphabet, alpha: float, p_run: float, run_min: int,
+               run_max: int, out=None, device: bool = False, stream=None):
+    """Order-1 Markov bytes (bzip2gpu_b200/csrc/gen.cu).  Host numpy array, or
+    a CUDA uint8 tensor when device=True (or `out` is one)."""
+    alph = np.ascontiguousarray(alphabet, dtype=np.uint8)
+    if out is None:
+        if device:
+            import torch
+            out = torch.empty(n, dtype=torch.uint8, device="cuda")
+        else:
+            out = np.empty(n, np.uint8)
+    on_dev = hasattr(out, "is_cuda") and out.is_cuda
+    ptr = out.data_ptr() if hasattr(out, "data_ptr") else out.ctypes.data
+    _check(lib().bz2g_gen_markov(seed & (2**64 - 1), alph.ctypes.data, alph.size, alpha, p_run,
+                                 run_min, run_max, ptr, n, int(on_dev),
+                                 _stream(stream) if on_dev else None))
+    return out
+
+
+def gen_uniform(n: int, seed: int, out=None, device: bool = False, stream=None):
+    if out is None:
+        if device:
+            import torch
+            out = torch.empty(n, dtype=torch.uint8, device="cuda")
+        else:
+            out = np.empty(n, np.uint8)
+    on_dev = hasattr(out, "is_cuda") and out.is_cuda
+    ptr = out.data_ptr() if hasattr(out, "data_ptr") else out.ctypes.data
+    _check(lib().bz2g_gen_uniform(seed & (2**64 - 1), ptr, n, int(on_dev),
+                                  _stream(stream) if on_dev else None))
+    return out

@@ -1,0 +1,449 @@
+// C-ABI entry points (include/bz2g.h).  Per-stage calls run the slab kernels
+// on a one-block slab whose workspace is sized for the call.
+#include <cuda_runtime.h>
+
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/bz2g.h"
+#include "compressor.h"
+#include "engine.h"
+
+namespace bz2g {
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg) {
+  g_last_error = msg;
+  return code;
+}
+
+template <typename F>
+int guard(F &&f) {
+  try {
+    f();
+    g_last_error.clear();
+    return BZ2G_OK;
+  } catch (const Error &e) {
+    return fail(e.code, e.what());
+  } catch (const std::bad_alloc &) {
+    return fail(BZ2G_ERR_ALLOC, "host allocation failed");
+  } catch (const std::exception &e) {
+    return fail(BZ2G_ERR_INTERNAL, e.what());
+  }
+}
+
+__global__ void k_present(const uint8_t *in, int n, uint32_t *present) {
+  __shared__ uint32_t p[8];
+  if (threadIdx.x < 8) p[threadIdx.x] = 0;
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    atomicOr(&p[in[i] >> 5], 1u << (in[i] & 31));
+  __syncthreads();
+  if (threadIdx.x < 8 && p[threadIdx.x]) atomicOr(&present[threadIdx.x], p[threadIdx.x]);
+}
+
+__global__ void k_histogram(const uint16_t *syms, int s, int32_t *freq) {
+  __shared__ int h[kMaxAlpha];
+  for (int i = threadIdx.x; i < kMaxAlpha; i += blockDim.x) h[i] = 0;
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < s; i += gridDim.x * blockDim.x) {
+    int v = syms[i];
+    if (v < kMaxAlpha) atomicAdd(&h[v], 1);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < kMaxAlpha; i += blockDim.x)
+    if (h[i]) atomicAdd(&freq[i], h[i]);
+}
+
+__global__ void k_set_block(int32_t *arr, int v) { arr[0] = v; }
+
+cudaStream_t S(void *p) { return reinterpret_cast<cudaStream_t>(p); }
+
+// One-block slab sized for `n` raw bytes.
+struct OneBlock {
+  std::unique_ptr<Workspace> ws;
+  SlabPlan plan;
+  OneBlock(int n, cudaStream_t st) {
+    ws.reset(Workspace::create_for(1, std::max(n, 1)));
+    int len = std::max(n, 1);
+    plan.build(&len, 1);
+    ws->upload_plan(plan, st);
+  }
+  const SlabDev &d() const { return ws->dev; }
+};
+
+void set_int(int32_t *dst, int v, cudaStream_t st) {
+  k_set_block<<<1, 1, 0, st>>>(dst, v);
+  BZ_LAUNCH_CHECK();
+}
+
+// Engines for the whole-stream calls, per device and configuration.
+struct EngineKey {
+  int dev, slab, workers;
+  int64_t maxb;
+  bool operator<(const EngineKey &o) const {
+    return std::tie(dev, slab, workers, maxb) < std::tie(o.dev, o.slab, o.workers, o.maxb);
+  }
+};
+std::mutex g_eng_mu;
+std::map<EngineKey, std::unique_ptr<Compressor>> g_engines;
+int g_slab = 32, g_workers = 3;
+bool g_timing = false;
+thread_local StageTimes g_last_stats;
+
+Compressor &engine_for(int64_t block_bytes) {
+  int dev = 0;
+  BZ_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(g_eng_mu);
+  EngineKey k{dev, g_slab, g_workers, block_bytes};
+  auto it = g_engines.find(k);
+  if (it != g_engines.end()) return *it->second;
+  // one engine per device: drop engines of other shapes on this device
+  for (auto i = g_engines.begin(); i != g_engines.end();) {
+    if (i->first.dev == dev) i = g_engines.erase(i);
+    else ++i;
+  }
+  CompressorConfig cfg;
+  cfg.slab_blocks = g_slab;
+  cfg.workers = g_workers;
+  cfg.max_block_bytes = block_bytes;
+  auto c = std::make_unique<Compressor>(cfg);
+  Compressor &ref = *c;
+  g_engines[k] = std::move(c);
+  return ref;
+}
+
+void compress_any(const uint8_t *in, size_t n, int level, int block_bytes, bool on_device,
+                  std::vector<uint8_t> &out) {
+  BZ_REQUIRE(block_bytes > 0 && block_bytes <= (1 << 24), kErrArg,
+             "block_bytes must be in (0, 16 MiB]");
+  BZ_REQUIRE(n == 0 || in != nullptr, kErrArg, "null input");
+  const int64_t nb = ((int64_t)n + block_bytes - 1) / block_bytes;
+  std::vector<const uint8_t *> ptrs(nb);
+  std::vector<int> lens(nb);
+  for (int64_t b = 0; b < nb; b++) {
+    ptrs[b] = in + b * (int64_t)block_bytes;
+    lens[b] = (int)std::min<int64_t>(block_bytes, (int64_t)n - b * (int64_t)block_bytes);
+  }
+  Compressor &c = engine_for(std::max<int64_t>(block_bytes, 1));
+  const_cast<CompressorConfig &>(c.config()).time_stages = g_timing;
+  g_last_stats = StageTimes();
+  if (on_device)
+    c.compress_device(ptrs.data(), lens.data(), (int)nb, level, out, &g_last_stats);
+  else
+    c.compress(ptrs.data(), lens.data(), (int)nb, level, out, &g_last_stats);
+}
+
+}  // namespace
+}  // namespace bz2g
+
+using namespace bz2g;
+
+extern "C" {
+
+const char *bz2g_last_error(void) { return g_last_error.c_str(); }
+int bz2g_version(void) { return 1; }
+
+size_t bz2g_rle1_bound(size_t n) { return (size_t)rle1_bound((int64_t)n); }
+
+size_t bz2g_compress_bound(size_t n, int block_bytes) {
+  if (block_bytes <= 0) block_bytes = 900000;
+  size_t nb = (n + block_bytes - 1) / block_bytes;
+  return 64 + nb * 20000 + (rle1_bound((int64_t)n) + nb * 16) * kMaxCodeLen / 8 + 16;
+}
+
+int bz2g_set_engine(int slab_blocks, int workers) {
+  return guard([&] {
+    BZ_REQUIRE(slab_blocks >= 0 && workers >= 0, kErrArg, "negative engine shape");
+    std::lock_guard<std::mutex> g(g_eng_mu);
+    if (slab_blocks > 0) g_slab = slab_blocks;
+    if (workers > 0) g_workers = workers;
+  });
+}
+
+int bz2g_compress(const uint8_t *in, size_t n, int level, int block_bytes, uint8_t **out,
+                  size_t *out_len) {
+  return guard([&] {
+    BZ_REQUIRE(out && out_len, kErrArg, "null output pointer");
+    std::vector<uint8_t> v;
+    compress_any(in, n, level, block_bytes, false, v);
+    uint8_t *p = (uint8_t *)std::malloc(std::max<size_t>(v.size(), 1));
+    BZ_REQUIRE(p, kErrAlloc, "malloc failed");
+    std::memcpy(p, v.data(), v.size());
+    *out = p;
+    *out_len = v.size();
+  });
+}
+
+int bz2g_compress_device(const uint8_t *d_in, size_t n, int level, int block_bytes,
+                         uint8_t **out, size_t *out_len) {
+  return guard([&] {
+    BZ_REQUIRE(out && out_len, kErrArg, "null output pointer");
+    std::vector<uint8_t> v;
+    compress_any(d_in, n, level, block_bytes, true, v);
+    uint8_t *p = (uint8_t *)std::malloc(std::max<size_t>(v.size(), 1));
+    BZ_REQUIRE(p, kErrAlloc, "malloc failed");
+    std::memcpy(p, v.data(), v.size());
+    *out = p;
+    *out_len = v.size();
+  });
+}
+
+int bz2g_compress_into(const uint8_t *in, size_t n, int level, int block_bytes, uint8_t *out,
+                       size_t cap, size_t *out_len) {
+  return guard([&] {
+    BZ_REQUIRE(out && out_len, kErrArg, "null output pointer");
+    std::vector<uint8_t> v;
+    compress_any(in, n, level, block_bytes, false, v);
+    BZ_REQUIRE(v.size() <= cap, kErrTooLarge, "output buffer too small");
+    std::memcpy(out, v.data(), v.size());
+    *out_len = v.size();
+  });
+}
+
+void bz2g_free(void *p) { std::free(p); }
+
+int bz2g_set_timing(int on) {
+  std::lock_guard<std::mutex> g(g_eng_mu);
+  g_timing = on != 0;
+  return BZ2G_OK;
+}
+
+int bz2g_last_stats(double *out, int n) {
+  const StageTimes &t = g_last_stats;
+  const double v[] = {(double)t.blocks, (double)t.n, (double)t.m,  (double)t.A,
+                      (double)t.s,      (double)t.g, (double)t.bits, t.rle1,
+                      t.bwt,            t.mtf,       t.rle2,       t.huffman,
+                      t.sizes,          t.place};
+  const int k = (int)(sizeof(v) / sizeof(v[0]));
+  for (int i = 0; i < n && i < k; i++) out[i] = v[i];
+  return k;
+}
+
+int64_t bz2g_launch_count(void) { return launch_count(); }
+
+int bz2g_rle1(const uint8_t *d_in, int n, uint8_t *d_out, int *m, void *stream) {
+  return guard([&] {
+    BZ_REQUIRE(n >= 0 && m, kErrArg, "bad arguments");
+    if (n == 0) {
+      *m = 0;
+      return;
+    }
+    BZ_REQUIRE(d_in && d_out, kErrArg, "null device pointer");
+    cudaStream_t st = S(stream);
+    OneBlock ob(n, st);
+    const SlabDev &d = ob.d();
+    BZ_CUDA(cudaMemcpyAsync(d.raw, d_in, n, cudaMemcpyDeviceToDevice, st));
+    stage_rle1_crc(d, st);
+    BZ_CUDA(cudaMemcpyAsync(d.h_flags, d.m, 4, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaStreamSynchronize(st));
+    const int mm = d.h_flags[0];
+    BZ_CUDA(cudaMemcpyAsync(d_out, d.rle1, mm, cudaMemcpyDeviceToDevice, st));
+    BZ_CUDA(cudaStreamSynchronize(st));
+    *m = mm;
+  });
+}
+
+int bz2g_crc32(const uint8_t *d_in, size_t n, uint32_t *crc, void *stream) {
+  return guard([&] {
+    BZ_REQUIRE(crc, kErrArg, "null crc pointer");
+    BZ_REQUIRE(n < (size_t)1 << 30, kErrTooLarge, "crc input above 1 GiB");
+    if (n == 0) {
+      *crc = 0;
+      return;
+    }
+    cudaStream_t st = S(stream);
+    OneBlock ob((int)n, st);
+    const SlabDev &d = ob.d();
+    BZ_CUDA(cudaMemcpyAsync(d.raw, d_in, n, cudaMemcpyDeviceToDevice, st));
+    launch_crc_only(d, st);
+    BZ_CUDA(cudaMemcpyAsync(d.h_flags, d.crc, 4, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaStreamSynchronize(st));
+    *crc = (uint32_t)d.h_flags[0];
+  });
+}
+
+int bz2g_bwt(const uint8_t *d_in, int m, int32_t *d_sa, void *stream) {
+  return guard([&] {
+    BZ_REQUIRE(m >= 0, kErrArg, "negative length");
+    if (m == 0) return;
+    BZ_REQUIRE(d_in && d_sa, kErrArg, "null device pointer");
+    cudaStream_t st = S(stream);
+    OneBlock ob(m, st);
+    const SlabDev &d = ob.d();
+    BZ_CUDA(cudaMemcpyAsync(d.rle1, d_in, m, cudaMemcpyDeviceToDevice, st));
+    set_int(d.m, m, st);
+    stage_bwt(d, (int)rle1_bound(m), st);
+    BZ_CUDA(cudaMemcpyAsync(d_sa, d.sa, sizeof(int32_t) * m, cudaMemcpyDeviceToDevice, st));
+    BZ_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int bz2g_mtf(const uint8_t *d_orig, const int32_t *d_sa, int m, uint8_t *d_out, int *orig_ptr,
+             uint8_t *present, int *n_in_use, void *stream) {
+  return guard([&] {
+    BZ_REQUIRE(m >= 0, kErrArg, "negative length");
+    if (m == 0) {
+      if (n_in_use) *n_in_use = 0;
+      return;
+    }
+    BZ_REQUIRE(d_orig && d_sa && d_out, kErrArg, "null device pointer");
+    cudaStream_t st = S(stream);
+    OneBlock ob(m, st);
+    const SlabDev &d = ob.d();
+    BZ_CUDA(cudaMemcpyAsync(d.rle1, d_orig, m, cudaMemcpyDeviceToDevice, st));
+    BZ_CUDA(cudaMemcpyAsync(d.sa, d_sa, sizeof(int32_t) * m, cudaMemcpyDeviceToDevice, st));
+    set_int(d.m, m, st);
+    set_int(d.orig_ptr, m, st);
+    stage_mtf(d, st);
+    BZ_CUDA(cudaMemcpyAsync(d_out, d.mtf, m, cudaMemcpyDeviceToDevice, st));
+    BZ_CUDA(cudaMemcpyAsync(d.h_flags, d.orig_ptr, 4, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaMemcpyAsync(d.h_flags + 1, d.n_in_use, 4, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaMemcpyAsync(d.h_flags + 2, d.present, 32, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaStreamSynchronize(st));
+    if (orig_ptr) *orig_ptr = d.h_flags[0];
+    if (n_in_use) *n_in_use = d.h_flags[1];
+    if (present) {
+      const uint32_t *pw = reinterpret_cast<const uint32_t *>(d.h_flags + 2);
+      for (int c = 0; c < 256; c++) present[c] = (pw[c >> 5] >> (c & 31)) & 1u;
+    }
+  });
+}
+
+int bz2g_symbols_table(const uint8_t *d_in, int n, uint8_t *table, int *count, void *stream) {
+  return guard([&] {
+    BZ_REQUIRE(n >= 0 && table && count, kErrArg, "bad arguments");
+    cudaStream_t st = S(stream);
+    uint32_t *pres = nullptr;
+    BZ_CUDA(cudaMallocAsync((void **)&pres, 32, st));
+    BZ_CUDA(cudaMemsetAsync(pres, 0, 32, st));
+    if (n > 0) {
+      int grid = std::min((n + 255) / 256, 1184);
+      k_present<<<grid, 256, 0, st>>>(d_in, n, pres);
+      BZ_LAUNCH_CHECK();
+    }
+    uint32_t h[8];
+    BZ_CUDA(cudaMemcpyAsync(h, pres, 32, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaFreeAsync(pres, st));
+    BZ_CUDA(cudaStreamSynchronize(st));
+    int c = 0;
+    for (int v = 0; v < 256; v++)
+      if ((h[v >> 5] >> (v & 31)) & 1u) table[c++] = (uint8_t)v;
+    *count = c;
+  });
+}
+
+int bz2g_rle2(const uint8_t *d_in, int m, int table_size, uint16_t *d_out, uint32_t *d_out_len,
+              void *stream) {
+  return guard([&] {
+    BZ_REQUIRE(m >= 0 && d_out_len, kErrArg, "bad arguments");
+    cudaStream_t st = S(stream);
+    if (m == 0) {
+      BZ_CUDA(cudaMemsetAsync(d_out_len, 0, sizeof(uint32_t), st));
+      return;
+    }
+    BZ_REQUIRE(d_in && d_out, kErrArg, "null device pointer");
+    BZ_REQUIRE(table_size >= 0 && table_size <= 256, kErrArg, "table_size outside [0, 256]");
+    OneBlock ob(m, st);
+    const SlabDev &d = ob.d();
+    BZ_CUDA(cudaMemcpyAsync(d.mtf, d_in, m, cudaMemcpyDeviceToDevice, st));
+    set_int(d.m, m, st);
+    set_int(d.n_in_use, table_size, st);
+    stage_rle2(d, st);
+    BZ_CUDA(cudaMemcpyAsync(d.h_flags, d.s, 4, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaStreamSynchronize(st));
+    const int s = d.h_flags[0];
+    BZ_CUDA(cudaMemcpyAsync(d_out, d.rle2, sizeof(uint16_t) * s, cudaMemcpyDeviceToDevice, st));
+    BZ_CUDA(cudaMemcpyAsync(d_out_len, d.s, sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    BZ_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int bz2g_huffman_build(const uint16_t *d_syms, int s, int n_in_use, uint8_t *len, int32_t *code,
+                       uint8_t *selectors, int *n_selectors, int *n_groups, void *stream) {
+  return guard([&] {
+    BZ_REQUIRE(s > 0 && d_syms && len && code && selectors && n_groups, kErrArg,
+               "bad arguments");
+    BZ_REQUIRE(n_in_use >= 0 && n_in_use <= 256, kErrArg, "n_in_use outside [0, 256]");
+    cudaStream_t st = S(stream);
+    // capacity: s symbols need an element layout of at least s entries
+    OneBlock ob(s, st);
+    const SlabDev &d = ob.d();
+    BZ_CUDA(cudaMemcpyAsync(d.rle2, d_syms, sizeof(uint16_t) * s, cudaMemcpyDeviceToDevice, st));
+    set_int(d.s, s, st);
+    set_int(d.n_in_use, n_in_use, st);
+    BZ_CUDA(cudaMemsetAsync(d.freq, 0, sizeof(int32_t) * kMaxAlpha, st));
+    k_histogram<<<std::min((s + 255) / 256, 296), 256, 0, st>>>(d.rle2, s, d.freq);
+    BZ_LAUNCH_CHECK();
+    stage_huffman(d, st);
+    const int nsel = (s + 49) / 50;
+    std::vector<uint8_t> hl(kMaxGroups * kMaxAlpha);
+    std::vector<int32_t> hc(kMaxGroups * kMaxAlpha);
+    int ng = 0;
+    BZ_CUDA(cudaMemcpyAsync(hl.data(), d.len, hl.size(), cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaMemcpyAsync(hc.data(), d.code, hc.size() * 4, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaMemcpyAsync(selectors, d.sel, nsel, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaMemcpyAsync(&ng, d.n_groups, 4, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaStreamSynchronize(st));
+    const int alpha = n_in_use + 2;
+    for (int t = 0; t < kMaxGroups; t++)
+      for (int v = 0; v < alpha; v++) {
+        len[t * kMaxAlpha + v] = hl[t * kMaxAlpha + v];
+        if (t < ng) code[t * kMaxAlpha + v] = hc[t * kMaxAlpha + v];
+      }
+    *n_groups = ng;
+    if (n_selectors) *n_selectors = nsel;
+  });
+}
+
+int bz2g_huffman_encode(const uint16_t *d_syms, int s, const uint8_t *len, const int32_t *code,
+                        const uint8_t *d_selectors, int n_selectors, int n_groups,
+                        uint32_t *d_words, int64_t *bits, void *stream) {
+  return guard([&] {
+    BZ_REQUIRE(s > 0 && d_syms && len && code && d_selectors && d_words && bits, kErrArg,
+               "bad arguments");
+    BZ_REQUIRE(n_groups >= 1 && n_groups <= kMaxGroups, kErrArg, "n_groups outside [1, 6]");
+    BZ_REQUIRE(n_selectors >= (s + 49) / 50, kErrArg, "too few selectors for s symbols");
+    cudaStream_t st = S(stream);
+    OneBlock ob(s, st);
+    const SlabDev &d = ob.d();
+    BZ_CUDA(cudaMemcpyAsync(d.rle2, d_syms, sizeof(uint16_t) * s, cudaMemcpyDeviceToDevice, st));
+    BZ_CUDA(cudaMemcpyAsync(d.sel, d_selectors, (s + 49) / 50, cudaMemcpyDeviceToDevice, st));
+    std::vector<uint8_t> hl(len, len + kMaxGroups * kMaxAlpha);
+    std::vector<int32_t> hc(code, code + kMaxGroups * kMaxAlpha);
+    BZ_CUDA(cudaMemcpyAsync(d.len, hl.data(), hl.size(), cudaMemcpyHostToDevice, st));
+    BZ_CUDA(cudaMemcpyAsync(d.code, hc.data(), hc.size() * 4, cudaMemcpyHostToDevice, st));
+    set_int(d.s, s, st);
+    set_int(d.n_sel, (s + 49) / 50, st);
+    set_int(d.n_groups, n_groups, st);
+    stage_sizes_payload_only(d, st);
+    int64_t total = 0;
+    BZ_CUDA(cudaMemcpyAsync(&total, d.pay_bits, 8, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaStreamSynchronize(st));
+    BZ_CUDA(cudaMemsetAsync(d_words, 0, sizeof(uint32_t) * ((total + 31) / 32), st));
+    launch_pack_words(d, d_words, st);
+    BZ_CUDA(cudaStreamSynchronize(st));
+    *bits = total;
+  });
+}
+
+int bz2g_count_frequencies(const uint16_t *d_syms, int s, int32_t *d_freqs, void *stream) {
+  return guard([&] {
+    BZ_REQUIRE(s >= 0 && d_freqs, kErrArg, "bad arguments");
+    if (s == 0) return;
+    cudaStream_t st = S(stream);
+    k_histogram<<<std::min((s + 255) / 256, 296), 256, 0, st>>>(d_syms, s, d_freqs);
+    BZ_LAUNCH_CHECK();
+    BZ_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,59 @@
+// Whole-stream driver: splits the input into slabs of blocks, runs every
+// stage on the GPU, and concatenates the slabs' parts of the .bz2 stream.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <memory>
+#include <vector>
+
+namespace bz2g {
+
+class Workspace;
+
+struct StageTimes {
+  // milliseconds of device time summed over slabs (CUDA events on each
+  // worker's stream), filled when timing is enabled
+  double rle1 = 0, bwt = 0, mtf = 0, rle2 = 0, huffman = 0, sizes = 0, place = 0;
+  // totals over all blocks, for the HBM byte model
+  // B = n + 10m + 28A + 14s + 5g + bits/8
+  int64_t blocks = 0, n = 0, m = 0, A = 0, s = 0, g = 0, bits = 0;
+};
+
+struct CompressorConfig {
+  int slab_blocks = 32;
+  int workers = 3;
+  int64_t max_block_bytes = 900000;
+  bool time_stages = false;
+};
+
+class Compressor {
+ public:
+  explicit Compressor(const CompressorConfig &cfg);
+  ~Compressor();
+  // Compress the blocks (host memory; pinned memory makes the copies
+  // asynchronous) into one stream with header digit `level`; appends to out.
+  void compress(const uint8_t *const *ptrs, const int *lens, int nblocks, int level,
+                std::vector<uint8_t> &out, StageTimes *times = nullptr);
+  // Same, with the blocks already in device memory (raw bytes of block b at
+  // d_ptrs[b]).
+  void compress_device(const uint8_t *const *d_ptrs, const int *lens, int nblocks, int level,
+                       std::vector<uint8_t> &out, StageTimes *times = nullptr);
+  const CompressorConfig &config() const { return cfg_; }
+  int device() const { return device_; }
+
+ private:
+  struct Worker;
+  void run(const uint8_t *const *ptrs, const int *lens, int nblocks, int level, bool on_device,
+           std::vector<uint8_t> &out, StageTimes *times);
+  CompressorConfig cfg_;
+  int device_ = 0;
+  std::vector<std::unique_ptr<Worker>> workers_;
+};
+
+// Append the end-of-stream marker and combined CRC at bit offset `bit` of
+// `out` (whose last byte may be partial), then pad to a byte.
+void append_eos(std::vector<uint8_t> &out, int64_t bit, uint32_t stream_crc);
+
+}  // namespace bz2g

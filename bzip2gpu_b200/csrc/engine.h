@@ -1,0 +1,132 @@
+// Slab engine: every stage runs over a batch ("slab") of independent blocks.
+//
+// HBM layout of a slab (all per-block arrays are indexed by one shared
+// element layout, so a kernel finds a block's data at off[b]):
+//   raw      uint8   block b at raw_off[b] (16-byte aligned), raw_len[b] bytes
+//   rle1     uint8   block b at off[b], m[b] bytes           (off[b] % kTile == 0)
+//   sa, isa, head    int32 at off[b], m[b] entries (block-local indices)
+//   keys[2]  uint64, vals[2] uint32: radix sort ping-pong, same layout
+//   last     uint8   BWT last column, same layout
+//   mtf      uint8   same layout
+//   rle2     uint16  same layout, s[b] <= m[b] + 1 <= cap[b] symbols
+//   sel      uint8   selectors at off[b]/32 (cap[b]/32 >= cap[b]/50 + 1)
+//   out      uint32  big-endian words of the slab's part of the .bz2 stream
+// Tiles of kTile elements never cross blocks; tile_block[t] names the owner.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace bz2g {
+
+// Per-slab plan, built on the host from the raw block lengths.
+struct SlabPlan {
+  int nblocks = 0;
+  std::vector<int64_t> raw_off, off, cap;
+  std::vector<int> raw_len;
+  std::vector<int> rt_block, rt_start, rt_first;  // raw tiles (rt_first: nblocks+1)
+  std::vector<int> tile_block;          // element tiles
+  std::vector<int> gt_block, gt_first;  // group tiles (kGroupTile groups each)
+  std::vector<int> gt_begin;            // first group tile of each block (nblocks+1)
+  int64_t raw_total = 0, elem_total = 0;
+  int max_m_bound = 0;
+  void build(const int *lens, int n);
+};
+
+constexpr int kGroupTile = 128;  // 50-symbol groups per group tile
+
+// Device pointers of one slab, passed to kernels by value.
+struct SlabDev {
+  int nblocks, ntiles, n_raw_tiles, n_group_tiles;
+  // plan
+  const int64_t *raw_off, *off, *cap;
+  const int *raw_len, *rt_block, *rt_start, *rt_first, *tile_block, *gt_block, *gt_first, *gt_begin;
+  // data
+  uint8_t *raw, *rle1, *last, *mtf;
+  int32_t *sa, *isa, *head;
+  uint64_t *keys[2];
+  uint32_t *vals[2];
+  uint16_t *rle2;
+  uint8_t *sel, *sel_mtf;
+  uint32_t *out;
+  // per-tile scratch
+  int32_t *tile_a, *tile_b, *tile_c;  // [ntiles] or [n_raw_tiles]
+  uint32_t *tile_hist;                 // [ntiles * 256]
+  int32_t *tile_last;                  // [ntiles * 256]
+  uint32_t *gt_bits;                   // [n_group_tiles]
+  uint32_t *grp_bits;                  // per group, at sel layout
+  // per-block
+  int32_t *m, *s, *n_in_use, *orig_ptr, *n_groups, *n_sel;
+  uint32_t *crc, *crc_acc, *present;  // present: 8 words per block
+  int32_t *freq;                       // [nblocks * 258]
+  uint8_t *len;                        // [nblocks * 6 * 258]
+  int32_t *code;                       // [nblocks * 6 * 258]
+  int32_t *rfreq;                      // [nblocks * 6 * 258]
+  int32_t *sort_len, *done, *ngroups;  // BWT control
+  int64_t *active_sum;                 // A: rotations in non-singleton groups, summed over rounds
+  int32_t *pstat;                      // [nblocks * 8]: heads and singletons at prefix 1,2,4,8
+  int64_t *hdr_bits, *pay_bits, *blk_start;
+  // radix sort control
+  int32_t *sort_ctl;                   // [0]=cur buffer, [1]=nontrivial flag, [2]=blocks still sorting
+  int32_t *h_flags;                    // pinned host mirror of small counters
+  // stream state: [0] = bit offset (u64), [1] = stream crc, [2] = slab first word,
+  // [3] = slab word count
+  uint64_t *stream;
+};
+
+// Owns the device buffers of a slab context (sized for a maximum slab).
+class Workspace {
+ public:
+  Workspace(int max_blocks, int64_t max_raw, int64_t max_elems, int max_tiles,
+            int max_raw_tiles, int max_group_tiles);
+  ~Workspace();
+  // Sized for slabs of up to max_blocks blocks of up to max_block_bytes each.
+  static Workspace *create_for(int max_blocks, int64_t max_block_bytes);
+  Workspace(const Workspace &) = delete;
+  Workspace &operator=(const Workspace &) = delete;
+
+  // Upload a plan (async on `st`; the plan's host vectors must stay alive until
+  // the stream reaches this point, so they are copied into pinned staging).
+  void upload_plan(const SlabPlan &p, cudaStream_t st);
+  SlabDev dev;
+  int max_blocks;
+  int64_t max_raw, max_elems, out_words;
+  int max_tiles, max_raw_tiles, max_group_tiles;
+  void *pinned_plan = nullptr;
+  size_t pinned_plan_bytes = 0;
+
+ private:
+  std::vector<void *> allocs_;
+  void *plan_dev_ = nullptr;
+  void *alloc(size_t bytes);
+};
+
+// ------------------------------------------------------------------ stages
+void stage_rle1_crc(const SlabDev &d, cudaStream_t st);
+// BWT over rle1[off[b], m[b]) -> sa.  max_m: host bound of max m[b].
+void stage_bwt(const SlabDev &d, int max_m, cudaStream_t st);
+void stage_mtf(const SlabDev &d, cudaStream_t st);
+void stage_rle2(const SlabDev &d, cudaStream_t st);
+void stage_huffman(const SlabDev &d, cudaStream_t st);
+// payload bit counts, header bit counts and selector MTF
+void stage_sizes(const SlabDev &d, cudaStream_t st);
+// payload bit counts only (tables, selectors and symbols already in place)
+void stage_sizes_payload_only(const SlabDev &d, cudaStream_t st);
+// Zero the slab's output words and write headers and payloads at their final
+// stream positions.  slab_start_bit: stream bit offset of the slab's first
+// block; w0: stream word index of out[0]; nwords: words to zero.
+void stage_place(const SlabDev &d, int64_t slab_start_bit, int64_t w0, int64_t nwords,
+                 cudaStream_t st);
+
+// Kernel launches issued by this library so far.
+int64_t launch_count();
+
+// Individual pieces used by the per-stage C-ABI.
+void launch_crc_only(const SlabDev &d, cudaStream_t st);
+void launch_pack_words(const SlabDev &d, uint32_t *words, cudaStream_t st);
+
+}  // namespace bz2g

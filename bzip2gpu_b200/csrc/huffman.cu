@@ -1,0 +1,231 @@
+// Huffman table selection and code lengths, for every block of a slab.
+//
+// Reference: src/compression/huffman.cu:126-364 (bzip2 1.0.8 sendMTFValues
+// semantics): nGroups from the symbol count; initial tables from the symbol
+// histogram; 4 passes of (per 50-symbol group: cost of every table, first
+// minimum wins, per-table frequencies of the chosen groups) each followed by
+// length-limited (17) Huffman code lengths per table; canonical codes.
+// The histogram is defined as zeroed (the reference leaves it uninitialised).
+#include "engine.h"
+
+namespace bz2g {
+
+namespace {
+
+__global__ void k_huff_init(SlabDev d) {
+  const int b = blockIdx.x;
+  const int s = d.s[b];
+  const int alpha = d.n_in_use[b] + 2;
+  uint8_t *len = d.len + (size_t)b * kMaxGroups * kMaxAlpha;
+  for (int i = threadIdx.x; i < kMaxGroups * kMaxAlpha; i += blockDim.x) len[i] = 15;
+  __syncwarp();
+  if (threadIdx.x != 0) return;
+  const int ng = s < 200 ? 2 : s < 600 ? 3 : s < 1200 ? 4 : s < 2400 ? 5 : 6;
+  d.n_groups[b] = ng;
+  d.n_sel[b] = (s + 49) / 50;
+  // initial partition, src/compression/huffman.cu:148-185
+  const int32_t *freq = d.freq + (size_t)b * kMaxAlpha;
+  int gs = 0, remaining = s;
+  for (int n_part = ng; n_part > 0; n_part--) {
+    int t_freq = remaining / n_part;
+    int ge = gs - 1, a_freq = 0;
+    while (a_freq < t_freq && ge < alpha) {
+      ge++;
+      a_freq += ge < kMaxAlpha ? freq[ge] : 0;
+    }
+    if (ge > gs && n_part != ng && n_part != 1 && ((ng - n_part) % 2 == 1)) {
+      a_freq -= ge < kMaxAlpha ? freq[ge] : 0;
+      ge--;
+    }
+    uint8_t *row = len + (n_part - 1) * kMaxAlpha;
+    for (int v = 0; v < alpha; v++) row[v] = (v >= gs && v <= ge) ? 0 : 15;
+    gs = ge + 1;
+    remaining -= a_freq;
+  }
+}
+
+// One thread per 50-symbol group.  Costs of all tables are packed in 10-bit
+// fields of one 64-bit word per symbol (50 * 17 < 1024), so a group's six
+// costs are one 64-bit sum.
+__global__ void __launch_bounds__(kGroupTile) k_huff_select(SlabDev d) {
+  __shared__ uint16_t sy[kGroupTile * kGroupSize];
+  __shared__ uint64_t plen[kMaxAlpha];
+  __shared__ int rf[kMaxGroups * kMaxAlpha];
+  const int gt = blockIdx.x;
+  const int b = d.gt_block[gt];
+  const int g0 = d.gt_first[gt];
+  const int nsel = d.n_sel[b];
+  if (g0 >= nsel) return;
+  const int ng_here = min(kGroupTile, nsel - g0);
+  const int s = d.s[b];
+  const int ngrp = d.n_groups[b];
+  const int alpha = d.n_in_use[b] + 2;
+  const int64_t off = d.off[b];
+  const int sym0 = g0 * kGroupSize;
+  const int nsym = min(s, (g0 + ng_here) * kGroupSize) - sym0;
+  const uint8_t *len = d.len + (size_t)b * kMaxGroups * kMaxAlpha;
+  for (int i = threadIdx.x; i < nsym; i += blockDim.x) sy[i] = d.rle2[off + sym0 + i];
+  for (int v = threadIdx.x; v < kMaxAlpha; v += blockDim.x) {
+    uint64_t p = 0;
+    if (v < alpha)
+      for (int t = 0; t < ngrp; t++) p |= (uint64_t)len[t * kMaxAlpha + v] << (10 * t);
+    plen[v] = p;
+  }
+  for (int i = threadIdx.x; i < kMaxGroups * kMaxAlpha; i += blockDim.x) rf[i] = 0;
+  __syncthreads();
+  const int g = threadIdx.x;
+  if (g < ng_here) {
+    const int a = g * kGroupSize;
+    const int e = min(a + kGroupSize, nsym);
+    uint64_t cost = 0;
+    for (int i = a; i < e; i++) cost += plen[sy[i]];
+    uint32_t bc = 0xFFFFFFFFu;
+    int bt = -1;
+    for (int t = 0; t < ngrp; t++) {
+      uint32_t c = (uint32_t)(cost >> (10 * t)) & 1023u;
+      if (c < bc) {
+        bc = c;
+        bt = t;
+      }
+    }
+    d.sel[off / 32 + g0 + g] = (uint8_t)bt;
+    for (int i = a; i < e; i++) atomicAdd(&rf[bt * kMaxAlpha + sy[i]], 1);
+  }
+  __syncthreads();
+  int32_t *rfreq = d.rfreq + (size_t)b * kMaxGroups * kMaxAlpha;
+  for (int i = threadIdx.x; i < ngrp * kMaxAlpha; i += blockDim.x)
+    if (rf[i]) atomicAdd(&rfreq[i], rf[i]);
+}
+
+// bzip2's length-limited Huffman lengths (src/compression/huffman.cu:13-124),
+// one lane per table; heap, weight and parent arrays live in shared memory.
+constexpr int kHeapN = kMaxAlpha + 2;
+constexpr int kNodeN = kMaxAlpha * 2;
+
+__global__ void __launch_bounds__(32) k_huff_lengths(SlabDev d) {
+  __shared__ int32_t heap_s[kMaxGroups][kHeapN];
+  __shared__ int32_t weight_s[kMaxGroups][kNodeN];
+  __shared__ int32_t parent_s[kMaxGroups][kNodeN];
+  const int b = blockIdx.x;
+  const int t = threadIdx.x;
+  const int ngrp = d.n_groups[b];
+  if (t >= ngrp) return;
+  const int alpha = d.n_in_use[b] + 2;
+  int32_t *heap = heap_s[t];
+  int32_t *weight = weight_s[t];
+  int32_t *parent = parent_s[t];
+  const int32_t *freq = d.rfreq + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
+  uint8_t *len = d.len + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
+  for (int i = 0; i < alpha; i++) {
+    int f = freq[i];
+    weight[i + 1] = (f == 0 ? 1 : f) << 8;
+  }
+  for (;;) {
+    int n_nodes = alpha, n_heap = 0;
+    heap[0] = 0;
+    weight[0] = 0;
+    parent[0] = -2;
+    for (int i = 1; i <= alpha; i++) {
+      parent[i] = -1;
+      n_heap++;
+      heap[n_heap] = i;
+      int zz = n_heap, tmp = heap[zz];
+      while (weight[tmp] < weight[heap[zz >> 1]]) {
+        heap[zz] = heap[zz >> 1];
+        zz >>= 1;
+      }
+      heap[zz] = tmp;
+    }
+    while (n_heap > 1) {
+      int n1 = 0, n2 = 0;
+      for (int pick = 0; pick < 2; pick++) {
+        int top = heap[1];
+        heap[1] = heap[n_heap];
+        n_heap--;
+        int zz = 1, tmp = heap[zz];
+        const int wt = weight[tmp];
+        for (;;) {
+          int yy = zz << 1;
+          if (yy > n_heap) break;
+          if (yy < n_heap && weight[heap[yy + 1]] < weight[heap[yy]]) yy++;
+          if (wt < weight[heap[yy]]) break;
+          heap[zz] = heap[yy];
+          zz = yy;
+        }
+        heap[zz] = tmp;
+        if (pick == 0) n1 = top;
+        else n2 = top;
+      }
+      n_nodes++;
+      parent[n1] = parent[n2] = n_nodes;
+      int32_t w1 = weight[n1], w2 = weight[n2];
+      int32_t d1 = w1 & 0xff, d2 = w2 & 0xff;
+      weight[n_nodes] = (int32_t)(((uint32_t)(w1 & 0xffffff00) + (uint32_t)(w2 & 0xffffff00)) |
+                                  (uint32_t)(1 + (d1 > d2 ? d1 : d2)));
+      parent[n_nodes] = -1;
+      n_heap++;
+      heap[n_heap] = n_nodes;
+      int zz = n_heap, tmp = heap[zz];
+      while (weight[tmp] < weight[heap[zz >> 1]]) {
+        heap[zz] = heap[zz >> 1];
+        zz >>= 1;
+      }
+      heap[zz] = tmp;
+    }
+    bool too_long = false;
+    for (int i = 1; i <= alpha; i++) {
+      int j = 0, k = i;
+      while (parent[k] >= 0) {
+        k = parent[k];
+        j++;
+      }
+      len[i - 1] = (uint8_t)j;
+      if (j > kMaxCodeLen) too_long = true;
+    }
+    if (!too_long) break;
+    for (int i = 1; i <= alpha; i++) {
+      int j = weight[i] >> 8;
+      j = 1 + (j / 2);
+      weight[i] = j << 8;
+    }
+  }
+}
+
+// Canonical codes (src/compression/huffman.cu:135-146,352-362).
+__global__ void k_huff_codes(SlabDev d) {
+  const int b = blockIdx.x;
+  const int t = threadIdx.x;
+  if (t >= d.n_groups[b]) return;
+  const int alpha = d.n_in_use[b] + 2;
+  const uint8_t *len = d.len + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
+  int32_t *code = d.code + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
+  int mn = 32, mx = 0;
+  for (int v = 0; v < alpha; v++) {
+    mn = min(mn, (int)len[v]);
+    mx = max(mx, (int)len[v]);
+  }
+  int vec = 0;
+  for (int l = mn; l <= mx; l++) {
+    for (int v = 0; v < alpha; v++)
+      if (len[v] == l) code[v] = vec++;
+    vec <<= 1;
+  }
+}
+
+}  // namespace
+
+void stage_huffman(const SlabDev &d, cudaStream_t st) {
+  k_huff_init<<<d.nblocks, 32, 0, st>>>(d);
+  BZ_LAUNCH_CHECK();
+  for (int it = 0; it < kIters; it++) {
+    BZ_CUDA(cudaMemsetAsync(d.rfreq, 0, sizeof(int32_t) * kMaxGroups * kMaxAlpha * d.nblocks, st));
+    k_huff_select<<<d.n_group_tiles, kGroupTile, 0, st>>>(d);
+    BZ_LAUNCH_CHECK();
+    k_huff_lengths<<<d.nblocks, 32, 0, st>>>(d);
+    BZ_LAUNCH_CHECK();
+  }
+  k_huff_codes<<<d.nblocks, 32, 0, st>>>(d);
+  BZ_LAUNCH_CHECK();
+}
+
+}  // namespace bz2g

@@ -1,0 +1,298 @@
+// Block headers, payload bit packing and stream placement, for a slab.
+//
+// Reference: src/compression/huffman_encode.cu:15-143 (per-symbol code from
+// the group's table, exclusive scan of code lengths to bit offsets, MSB-first
+// placement) and src/compression/compress.cu:119-137,284-375 (selector MTF
+// and the block header fields).  Here the block header and payload are written
+// straight to their final bit position in the .bz2 stream: the output is an
+// array of big-endian 32-bit words (so memory order is stream byte order),
+// zeroed first and OR-ed into, since neighbouring blocks share edge words.
+#include "engine.h"
+
+namespace bz2g {
+
+namespace {
+
+__device__ __forceinline__ uint32_t bswap32(uint32_t w) { return __byte_perm(w, 0, 0x0123); }
+
+// MSB-first bit writer into zeroed big-endian words.
+struct BitSink {
+  uint32_t *out;
+  int64_t word;
+  uint64_t acc;
+  int n;
+  __device__ void init(uint32_t *o, int64_t bit) {
+    out = o;
+    word = bit >> 5;
+    acc = 0;
+    n = (int)(bit & 31);
+  }
+  __device__ __forceinline__ void put(uint32_t v, int nb) {
+    acc = (acc << nb) | v;
+    n += nb;
+    if (n >= 32) {
+      uint32_t w = (uint32_t)(acc >> (n - 32));
+      atomicOr(out + word, bswap32(w));
+      word++;
+      n -= 32;
+    }
+  }
+  __device__ void flush() {
+    if (n > 0) atomicOr(out + word, bswap32((uint32_t)(acc << (32 - n))));
+    n = 0;
+  }
+};
+
+// Selector MTF and header size; one warp per block.
+__global__ void k_sel_mtf_hdr(SlabDev d) {
+  const int b = blockIdx.x;
+  const int ngrp = d.n_groups[b];
+  const int nsel = d.n_sel[b];
+  const int alpha = d.n_in_use[b] + 2;
+  const uint8_t *sel = d.sel + d.off[b] / 32;
+  uint8_t *smtf = d.sel_mtf + d.off[b] / 32;
+  const int ln = threadIdx.x;
+  // table delta bits: lane t < ngrp
+  int64_t tb = 0;
+  if (ln < ngrp) {
+    const uint8_t *len = d.len + ((size_t)b * kMaxGroups + ln) * kMaxAlpha;
+    int cur = len[0];
+    tb = 5;
+    for (int v = 0; v < alpha; v++) {
+      int tg = len[v];
+      tb += 2 * abs(tg - cur) + 1;
+      cur = tg;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) tb += __shfl_xor_sync(0xffffffffu, tb, o);
+  // used 16-symbol ranges
+  int ranges = 0;
+  if (ln < 16) {
+    uint32_t w = d.present[b * 8 + (ln >> 1)];
+    uint32_t half = (ln & 1) ? (w >> 16) : (w & 0xffffu);
+    ranges = half != 0;
+  }
+  for (int o = 16; o > 0; o >>= 1) ranges += __shfl_xor_sync(0xffffffffu, ranges, o);
+  if (ln == 0) {
+    uint8_t pos[kMaxGroups];
+    for (int i = 0; i < ngrp; i++) pos[i] = (uint8_t)i;
+    int64_t unary = 0;
+    for (int i = 0; i < nsel; i++) {
+      uint8_t v = sel[i];
+      int j = 0;
+      uint8_t tmp = pos[0];
+      while (v != tmp) {
+        j++;
+        uint8_t t2 = tmp;
+        tmp = pos[j];
+        pos[j] = t2;
+      }
+      pos[0] = tmp;
+      smtf[i] = (uint8_t)j;
+      unary += j + 1;
+    }
+    d.hdr_bits[b] = 48 + 32 + 1 + 24 + 16 + 16 * ranges + 3 + 15 + unary + tb;
+  }
+}
+
+// Payload bits per 50-symbol group; exclusive offsets within the group tile.
+__global__ void __launch_bounds__(kGroupTile) k_pay_bits(SlabDev d) {
+  __shared__ uint32_t scratch[8];
+  const int gt = blockIdx.x;
+  const int b = d.gt_block[gt];
+  const int g0 = d.gt_first[gt];
+  const int nsel = d.n_sel[b];
+  if (g0 >= nsel) {
+    if (threadIdx.x == 0) d.gt_bits[gt] = 0;
+    return;
+  }
+  const int s = d.s[b];
+  const int64_t off = d.off[b];
+  const int g = g0 + threadIdx.x;
+  uint32_t bits = 0;
+  if (g < nsel) {
+    const int t = d.sel[off / 32 + g];
+    const uint8_t *len = d.len + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
+    const int a = g * kGroupSize, e = min(a + kGroupSize, s);
+    for (int i = a; i < e; i++) bits += len[d.rle2[off + i]];
+  }
+  uint32_t tot;
+  uint32_t ex = block_excl_sum(bits, scratch, &tot);
+  if (g < nsel) d.grp_bits[off / 32 + g] = ex;
+  if (threadIdx.x == 0) d.gt_bits[gt] = tot;
+}
+
+// Per block: exclusive sum over its group tiles; payload bits.
+__global__ void __launch_bounds__(256) k_pay_block(SlabDev d) {
+  __shared__ uint32_t scratch[40];
+  const int b = blockIdx.x;
+  const int t0 = d.gt_begin[b], nt = d.gt_begin[b + 1] - t0;
+  int64_t carry = 0;
+  for (int base = 0; base < nt; base += 256) {
+    int k = base + threadIdx.x;
+    uint32_t v = k < nt ? d.gt_bits[t0 + k] : 0;
+    uint32_t tot;
+    uint32_t ex = block_excl_sum(v, scratch, &tot);
+    if (k < nt) d.gt_bits[t0 + k] = (uint32_t)(carry + ex);
+    carry += tot;
+  }
+  if (threadIdx.x == 0) d.pay_bits[b] = carry;
+}
+
+__global__ void k_block_starts(SlabDev d, int64_t slab_start) {
+  if (threadIdx.x != 0) return;
+  int64_t run = slab_start;
+  for (int b = 0; b < d.nblocks; b++) {
+    d.blk_start[b] = run;
+    run += d.hdr_bits[b] + d.pay_bits[b];
+  }
+}
+
+// Block header at its stream position (src/compression/compress.cu:290-353).
+__global__ void k_write_header(SlabDev d, int64_t w0) {
+  if (threadIdx.x != 0) return;
+  const int b = blockIdx.x;
+  const int ngrp = d.n_groups[b];
+  const int nsel = d.n_sel[b];
+  const int alpha = d.n_in_use[b] + 2;
+  const uint32_t *pres = d.present + b * 8;
+  BitSink w;
+  w.init(d.out, d.blk_start[b] - w0 * 32);
+  w.put(0x314159u, 24);
+  w.put(0x265359u, 24);
+  w.put(d.crc[b], 32);
+  w.put(0, 1);
+  w.put((uint32_t)d.orig_ptr[b], 24);
+  uint32_t l1 = 0;
+  for (int r = 0; r < 16; r++) {
+    uint32_t half = (pres[r >> 1] >> ((r & 1) * 16)) & 0xffffu;
+    if (half) l1 |= 1u << (15 - r);
+  }
+  w.put(l1, 16);
+  for (int r = 0; r < 16; r++) {
+    uint32_t half = (pres[r >> 1] >> ((r & 1) * 16)) & 0xffffu;
+    if (!half) continue;
+    uint32_t l2 = 0;
+    for (int q = 0; q < 16; q++)
+      if ((half >> q) & 1u) l2 |= 1u << (15 - q);
+    w.put(l2, 16);
+  }
+  w.put((uint32_t)ngrp, 3);
+  w.put((uint32_t)nsel, 15);
+  const uint8_t *smtf = d.sel_mtf + d.off[b] / 32;
+  for (int i = 0; i < nsel; i++) {
+    int j = smtf[i];
+    w.put(((1u << j) - 1u) << 1, j + 1);
+  }
+  for (int t = 0; t < ngrp; t++) {
+    const uint8_t *len = d.len + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
+    int cur = len[0];
+    w.put((uint32_t)cur, 5);
+    for (int v = 0; v < alpha; v++) {
+      int tg = len[v];
+      while (cur < tg) {
+        w.put(2, 2);
+        cur++;
+      }
+      while (cur > tg) {
+        w.put(3, 2);
+        cur--;
+      }
+      w.put(0, 1);
+    }
+  }
+  w.flush();
+}
+
+// Payload: one thread per 50-symbol group.
+__global__ void __launch_bounds__(kGroupTile) k_write_payload(SlabDev d, int64_t w0) {
+  const int gt = blockIdx.x;
+  const int b = d.gt_block[gt];
+  const int g0 = d.gt_first[gt];
+  const int nsel = d.n_sel[b];
+  const int g = g0 + threadIdx.x;
+  if (g >= nsel) return;
+  const int s = d.s[b];
+  const int64_t off = d.off[b];
+  const int t = d.sel[off / 32 + g];
+  const uint8_t *len = d.len + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
+  const int32_t *code = d.code + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
+  int64_t bit = d.blk_start[b] + d.hdr_bits[b] + d.gt_bits[gt] + d.grp_bits[off / 32 + g];
+  BitSink w;
+  w.init(d.out, bit - w0 * 32);
+  const int a = g * kGroupSize, e = min(a + kGroupSize, s);
+  for (int i = a; i < e; i++) {
+    int v = d.rle2[off + i];
+    w.put((uint32_t)code[v], len[v]);
+  }
+  w.flush();
+}
+
+// Payload only, in the reference's word layout (word w = stream bits
+// [32w, 32w+32), first bit in the MSB, host byte order), for one block.
+__global__ void __launch_bounds__(kGroupTile) k_pack_words(SlabDev d, uint32_t *words) {
+  const int gt = blockIdx.x;
+  const int b = d.gt_block[gt];
+  const int g0 = d.gt_first[gt];
+  const int nsel = d.n_sel[b];
+  const int g = g0 + threadIdx.x;
+  if (g >= nsel) return;
+  const int s = d.s[b];
+  const int64_t off = d.off[b];
+  const int t = d.sel[off / 32 + g];
+  const uint8_t *len = d.len + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
+  const int32_t *code = d.code + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
+  int64_t bit = (int64_t)d.gt_bits[gt] + d.grp_bits[off / 32 + g];
+  int64_t word = bit >> 5;
+  int n = (int)(bit & 31);
+  uint64_t acc = 0;
+  const int a = g * kGroupSize, e = min(a + kGroupSize, s);
+  for (int i = a; i < e; i++) {
+    int v = d.rle2[off + i];
+    int nb = len[v];
+    acc = (acc << nb) | (uint32_t)code[v];
+    n += nb;
+    if (n >= 32) {
+      atomicOr(words + word, (uint32_t)(acc >> (n - 32)));
+      word++;
+      n -= 32;
+    }
+  }
+  if (n > 0) atomicOr(words + word, (uint32_t)(acc << (32 - n)));
+}
+
+}  // namespace
+
+void stage_sizes(const SlabDev &d, cudaStream_t st) {
+  k_sel_mtf_hdr<<<d.nblocks, 32, 0, st>>>(d);
+  BZ_LAUNCH_CHECK();
+  k_pay_bits<<<d.n_group_tiles, kGroupTile, 0, st>>>(d);
+  BZ_LAUNCH_CHECK();
+  k_pay_block<<<d.nblocks, 256, 0, st>>>(d);
+  BZ_LAUNCH_CHECK();
+}
+
+void stage_sizes_payload_only(const SlabDev &d, cudaStream_t st) {
+  k_pay_bits<<<d.n_group_tiles, kGroupTile, 0, st>>>(d);
+  BZ_LAUNCH_CHECK();
+  k_pay_block<<<d.nblocks, 256, 0, st>>>(d);
+  BZ_LAUNCH_CHECK();
+}
+
+void stage_place(const SlabDev &d, int64_t slab_start_bit, int64_t w0, int64_t nwords,
+                 cudaStream_t st) {
+  BZ_CUDA(cudaMemsetAsync(d.out, 0, sizeof(uint32_t) * nwords, st));
+  k_block_starts<<<1, 32, 0, st>>>(d, slab_start_bit);
+  BZ_LAUNCH_CHECK();
+  k_write_header<<<d.nblocks, 32, 0, st>>>(d, w0);
+  BZ_LAUNCH_CHECK();
+  k_write_payload<<<d.n_group_tiles, kGroupTile, 0, st>>>(d, w0);
+  BZ_LAUNCH_CHECK();
+}
+
+void launch_pack_words(const SlabDev &d, uint32_t *words, cudaStream_t st) {
+  k_pack_words<<<d.n_group_tiles, kGroupTile, 0, st>>>(d, words);
+  BZ_LAUNCH_CHECK();
+}
+
+}  // namespace bz2g

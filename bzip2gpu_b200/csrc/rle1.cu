@@ -1,0 +1,368 @@
+// RLE1 (runs cut at 259) and the block CRC-32, over every block of a slab.
+//
+// Reference: src/compression/rle1.cu:13-113 (RLE1), src/compression/crc32.cpp
+// (CRC).  A maximal run of length L is emitted as floor(L/259) chunks
+// "cccc 255" followed by the remainder r = L mod 259: r < 4 copies of c, or
+// "cccc (r-4)".  Position j of a run (j = i - run_start) emits
+//   1 byte (c)            if j mod 259 < 3,
+//   2 bytes (c, len-4)    if j mod 259 == 3,  len = length of its 259-chunk,
+//   nothing               otherwise,
+// so every output offset is an exclusive scan of a per-position count, and the
+// run start / end of a position are a max-scan / min-scan of run-start flags.
+//
+// CRC: crc0(D) (zero init, no final complement) is linear over GF(2), so each
+// 4096-byte tile's crc0 is shifted by x^(8 * bytes after the tile) mod P and
+// XOR-ed into the block; the init term ~0 * x^(8n) is added at the end.
+#include "engine.h"
+
+namespace bz2g {
+
+namespace {
+
+constexpr uint32_t kPoly = 0x04C11DB7u;
+
+constexpr uint32_t gf_mul_c(uint32_t a, uint32_t b) {
+  uint32_t r = 0;
+  for (int i = 31; i >= 0; --i) {
+    r = (r << 1) ^ ((r & 0x80000000u) ? kPoly : 0u);
+    if ((b >> i) & 1u) r ^= a;
+  }
+  return r;
+}
+constexpr uint32_t xpow8_pow2(int i) {
+  uint32_t v = 0x100u;  // x^8
+  for (int k = 0; k < i; ++k) v = gf_mul_c(v, v);
+  return v;
+}
+
+#define XP4(i) xpow8_pow2(i), xpow8_pow2(i + 1), xpow8_pow2(i + 2), xpow8_pow2(i + 3)
+// c_xpow[i] = x^(8 * 2^i) mod P
+__constant__ uint32_t c_xpow[32] = {XP4(0),  XP4(4),  XP4(8),  XP4(12),
+                                    XP4(16), XP4(20), XP4(24), XP4(28)};
+#undef XP4
+
+__device__ __forceinline__ uint32_t gf_mul(uint32_t a, uint32_t b) {
+  uint32_t r = 0;
+#pragma unroll 8
+  for (int i = 31; i >= 0; --i) {
+    r = (r << 1) ^ ((r & 0x80000000u) ? kPoly : 0u);
+    if ((b >> i) & 1u) r ^= a;
+  }
+  return r;
+}
+
+// x^(8j) mod P
+__device__ __forceinline__ uint32_t xpow8(uint64_t j) {
+  uint32_t r = 1u;
+  for (int i = 0; j; ++i, j >>= 1)
+    if (j & 1u) r = gf_mul(r, c_xpow[i]);
+  return r;
+}
+
+__device__ __forceinline__ void crc_table_fill(uint32_t *tbl) {
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+    uint32_t c = (uint32_t)i << 24;
+    for (int k = 0; k < 8; k++) c = (c & 0x80000000u) ? (c << 1) ^ kPoly : (c << 1);
+    tbl[i] = c;
+  }
+}
+
+// Stage one raw tile into shared memory: sb[0..len) = bytes, *prev = byte
+// before the tile (or -1 at the block start).
+__device__ __forceinline__ int load_raw_tile(const SlabDev &d, int t, uint8_t *sb, int *blk,
+                                             int *start, int *n_out, int *prev) {
+  int b = d.rt_block[t];
+  int st = d.rt_start[t];
+  int n = d.raw_len[b];
+  int len = min(kRawTile, n - st);
+  const uint8_t *base = d.raw + d.raw_off[b] + st;
+  int nw = (len + 15) >> 4;
+  for (int w = threadIdx.x; w < nw; w += blockDim.x)
+    reinterpret_cast<uint4 *>(sb)[w] = reinterpret_cast<const uint4 *>(base)[w];
+  *prev = st > 0 ? (int)base[-1] : -1;
+  *blk = b;
+  *start = st;
+  *n_out = n;
+  return len;
+}
+
+__global__ void __launch_bounds__(256) k_rle1_scan_tiles(SlabDev d) {
+  __shared__ __align__(16) uint8_t sb[kRawTile + 16];
+  __shared__ uint32_t tbl[256];
+  __shared__ int red[2][9];
+  const int t = blockIdx.x;
+  int b, st, n, prev;
+  crc_table_fill(tbl);
+  int len = load_raw_tile(d, t, sb, &b, &st, &n, &prev);
+  __syncthreads();
+
+  // run starts: first and last in this tile (block-local indices)
+  int first = INT32_MAX, last = -1;
+  const int p0 = threadIdx.x * kTileItems;
+  for (int k = 0; k < kTileItems; k++) {
+    int p = p0 + k;
+    if (p >= len) break;
+    int pv = p == 0 ? prev : (int)sb[p - 1];
+    if ((int)sb[p] != pv) {
+      first = min(first, st + p);
+      last = max(last, st + p);
+    }
+  }
+  // block min / max
+  for (int o = 16; o > 0; o >>= 1) {
+    first = min(first, __shfl_xor_sync(0xffffffffu, first, o));
+    last = max(last, __shfl_xor_sync(0xffffffffu, last, o));
+  }
+  if (lane_id() == 0) {
+    red[0][warp_id()] = first;
+    red[1][warp_id()] = last;
+  }
+
+  // CRC of the tile, right-aligned into a virtual 4096-byte tile (leading
+  // zeros leave a zero-init CRC unchanged)
+  if (warp_id() == 0) {
+    const int pad = kRawTile - len;
+    uint32_t r = 0;
+    const int v0 = lane_id() * 128;
+    for (int v = max(v0, pad); v < v0 + 128; v++) {
+      uint32_t byte = sb[v - pad];
+      r = (r << 8) ^ tbl[(r >> 24) ^ byte];
+    }
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+      int dd = 1 << k;
+      uint32_t o = __shfl_down_sync(0xffffffffu, r, dd);
+      if ((lane_id() & (2 * dd - 1)) == 0) r = gf_mul(r, c_xpow[7 + k]) ^ o;
+    }
+    if (lane_id() == 0) {
+      uint64_t after = (uint64_t)(n - (st + len));
+      atomicXor(&d.crc_acc[b], gf_mul(r, xpow8(after)));
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int f = INT32_MAX, l = -1;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+      f = min(f, red[0][w]);
+      l = max(l, red[1][w]);
+    }
+    d.tile_a[t] = f;  // first run start in tile
+    d.tile_b[t] = l;  // last run start in tile
+  }
+}
+
+// Per block: exclusive max of last-starts (run start carried into a tile) and
+// exclusive min of first-starts (next run start after a tile), and the CRC.
+__global__ void __launch_bounds__(256) k_rle1_block_carry(SlabDev d, const int *rt_first) {
+  __shared__ int scratch[40];
+  __shared__ int sx[256];
+  const int b = blockIdx.x;
+  const int t0 = rt_first[b], nt = rt_first[b + 1] - t0;
+  const int n = d.raw_len[b];
+  int carry = -1;
+  for (int base = 0; base < nt; base += 256) {
+    int k = base + threadIdx.x;
+    int v = k < nt ? d.tile_b[t0 + k] : -1;
+    int inc = block_incl_max(v, scratch, -1);
+    sx[threadIdx.x] = inc;
+    __syncthreads();
+    int ex = threadIdx.x == 0 ? carry : max(carry, sx[threadIdx.x - 1]);
+    if (k < nt) d.tile_b[t0 + k] = ex;
+    int c2 = max(carry, sx[255]);
+    __syncthreads();
+    carry = c2;
+  }
+  int carry_min = n;
+  // walk backwards for the suffix minimum
+  for (int base = ((nt - 1) / 256) * 256; base >= 0; base -= 256) {
+    int k = base + threadIdx.x;
+    int v = k < nt ? d.tile_a[t0 + k] : INT32_MAX;
+    int inc = block_suffix_min(v, scratch, INT32_MAX);
+    sx[threadIdx.x] = inc;
+    __syncthreads();
+    int ex = threadIdx.x == 255 ? carry_min : min(carry_min, sx[threadIdx.x + 1]);
+    if (k < nt) d.tile_a[t0 + k] = ex;
+    int c2 = min(carry_min, sx[0]);
+    __syncthreads();
+    carry_min = c2;
+  }
+  if (threadIdx.x == 0) d.crc[b] = ~(gf_mul(0xFFFFFFFFu, xpow8((uint64_t)n)) ^ d.crc_acc[b]);
+}
+
+__device__ __forceinline__ int rle1_count_of(int j) {
+  int q = j % 259;
+  return q < 3 ? 1 : (q == 3 ? 2 : 0);
+}
+
+__global__ void __launch_bounds__(256) k_rle1_count(SlabDev d) {
+  __shared__ __align__(16) uint8_t sb[kRawTile + 16];
+  __shared__ int scratch[40];
+  const int t = blockIdx.x;
+  int b, st, n, prev;
+  int len = load_raw_tile(d, t, sb, &b, &st, &n, &prev);
+  __syncthreads();
+  const int p0 = threadIdx.x * kTileItems;
+  int ls = -1;
+  for (int k = 0; k < kTileItems; k++) {
+    int p = p0 + k;
+    if (p >= len) break;
+    int pv = p == 0 ? prev : (int)sb[p - 1];
+    if ((int)sb[p] != pv) ls = st + p;
+  }
+  int inc = block_incl_max(ls, scratch, -1);
+  // exclusive: max over earlier threads, with the tile carry
+  int ex = __shfl_up_sync(0xffffffffu, inc, 1);
+  __shared__ int wl[8];
+  if (lane_id() == 31) wl[warp_id()] = inc;
+  __syncthreads();
+  if (lane_id() == 0) ex = warp_id() == 0 ? -1 : wl[warp_id() - 1];
+  int cur = max(ex, d.tile_b[t]);
+  int cnt = 0;
+  for (int k = 0; k < kTileItems; k++) {
+    int p = p0 + k;
+    if (p >= len) break;
+    int pv = p == 0 ? prev : (int)sb[p - 1];
+    if ((int)sb[p] != pv) cur = st + p;
+    cnt += rle1_count_of(st + p - cur);
+  }
+  int total;
+  block_excl_sum(cnt, scratch, &total);
+  if (threadIdx.x == 0) d.tile_c[t] = total;
+}
+
+// Per block: exclusive sum of tile output counts; m[b] = RLE1 length.
+__global__ void __launch_bounds__(256) k_rle1_block_offsets(SlabDev d, const int *rt_first) {
+  __shared__ int scratch[40];
+  const int b = blockIdx.x;
+  const int t0 = rt_first[b], nt = rt_first[b + 1] - t0;
+  int carry = 0;
+  for (int base = 0; base < nt; base += 256) {
+    int k = base + threadIdx.x;
+    int v = k < nt ? d.tile_c[t0 + k] : 0;
+    int tot;
+    int ex = block_excl_sum(v, scratch, &tot);
+    if (k < nt) d.tile_c[t0 + k] = carry + ex;
+    carry += tot;
+  }
+  if (threadIdx.x == 0) d.m[b] = carry;
+}
+
+__global__ void __launch_bounds__(256) k_rle1_write(SlabDev d) {
+  __shared__ __align__(16) uint8_t sb[kRawTile + 16];
+  __shared__ int scratch[40];
+  __shared__ int wl[8], wf[8];
+  const int t = blockIdx.x;
+  int b, st, n, prev;
+  int len = load_raw_tile(d, t, sb, &b, &st, &n, &prev);
+  __syncthreads();
+  const int p0 = threadIdx.x * kTileItems;
+  int ls = -1, fs = INT32_MAX;
+  for (int k = 0; k < kTileItems; k++) {
+    int p = p0 + k;
+    if (p >= len) break;
+    int pv = p == 0 ? prev : (int)sb[p - 1];
+    if ((int)sb[p] != pv) {
+      ls = st + p;
+      fs = min(fs, st + p);
+    }
+  }
+  // exclusive max of last starts over earlier threads
+  int inc = warp_incl_max(ls);
+  int exw = __shfl_up_sync(0xffffffffu, inc, 1);
+  if (lane_id() == 31) wl[warp_id()] = inc;
+  // exclusive min of first starts over later threads
+  int incm = warp_incl_min_rev(fs);
+  int exm = __shfl_down_sync(0xffffffffu, incm, 1);
+  if (lane_id() == 0) wf[warp_id()] = incm;
+  __syncthreads();
+  int before = lane_id() == 0 ? -1 : exw;
+  for (int w = 0; w < (int)warp_id(); w++) before = max(before, wl[w]);
+  int after = lane_id() == 31 ? INT32_MAX : exm;
+  for (int w = warp_id() + 1; w < (int)(blockDim.x >> 5); w++) after = min(after, wf[w]);
+  before = max(before, d.tile_b[t]);
+  after = min(after, d.tile_a[t]);  // next start after the tile (or n)
+
+  int ends[kTileItems];
+  {
+    int cur = after;
+#pragma unroll
+    for (int k = kTileItems - 1; k >= 0; k--) {
+      int p = p0 + k;
+      ends[k] = cur;
+      if (p < len) {
+        int pv = p == 0 ? prev : (int)sb[p - 1];
+        if ((int)sb[p] != pv) cur = st + p;
+      }
+    }
+  }
+  int cnt = 0;
+  {
+    int cur = before;
+    for (int k = 0; k < kTileItems; k++) {
+      int p = p0 + k;
+      if (p >= len) break;
+      int pv = p == 0 ? prev : (int)sb[p - 1];
+      if ((int)sb[p] != pv) cur = st + p;
+      cnt += rle1_count_of(st + p - cur);
+    }
+  }
+  int tot;
+  int o = block_excl_sum(cnt, scratch, &tot);
+  uint8_t *out = d.rle1 + d.off[b] + d.tile_c[t] + o;
+  int cur = before;
+#pragma unroll
+  for (int k = 0; k < kTileItems; k++) {
+    int p = p0 + k;
+    if (p < len) {
+      uint8_t c = sb[p];
+      int pv = p == 0 ? prev : (int)sb[p - 1];
+      if ((int)c != pv) cur = st + p;
+      int j = st + p - cur;
+      int q = j % 259;
+      if (q < 3) {
+        *out++ = c;
+      } else if (q == 3) {
+        int run_len = ends[k] - cur;
+        int chunk_len = min(259, run_len - (j / 259) * 259);
+        *out++ = c;
+        *out++ = (uint8_t)(chunk_len - 4);
+      }
+    }
+  }
+}
+
+}  // namespace
+
+void stage_rle1_crc(const SlabDev &d, cudaStream_t st) {
+  const int *rt_first = d.rt_first;
+  BZ_CUDA(cudaMemsetAsync(d.crc_acc, 0, sizeof(uint32_t) * d.nblocks, st));
+  if (d.n_raw_tiles > 0) {
+    k_rle1_scan_tiles<<<d.n_raw_tiles, 256, 0, st>>>(d);
+    BZ_LAUNCH_CHECK();
+  }
+  k_rle1_block_carry<<<d.nblocks, 256, 0, st>>>(d, rt_first);
+  BZ_LAUNCH_CHECK();
+  if (d.n_raw_tiles > 0) {
+    k_rle1_count<<<d.n_raw_tiles, 256, 0, st>>>(d);
+    BZ_LAUNCH_CHECK();
+  }
+  k_rle1_block_offsets<<<d.nblocks, 256, 0, st>>>(d, rt_first);
+  BZ_LAUNCH_CHECK();
+  if (d.n_raw_tiles > 0) {
+    k_rle1_write<<<d.n_raw_tiles, 256, 0, st>>>(d);
+    BZ_LAUNCH_CHECK();
+  }
+}
+
+void launch_crc_only(const SlabDev &d, cudaStream_t st) {
+  const int *rt_first = d.rt_first;
+  BZ_CUDA(cudaMemsetAsync(d.crc_acc, 0, sizeof(uint32_t) * d.nblocks, st));
+  if (d.n_raw_tiles > 0) {
+    k_rle1_scan_tiles<<<d.n_raw_tiles, 256, 0, st>>>(d);
+    BZ_LAUNCH_CHECK();
+  }
+  k_rle1_block_carry<<<d.nblocks, 256, 0, st>>>(d, rt_first);
+  BZ_LAUNCH_CHECK();
+}
+
+}  // namespace bz2g

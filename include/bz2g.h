@@ -1,0 +1,160 @@
+/*
+ * bz2g.h -- C-ABI of bzip2gpu-b200, the B200 (sm_100a) implementation of the
+ * bzip2gpu compression path.
+ *
+ * Plain pointers and sizes only.  "d_" arguments are device pointers on the
+ * current CUDA device; `stream` is a cudaStream_t (NULL = legacy default
+ * stream).  Every function returns BZ2G_OK or an error code; the message of
+ * the last error on the calling thread is bz2g_last_error().  Functions that
+ * return host-visible results (lengths, origPtr, tables) synchronise `stream`
+ * before returning, as the reference's do.
+ *
+ * Each declaration names the reference interface it replaces (paths are
+ * within SebastianBoteroLeonik/bzip2gpu).
+ */
+#ifndef BZ2G_H
+#define BZ2G_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BZ2G_OK 0
+#define BZ2G_ERR_CUDA 1
+#define BZ2G_ERR_ARG 2
+#define BZ2G_ERR_ALLOC 3
+#define BZ2G_ERR_INTERNAL 4
+#define BZ2G_ERR_TOO_LARGE 5
+
+#define BZ2G_MAX_GROUPS 6  /* include/compression.h:65 max_n_groups */
+#define BZ2G_MAX_ALPHA 258 /* include/compression.h:66 max_alphabet_size */
+
+const char *bz2g_last_error(void);
+int bz2g_version(void);
+
+/* ----------------------------------------------------------- whole stream */
+
+/* Compress n host bytes into a complete .bz2 stream: header "BZh" + level
+ * digit, one block per block_bytes raw bytes (the reference always splits at
+ * its input buffer size, 900000), end-of-stream marker and combined CRC.
+ * *out is allocated here (release with bz2g_free).  Empty input gives the
+ * 14-byte empty stream.
+ * Replaces: bzip2_gpu_compress(BZFileInputStream&, int n, std::vector<uint8_t>&)
+ *           include/compression.h:86-87, src/compression/compress.cu:184-378 */
+int bz2g_compress(const uint8_t *in, size_t n, int level, int block_bytes, uint8_t **out,
+                  size_t *out_len);
+
+/* As bz2g_compress with the input already in device memory. */
+int bz2g_compress_device(const uint8_t *d_in, size_t n, int level, int block_bytes,
+                         uint8_t **out, size_t *out_len);
+
+/* As bz2g_compress into a caller buffer of `cap` bytes (BZ2G_ERR_TOO_LARGE if
+ * it does not fit; bz2g_compress_bound gives a sufficient size). */
+int bz2g_compress_into(const uint8_t *in, size_t n, int level, int block_bytes, uint8_t *out,
+                       size_t cap, size_t *out_len);
+size_t bz2g_compress_bound(size_t n, int block_bytes);
+void bz2g_free(void *p);
+
+/* Engine shape used by the whole-stream calls on this thread's device:
+ * blocks per slab and worker streams.  0 keeps the current value. */
+int bz2g_set_engine(int slab_blocks, int workers);
+
+/* Measurement (no counterpart in the reference, which only prints wall-clock
+ * Stopwatch lines, include/stopwatch.h:12-42).  bz2g_set_timing(1) records
+ * CUDA events around every stage of the following whole-stream calls.
+ * bz2g_last_stats fills out[0..n) with, for the last whole-stream call on
+ * this thread: blocks, sum n, sum m, sum A, sum s, sum groups, payload bits,
+ * then device ms of RLE1+CRC, BWT, MTF, RLE2, Huffman, sizes, placement;
+ * returns the number of fields.  bz2g_launch_count: kernels launched by this
+ * library since it was loaded. */
+int bz2g_set_timing(int on);
+int bz2g_last_stats(double *out, int n);
+int64_t bz2g_launch_count(void);
+
+/* ------------------------------------------------------------- per stage */
+
+/* Upper bound of the RLE1 output of n bytes (n + n/4 + 8). */
+size_t bz2g_rle1_bound(size_t n);
+
+/* RLE1 with runs cut at 259; d_out holds bz2g_rle1_bound(n) bytes; *m gets
+ * the output length.
+ * Replaces: int rle1_compress(const uint8_t*, int, uint8_t*&, cudaStream_t)
+ *           include/compression.h:17-18, src/compression/rle1.cu:60-113 */
+int bz2g_rle1(const uint8_t *d_in, int n, uint8_t *d_out, int *m, void *stream);
+
+/* bzip2 block CRC of n device bytes.
+ * Replaces: uint32_t bzip2_crc32(const uint8_t*, size_t)
+ *           src/compression/crc32.h:7-8, src/compression/crc32.cpp:22-29 */
+int bz2g_crc32(const uint8_t *d_in, size_t n, uint32_t *crc, void *stream);
+
+/* Suffix array of the cyclic rotations of d_in[0..m) (equal rotations in
+ * index order) into d_sa[0..m).
+ * Replaces: void fbwt(const uint8_t*, int, int*&, cudaStream_t)
+ *           include/compression.h:81, src/compression/fbwt.cu:47-106 */
+int bz2g_bwt(const uint8_t *d_in, int m, int32_t *d_sa, void *stream);
+
+/* Move-to-front of L[i] = d_orig[(d_sa[i]-1) mod m] with the list starting as
+ * the ascending in-use symbols; *orig_ptr = i with d_sa[i] == 0; present
+ * (256 bytes, may be NULL) gets 0/1 per byte value; *n_in_use the count.
+ * Replaces: int fmtf(const uint8_t*, const int*, int, uint8_t*&, int&, bool*,
+ *           cudaStream_t) include/compression.h:53-55, src/compression/fmtf.cu:147-230 */
+int bz2g_mtf(const uint8_t *d_orig, const int32_t *d_sa, int m, uint8_t *d_out, int *orig_ptr,
+             uint8_t *present, int *n_in_use, void *stream);
+
+/* Ascending byte values present in d_in[0..n) into table (256 bytes).
+ * Replaces: int make_symbols_table(const uint8_t*, int, uint8_t*&, cudaStream_t)
+ *           include/compression.h:43-44, src/compression/fmtf.cu:114-140 */
+int bz2g_symbols_table(const uint8_t *d_in, int n, uint8_t *table, int *count, void *stream);
+
+/* RUNA/RUNB coding of MTF values, EOB = table_size + 1.  d_out holds m + 1
+ * symbols; *d_out_len (device) gets the count.  m == 0 writes 0 and no EOB.
+ * Replaces: void rle2_compress(const uint8_t*, int, uint16_t*, uint32_t*, int,
+ *           cudaStream_t) include/compression.h:30-31, src/compression/rle2.cu:99-158 */
+int bz2g_rle2(const uint8_t *d_in, int m, int table_size, uint16_t *d_out, uint32_t *d_out_len,
+              void *stream);
+
+/* Table selection (4 refinement passes), code lengths (max 17) and canonical
+ * codes for s symbols over nInUse + 2 values.  len / code are host arrays
+ * [6][258] (rows >= *n_groups of code untouched); selectors is a host array
+ * of ceil(s/50) bytes.
+ * Replaces: int huffman_build_trees(uint16_t*, int, int, uint8_t[6][258],
+ *           int32_t[6][258], uint8_t*&, int&, cudaStream_t)
+ *           include/compression.h:67-72, src/compression/huffman.cu:256-364 */
+int bz2g_huffman_build(const uint16_t *d_syms, int s, int n_in_use, uint8_t *len, int32_t *code,
+                       uint8_t *selectors, int *n_selectors, int *n_groups, void *stream);
+
+/* MSB-first packing of the codes into 32-bit words (word w = bits
+ * [32w, 32w+32), first bit in the MSB).  d_words must hold
+ * (17 * s + 31) / 32 words; *bits gets the bit count.
+ * Replaces: int huffman_encode(uint16_t*, int, int, uint32_t*&, uint8_t[6][258],
+ *           int32_t[6][258], uint8_t*, int32_t, int, cudaStream_t)
+ *           include/compression.h:89-94, src/compression/huffman_encode.cu:75-143 */
+int bz2g_huffman_encode(const uint16_t *d_syms, int s, const uint8_t *len, const int32_t *code,
+                        const uint8_t *d_selectors, int n_selectors, int n_groups,
+                        uint32_t *d_words, int64_t *bits, void *stream);
+
+/* Symbol histogram over 258 values (freqs is a device array the caller has
+ * zeroed, as the reference's own test does).
+ * Replaces: __global__ count_frequencies(uint16_t*, int, int*)
+ *           src/compression/huffman.cu:126-133 */
+int bz2g_count_frequencies(const uint16_t *d_syms, int s, int32_t *d_freqs, void *stream);
+
+/* ------------------------------------------------------ synthetic inputs */
+/* Seeded workload generators (no counterpart in the reference, which has no
+ * data generator): identical bytes on the host and the device.
+ * bz2g_gen_markov: order-1 Markov source over alphabet[0..A) with
+ * Dirichlet(alpha) transition rows and run starts of probability p_run and
+ * length uniform in [run_min, run_max]; definition in
+ * bzip2gpu_b200/csrc/gen.cu.  on_device != 0: out is a device pointer. */
+int bz2g_gen_markov(uint64_t seed, const uint8_t *alphabet, int A, double alpha, double p_run,
+                    int run_min, int run_max, uint8_t *out, int64_t n, int on_device,
+                    void *stream);
+int bz2g_gen_uniform(uint64_t seed, uint8_t *out, int64_t n, int on_device, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,208 @@
+"""GPU parity: every stage through the C-ABI against the oracle, bit-exact,
+on the reference tests' vectors and on the project's workloads; whole
+streams byte-identical to the oracle and decodable by libbz2."""
+import bz2
+
+import numpy as np
+import pytest
+
+import conftest as C
+import oracle
+import bzip2gpu_b200 as B
+import bzip2gpu_b200.workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+# ------------------------------------------------------------------- RLE1
+@pytest.mark.parametrize("R", [20, 3, 10000])
+def test_rle1_reference_vectors(torch_cuda, R):
+    a = C.ref_rle1_input(R)
+    got = B.rle1(dev(torch_cuda, a)).cpu().numpy()
+    assert np.array_equal(got, oracle.rle1(a))
+
+
+@pytest.mark.parametrize("case", ["one", "four", "259", "260", "263", "518", "long", "alt",
+                                  "tile_edge", "markov"])
+def test_rle1_edges(torch_cuda, case):
+    a = {
+        "one": np.array([5], np.uint8),
+        "four": np.full(4, 9, np.uint8),
+        "259": np.full(259, 1, np.uint8),
+        "260": np.full(260, 1, np.uint8),
+        "263": np.full(263, 1, np.uint8),
+        "518": np.full(518, 0, np.uint8),
+        "long": np.concatenate([np.full(900000, 3, np.uint8), [4, 4, 4, 4, 5]]).astype(np.uint8),
+        "alt": np.tile(np.array([1, 2], np.uint8), 50000),
+        "tile_edge": np.concatenate([np.full(4094, 1), np.full(10, 2), np.full(4090, 3)]).astype(np.uint8),
+        "markov": W.small_markov(1 << 20, seed=11),
+    }[case]
+    got = B.rle1(dev(torch_cuda, a)).cpu().numpy()
+    assert np.array_equal(got, oracle.rle1(a))
+
+
+@pytest.mark.parametrize("n", [1, 15, 16, 4095, 4096, 4097, 900000, 1000003])
+def test_crc32(torch_cuda, n):
+    a = B.gen_uniform(n, n)
+    assert B.crc32(dev(torch_cuda, a)) == oracle.crc32(a)
+
+
+# -------------------------------------------------------------------- BWT
+@pytest.mark.parametrize("A", [256, 4, 1])
+def test_bwt_reference_vectors(torch_cuda, A):
+    a = C.ref_bwt_input(A)
+    assert np.array_equal(B.bwt(dev(torch_cuda, a)).cpu().numpy(), oracle.bwt(a))
+
+
+@pytest.mark.parametrize("case", ["m1", "m2", "m7", "m8", "m9", "periodic3", "periodic17_exact",
+                                  "periodic17_seam", "zeros_rle", "markov900k", "uniform"])
+def test_bwt_cases(torch_cuda, case):
+    a = {
+        "m1": np.array([3], np.uint8),
+        "m2": np.array([3, 1], np.uint8),
+        "m7": np.array([1, 2, 1, 2, 1, 2, 1], np.uint8),
+        "m8": np.array([5, 5, 5, 5, 5, 5, 5, 5], np.uint8),
+        "m9": np.array([2, 1, 2, 1, 2, 1, 2, 1, 2], np.uint8),
+        "periodic3": np.tile(np.array([7, 3, 9], np.uint8), 3000),
+        "periodic17_exact": W.periodic17(17 * 5000),
+        "periodic17_seam": W.periodic17(90001),
+        "zeros_rle": oracle.rle1(np.zeros(900000, np.uint8)),
+        "markov900k": oracle.rle1(W.small_markov(900000, seed=3)),
+        "uniform": B.gen_uniform(300000, 5),
+    }[case]
+    got = B.bwt(dev(torch_cuda, a)).cpu().numpy()
+    assert np.array_equal(got, oracle.bwt(a))
+
+
+# -------------------------------------------------------------------- MTF
+@pytest.mark.parametrize("A", [256, 4])
+def test_mtf_reference_vectors(torch_cuda, A):
+    a = C.ref_mtf_input(A)
+    sa = ((np.arange(a.size) + 1) % a.size).astype(np.int32)
+    got, op, pres, nu = B.mtf(dev(torch_cuda, a), dev(torch_cuda, sa))
+    ref, op2, pres2, nu2 = oracle.mtf(a, sa)
+    assert np.array_equal(got.cpu().numpy(), ref)
+    assert (op, nu) == (op2, nu2) and np.array_equal(pres, pres2)
+
+
+def test_mtf_real_sa_and_symbols_table(torch_cuda):
+    r1 = oracle.rle1(W.small_markov(900000, seed=5))
+    sa = oracle.bwt(r1)
+    got, op, pres, nu = B.mtf(dev(torch_cuda, r1), dev(torch_cuda, sa))
+    ref, op2, pres2, nu2 = oracle.mtf(r1, sa)
+    assert np.array_equal(got.cpu().numpy(), ref) and (op, nu) == (op2, nu2)
+    assert np.array_equal(B.symbols_table(dev(torch_cuda, r1)), oracle.symbols_table(r1))
+
+
+def test_symbols_table_reference_vector(torch_cuda):
+    # tests/compression/fmtf.cu:21-46 of the reference
+    C.srand(2137)
+    tbl = [i for i in range(256) if C.glibc_rand(1)[0] % 3 == 0]
+    idx = C.glibc_rand(100000) % len(tbl)
+    data = np.array(tbl, np.uint8)[idx]
+    assert list(B.symbols_table(dev(torch_cuda, data))) == tbl
+
+
+# ------------------------------------------------------------------- RLE2
+@pytest.mark.parametrize("case", ["R20", "R10000", "incompressible", "zeros", "single_zero",
+                                  "one_nonzero", "tile_runs"])
+def test_rle2(torch_cuda, case):
+    a = {
+        "R20": C.ref_rle2_input(20),
+        "R10000": C.ref_rle2_input(10000),
+        "incompressible": C.ref_rle2_incompressible(),
+        "zeros": np.zeros(1000000, np.uint8),
+        "single_zero": np.array([0], np.uint8),
+        "one_nonzero": np.array([4], np.uint8),
+        "tile_runs": np.concatenate([np.zeros(4095), [1], np.zeros(8193), [2, 0, 0]]).astype(np.uint8),
+    }[case]
+    ts = C.table_size(a)
+    got = B.rle2(dev(torch_cuda, a), ts).cpu().numpy().view(np.uint16)
+    assert np.array_equal(got, oracle.rle2(a, ts))
+
+
+# ---------------------------------------------------------------- Huffman
+def _huff_cases():
+    r1 = oracle.rle1(W.small_markov(900000, seed=9))
+    mt, _, _, nu = oracle.mtf(r1, oracle.bwt(r1))
+    small = oracle.rle2(np.array([1, 0, 0, 2, 3, 0, 1], np.uint8), 4)
+    return {
+        "reference_vector": (C.ref_huffman_input(), 15),
+        "markov_block": (oracle.rle2(mt, nu), nu),
+        "tiny": (small, 4),
+        "s199": (C.ref_huffman_input(199, 15), 15),
+        "s600": (C.ref_huffman_input(600, 15), 15),
+    }
+
+
+@pytest.mark.parametrize("case", ["reference_vector", "markov_block", "tiny", "s199", "s600"])
+def test_huffman_build_and_encode(torch_cuda, case):
+    syms, nu = _huff_cases()[case]
+    d = dev(torch_cuda, syms.astype(np.int16))
+    ln, code, sel, ng = B.huffman_build(d, nu)
+    ln2, code2, sel2, ng2 = oracle.huffman_build(syms, nu)
+    alpha = nu + 2
+    assert ng == ng2
+    assert np.array_equal(sel, sel2)
+    assert np.array_equal(ln[:, :alpha], ln2[:, :alpha])
+    assert np.array_equal(code[:ng, :alpha], code2[:ng, :alpha])
+    words, bits = B.huffman_encode(d, ln, code, dev(torch_cuda, sel), ng)
+    w2, b2 = oracle.encode(syms, sel2, ln2, code2)
+    assert bits == b2 and np.array_equal(words, w2)
+
+
+def test_count_frequencies(torch_cuda):
+    # tests/compression/huffman.cu:9-37 of the reference
+    C.srand(2137)
+    data = (C.glibc_rand(10000) % 300 % 258).astype(np.uint16)
+    f = B.count_frequencies(dev(torch_cuda, data.astype(np.int16)))
+    assert np.array_equal(f, np.bincount(data, minlength=258))
+
+
+# ----------------------------------------------------------- whole stream
+def _stream_case(name):
+    return {
+        "empty": (np.zeros(0, np.uint8), 9, 900000),
+        "one": (np.array([65], np.uint8), 9, 900000),
+        "hello_l1": (np.frombuffer(b"hello world!\n", np.uint8), 1, 900000),
+        "exact_block": (W.small_markov(900000, seed=21), 9, 900000),
+        "two_blocks_exact": (W.small_markov(1800000, seed=22), 9, 900000),
+        "block_plus_one": (W.small_markov(900001, seed=23), 9, 900000),
+        "zeros": (np.zeros(2700000, np.uint8), 9, 900000),
+        "uniform": (B.gen_uniform(1000000, 24), 5, 900000),
+        "periodic17": (W.periodic17(1000000), 9, 900000),
+        "small_blocks": (W.small_markov(200000, seed=25), 3, 1000),
+        "odd_blocks": (W.small_markov(500000, seed=26), 9, 99999),
+    }[name]
+
+
+@pytest.mark.parametrize("name", ["empty", "one", "hello_l1", "exact_block", "two_blocks_exact",
+                                  "block_plus_one", "zeros", "uniform", "periodic17",
+                                  "small_blocks", "odd_blocks"])
+def test_stream_matches_oracle(torch_cuda, name):
+    a, level, bb = _stream_case(name)
+    got = B.compress(a, level, bb)
+    ref = oracle.compress(a, level, bb, threads=8)
+    assert got == ref
+    assert bz2.decompress(got) == a.tobytes()
+
+
+def test_config0_stream_bit_exact(torch_cuda):
+    a = W.small_markov()
+    got = B.compress(a, 9)
+    assert got == oracle.compress(a, 9, threads=8)
+    assert bz2.decompress(got) == a.tobytes()
+    dgot = B.compress_device(dev(torch_cuda, a), 9)
+    assert dgot == got
+
+
+def test_levels_set_header_digit_only(torch_cuda):
+    a = W.small_markov(300000, seed=31)
+    base = B.compress(a, 9)
+    for lvl in range(1, 10):
+        s = B.compress(a, lvl)
+        assert s[:4] == b"BZh" + bytes([48 + lvl]) and s[4:] == base[4:]

@@ -1,0 +1,110 @@
+"""Oracle properties: streams decode with libbz2 (the round-trip decoder),
+Huffman tables are valid prefix codes, and the reference's documented edge
+behaviour (empty stream, 259-runs, block CRC position)."""
+import bz2
+
+import numpy as np
+import pytest
+
+import conftest as C
+import oracle
+import bzip2gpu_b200.workloads as W
+
+
+def test_empty_stream_is_14_bytes():
+    # tests/compression/compress.cu:28-50 of the reference (commented-out expectation)
+    s = oracle.compress(b"", 9)
+    assert s == b"BZh9" + bytes.fromhex("177245385090") + b"\0\0\0\0"
+    assert bz2.decompress(s) == b""
+
+
+def test_single_block_header_and_crc():
+    data = b"hello world!\n"
+    s = oracle.compress(data, 1)
+    assert s[:4] == b"BZh1" and s[4:10] == bytes.fromhex("314159265359")
+    assert int.from_bytes(s[10:14], "big") == oracle.crc32(data)
+    assert bz2.decompress(s) == data
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 258, 259, 260, 263, 518, 1000, 5000])
+def test_runs_round_trip(n):
+    data = b"a" * n + b"b" + b"a" * (n // 2)
+    assert bz2.decompress(oracle.compress(data)) == data
+
+
+def test_259_runs_decode():
+    data = b"\x07" * 259 * 3 + b"\x07" * 4
+    r = oracle.rle1(np.frombuffer(data, np.uint8))
+    assert list(r[:5]) == [7, 7, 7, 7, 255]
+    assert bz2.decompress(oracle.compress(data)) == data
+
+
+def test_config0_round_trip_and_multiblock():
+    a = W.small_markov()
+    s = oracle.compress(a, 9, 900000, threads=4)
+    assert bz2.decompress(s) == a.tobytes()
+    bits = np.unpackbits(np.frombuffer(s, np.uint8))
+    magic = np.unpackbits(np.frombuffer(bytes.fromhex("314159265359"), np.uint8))
+    win = np.lib.stride_tricks.sliding_window_view(bits, 48)
+    assert int((win == magic).all(axis=1).sum()) == 5
+
+
+def test_multithreaded_equals_single():
+    a = W.small_markov(2 << 20, seed=7)
+    assert oracle.compress(a, 9, 300000, threads=1) == oracle.compress(a, 9, 300000, threads=8)
+
+
+def _decode(words, bits, sel, ln, code, alpha, n):
+    tabs = []
+    for t in range(6):
+        d = {}
+        for v in range(alpha):
+            d[(int(ln[t][v]), int(code[t][v]))] = v
+        tabs.append(d)
+    out = []
+    pos = 0
+    stream = np.unpackbits(words.astype(">u4").view(np.uint8))
+    while pos < bits:
+        t = sel[len(out) // 50]
+        c = 0
+        for L in range(1, 21):
+            c = (c << 1) | int(stream[pos + L - 1])
+            if (L, c) in tabs[t]:
+                out.append(tabs[t][(L, c)])
+                pos += L
+                break
+        else:
+            raise AssertionError("undecodable")
+    assert len(out) == n
+    return np.array(out, np.uint16)
+
+
+def test_huffman_round_trip_reference_vector():
+    # tests/compression/huffman.cu:161-225 of the reference: build, encode, decode
+    syms = C.ref_huffman_input()
+    ln, code, sel, ng = oracle.huffman_build(syms, 15)
+    assert ng == 6 and sel.size == 200 and sel.max() < 6
+    words, bits = oracle.encode(syms, sel, ln, code)
+    assert np.array_equal(_decode(words, bits, sel, ln, code, 17, syms.size), syms)
+    for t in range(ng):
+        kraft = sum(2.0 ** -int(l) for l in ln[t][:17])
+        assert abs(kraft - 1.0) < 1e-9 and ln[t][:17].max() <= 17
+
+
+def test_code_lengths_limit_17():
+    # Fibonacci-like frequencies force depth > 17 before the rescaling pass
+    f = np.zeros(258, np.int32)
+    a, b = 1, 1
+    for i in range(30):
+        f[i] = a
+        a, b = b, a + b
+    ln = oracle.code_lengths(f, 30, 17)
+    assert ln.max() <= 17
+    assert abs(sum(2.0 ** -int(x) for x in ln) - 1.0) < 1e-9
+
+
+def test_stress_segments_round_trip():
+    a = np.concatenate([np.zeros(300000, np.uint8), W.periodic17(300000),
+                        np.frombuffer(bz2.compress(b"x" * 1000), np.uint8)])
+    s = oracle.compress(a, 9, 900000)
+    assert bz2.decompress(s) == a.tobytes()
