@@ -108,3 +108,20 @@ def test_stress_segments_round_trip():
                         np.frombuffer(bz2.compress(b"x" * 1000), np.uint8)])
     s = oracle.compress(a, 9, 900000)
     assert bz2.decompress(s) == a.tobytes()
+
+
+def test_reference_format_limits_rejected_by_libbz2():
+    """The reference's two known format deviations, pinned: (1) a 900k raw
+    block whose RLE1 output exceeds 900,000 bytes (runs of exactly 4 grow to
+    5 bytes) and (2) a 900k block under a header digit below 9 are emitted
+    bit-exactly by the reference path and rejected by libbz2."""
+    a = np.frombuffer(b"aaaab" * 180000, np.uint8)
+    assert oracle.rle1(a).size == 1080000
+    with pytest.raises(OSError):
+        bz2.decompress(oracle.compress(a, 9))
+    b = np.frombuffer(b"ab" * 300000, np.uint8)
+    for lvl in (1, 5):
+        with pytest.raises(OSError):
+            bz2.decompress(oracle.compress(b, lvl))
+    for lvl in (6, 9):
+        assert bz2.decompress(oracle.compress(b, lvl)) == b.tobytes()
