@@ -143,6 +143,10 @@ void compress_any(const uint8_t *in, size_t n, int level, int block_bytes, bool 
 }
 
 }  // namespace
+
+// Lets other translation units report through bz2g_last_error().
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+
 }  // namespace bz2g
 
 using namespace bz2g;

@@ -85,6 +85,20 @@ size_t bz2g_rle1_bound(size_t n);
  *           include/compression.h:17-18, src/compression/rle1.cu:60-113 */
 int bz2g_rle1(const uint8_t *d_in, int n, uint8_t *d_out, int *m, void *stream);
 
+/* Same result as bz2g_rle1, allocating nothing: no counterpart in the
+ * reference.  For callers that may not allocate device memory while they run
+ * (a service that reserves its whole memory budget at start-up, or a hot path
+ * that must not take cudaMalloc / cudaFree's implicit synchronisation).  Its
+ * scratch is one static device array in the library (about 1 MiB, held by
+ * every GPU that loads the library until the process exits), so n is at
+ * most 1048576 bytes (BZ2G_ERR_TOO_LARGE beyond, with a message in
+ * bz2g_last_error).  d_out holds bz2g_rle1_bound(n) bytes.  The first call on
+ * a device looks up the array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  Calls share the array: calls
+ * that overlap on the GPU (for example on two streams) race, so serialise
+ * them. */
+int bz2g_rle1_noalloc(const uint8_t *d_in, int n, uint8_t *d_out, int *m, void *stream);
+
 /* bzip2 block CRC of n device bytes.
  * Replaces: uint32_t bzip2_crc32(const uint8_t*, size_t)
  *           src/compression/crc32.h:7-8, src/compression/crc32.cpp:22-29 */
