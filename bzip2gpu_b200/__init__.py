@@ -20,7 +20,7 @@ import numpy as np
 
 __all__ = [
     "Bz2gError", "lib", "lib_path", "compress", "compress_device", "compress_bound",
-    "set_engine", "rle1", "crc32", "bwt", "mtf", "symbols_table", "rle2", "huffman_build",
+    "set_engine", "compress_into", "compress_device_into", "rle1", "crc32", "bwt", "mtf", "symbols_table", "rle2", "huffman_build",
     "huffman_encode", "count_frequencies", "gen_markov", "gen_uniform", "MAX_GROUPS",
     "MAX_ALPHA",
 ]
@@ -39,6 +39,7 @@ _SIGS = {
     "bz2g_compress": (_i, [_vp, _sz, _i, _i, _c.POINTER(_u8p), _c.POINTER(_sz)]),
     "bz2g_compress_device": (_i, [_vp, _sz, _i, _i, _c.POINTER(_u8p), _c.POINTER(_sz)]),
     "bz2g_compress_into": (_i, [_vp, _sz, _i, _i, _vp, _sz, _c.POINTER(_sz)]),
+    "bz2g_compress_device_into": (_i, [_vp, _sz, _i, _i, _vp, _sz, _c.POINTER(_sz)]),
     "bz2g_compress_bound": (_sz, [_sz, _i]),
     "bz2g_free": (None, [_vp]),
     "bz2g_set_engine": (_i, [_i, _i]),
@@ -127,6 +128,38 @@ def compress(data, level: int = 9, block_bytes: int = 900000) -> bytes:
         lib().bz2g_free(out)
 
 
+def compress_into(data, out, level: int = 9, block_bytes: int = 900000) -> int:
+    """Whole .bz2 stream of host bytes written into `out` (a host buffer: numpy
+    array or CPU tensor; page-locked memory receives the device copies
+    directly).  Returns the stream length; raises if `out` is too small."""
+    if hasattr(data, "data_ptr") and not getattr(data, "is_cuda", False):
+        ptr, n = data.data_ptr(), data.numel()
+    else:
+        keep, ptr = _host_view(data)
+        n = keep.size
+    if hasattr(out, "data_ptr"):
+        optr, cap = out.data_ptr(), out.numel() * out.element_size()
+    else:
+        optr, cap = out.ctypes.data, out.nbytes
+    ln = _sz()
+    _check(lib().bz2g_compress_into(ptr if n else None, n, level, block_bytes, optr, cap,
+                                    ctypes.byref(ln)))
+    return ln.value
+
+
+def compress_device_into(d_in, out, level: int = 9, block_bytes: int = 900000) -> int:
+    """Whole .bz2 stream of a CUDA uint8 tensor written into host buffer `out`."""
+    if hasattr(out, "data_ptr"):
+        optr, cap = out.data_ptr(), out.numel() * out.element_size()
+    else:
+        optr, cap = out.ctypes.data, out.nbytes
+    ln = _sz()
+    n = d_in.numel()
+    _check(lib().bz2g_compress_device_into(_ptr(d_in) if n else None, n, level, block_bytes,
+                                           optr, cap, ctypes.byref(ln)))
+    return ln.value
+
+
 def compress_device(d_in, level: int = 9, block_bytes: int = 900000) -> bytes:
     """Whole .bz2 stream of a CUDA uint8 tensor."""
     out = _u8p()
@@ -153,7 +186,8 @@ def set_timing(on: bool) -> None:
 
 
 STAT_FIELDS = ("blocks", "n", "m", "A", "s", "g", "bits", "ms_rle1", "ms_bwt", "ms_mtf",
-               "ms_rle2", "ms_huffman", "ms_sizes", "ms_place")
+               "ms_rle2", "ms_huffman", "ms_sizes", "ms_place", "scatter_launches",
+               "scatter_ms", "scatter_bytes")
 
 
 def last_stats() -> dict:

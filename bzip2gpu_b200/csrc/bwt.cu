@@ -5,17 +5,23 @@
 //
 // Here:
 //   1. One segmented LSD radix sort (segments = blocks) of every rotation by
-//      its first 8 bytes (cyclic, big-endian 64-bit key), index as value.
-//      The sort is stable from index order, so ties are index-ascending.
-//   2. Ranks are group heads: head(j) = first sorted position of j's group.
-//      ISA[i] = head of rotation i, HEAD[j] = head of sorted position j.
-//   3. Round with shift h (prefix length h -> 2h): each position j of a block
-//      still sorting gets key (HEAD[j] << kb) | ISA[(SA[j] + h) mod m]
-//      (0 for singletons) and is re-sorted stably within its block.
-//   4. A block stops when every group is a singleton, when a round splits no
-//      group (the rest are equal rotations, already index-ascending), or when
-//      the prefix length reaches m.
-// Block-local ranks fit kb = ceil(log2(max m + 1)) bits, so keys are 2*kb bits.
+//      its first P bytes (cyclic, big-endian), stable from index order, so
+//      ties are index-ascending.
+//   2. Ranks are group heads: head = first SA position of the group;
+//      ISA[i] = head of rotation i.  Rotations in groups of size 1 are final.
+//   3. The rotations still in groups of size >= 2 ("active") are compacted,
+//      per block, with their SA position.  Round with shift h (prefix length
+//      h -> 2h) keys them (head << kb) | ISA[(i + h) mod m] and re-sorts them
+//      stably; the k-th of them in sorted order goes to the k-th active SA
+//      position (groups are contiguous, so this sorts within each group).
+//   4. A block stops when no rotation is active, when a round splits no group
+//      (the rest are equal rotations, already index-ascending), or when the
+//      prefix length reaches m.
+// Block-local ranks fit kb = ceil(log2(max m + 1)) bits.  When 3*kb <= 64
+// (m < 2^21, every bzip2 block) key and rotation share one 64-bit item and
+// the sort moves items only: the first sort keys the first P = 4 bytes
+// (item = prefix << 32 | i), rounds use item = head << 2kb | rank << kb | i.
+// Larger m keeps separate 64-bit keys and 32-bit rotations, with P = 8.
 #include <algorithm>
 
 #include "engine.h"
@@ -29,6 +35,17 @@ constexpr int kRadix = 1 << kRadixBits;
 constexpr int kSortWarps = kTileThreads / 32;  // 8
 constexpr size_t kScatterSmem =
     (size_t)kTile * 8 + (size_t)kTile * 4 + (size_t)kSortWarps * kRadix * 4 + 2 * kRadix * 4;
+
+// How a sorted element is stored: packed (one item: key << low | rotation)
+// or as separate keys[] and vals[].
+struct Layout {
+  int packed;
+  int low;
+};
+
+__device__ __forceinline__ uint64_t key_of(const Layout L, uint64_t item) {
+  return L.packed ? item >> L.low : item;
+}
 
 __device__ __forceinline__ int tile_valid(const SlabDev &d, int t, const int32_t *lens, int *b_out,
                                           int *lt_out) {
@@ -82,11 +99,14 @@ __global__ void __launch_bounds__(256) k_radix_scan(SlabDev d) {
 // (lane l, item i <-> element w*512 + i*32 + l) so that ranking item by item
 // with __match_any_sync keeps the original order; the tile is sorted locally
 // in shared memory, then written so that equal digits go out contiguously.
-__global__ void __launch_bounds__(256) k_radix_scatter(SlabDev d, int shift) {
+__global__ void __launch_bounds__(256) k_radix_scatter(SlabDev d, int shift, int has_vals,
+                                                       int timed) {
   if (!d.sort_ctl[1]) return;
   int b, lt;
   int valid = tile_valid(d, blockIdx.x, d.sort_len, &b, &lt);
   if (valid == 0) return;
+  if (timed >= 0 && threadIdx.x == 0)
+    atomicAdd((unsigned long long *)&d.kt_elems[timed], (unsigned long long)valid);
   extern __shared__ __align__(16) uint8_t smem[];
   uint64_t *sk = reinterpret_cast<uint64_t *>(smem);
   uint32_t *sv = reinterpret_cast<uint32_t *>(sk + kTile);
@@ -97,6 +117,11 @@ __global__ void __launch_bounds__(256) k_radix_scatter(SlabDev d, int shift) {
   const uint64_t *K = d.keys[cur] + d.off[b] + lt;
   const uint32_t *V = d.vals[cur] + d.off[b] + lt;
   const int w = warp_id(), ln = lane_id();
+  if (!has_vals) {  // keys only: the value array area holds the counters
+    wcnt = reinterpret_cast<uint32_t *>(sk + kTile);
+    lbase = wcnt + kSortWarps * kRadix;
+    goff = lbase + kRadix;
+  }
   for (int i = threadIdx.x; i < kSortWarps * kRadix; i += blockDim.x) wcnt[i] = 0;
   goff[threadIdx.x] = d.tile_hist[(size_t)blockIdx.x * kRadix + threadIdx.x];
   __syncthreads();
@@ -110,7 +135,7 @@ __global__ void __launch_bounds__(256) k_radix_scatter(SlabDev d, int shift) {
     int e = w * 512 + i * 32 + ln;
     bool ok = e < valid;
     key[i] = ok ? K[e] : 0;
-    val[i] = ok ? V[e] : 0;
+    val[i] = ok && has_vals ? V[e] : 0;
     int dg = ok ? (int)((key[i] >> shift) & (kRadix - 1)) : kRadix + 1;
     unsigned peers = __match_any_sync(0xffffffffu, dg);
     uint32_t before = ok ? wcnt[w * kRadix + dg] : 0;
@@ -142,7 +167,7 @@ __global__ void __launch_bounds__(256) k_radix_scatter(SlabDev d, int shift) {
       int dg = (int)((key[i] >> shift) & (kRadix - 1));
       uint32_t pos = lbase[dg] + wcnt[w * kRadix + dg] + rank[i];
       sk[pos] = key[i];
-      sv[pos] = val[i];
+      if (has_vals) sv[pos] = val[i];
     }
   }
   __syncthreads();
@@ -153,7 +178,7 @@ __global__ void __launch_bounds__(256) k_radix_scatter(SlabDev d, int shift) {
     int dg = (int)((kk >> shift) & (kRadix - 1));
     uint32_t g = goff[dg] + (uint32_t)k - lbase[dg];
     KO[g] = kk;
-    VO[g] = sv[k];
+    if (has_vals) VO[g] = sv[k];
   }
 }
 
@@ -162,14 +187,24 @@ __global__ void k_radix_flip(SlabDev d) {
   d.sort_ctl[1] = 0;
 }
 
-void radix_sort(const SlabDev &d, int nbits, cudaStream_t st) {
-  for (int shift = 0; shift < nbits; shift += kRadixBits) {
+// Stable sort of each block's elements by key bits [lo, hi).
+void radix_sort(const SlabDev &d, int lo, int hi, int has_vals, cudaStream_t st) {
+  const size_t smem = has_vals ? kScatterSmem : (size_t)kTile * 8 + (size_t)kSortWarps * kRadix * 4 +
+                                                    2 * kRadix * 4;
+  for (int shift = lo; shift < hi; shift += kRadixBits) {
     k_radix_hist<<<d.ntiles, 256, 0, st>>>(d, shift);
     BZ_LAUNCH_CHECK();
     k_radix_scan<<<d.nblocks, 256, 0, st>>>(d);
     BZ_LAUNCH_CHECK();
-    k_radix_scatter<<<d.ntiles, 256, kScatterSmem, st>>>(d, shift);
+    int timed = -1;
+    if (d.kt_on && *d.kt_n < kMaxTimedLaunches) {
+      timed = (*d.kt_n)++;
+      d.kt_bpe[timed] = has_vals ? 24 : 16;
+      BZ_CUDA(cudaEventRecord(d.kt_ev[2 * timed], st));
+    }
+    k_radix_scatter<<<d.ntiles, 256, smem, st>>>(d, shift, has_vals, timed);
     BZ_LAUNCH_CHECK();
+    if (timed >= 0) BZ_CUDA(cudaEventRecord(d.kt_ev[2 * timed + 1], st));
     k_radix_flip<<<1, 1, 0, st>>>(d);
     BZ_LAUNCH_CHECK();
   }
@@ -182,20 +217,24 @@ __global__ void k_bwt_init(SlabDev d) {
     d.sort_ctl[0] = 0;
     d.sort_ctl[1] = 0;
     d.sort_ctl[2] = 0;
+    d.sort_ctl[3] = 0;
   }
   if (b >= d.nblocks) return;
   int m = d.m[b];
   d.sort_len[b] = m > 1 ? m : 0;
   d.done[b] = m > 1 ? 0 : 1;
   d.ngroups[b] = -1;
+  d.act_len[b] = 0;
   d.active_sum[b] = 0;
   for (int k = 0; k < 8; k++) d.pstat[b * 8 + k] = 0;
   if (m == 1) d.sa[d.off[b]] = 0;
 }
 
-// Group heads and singletons of the prefix-1, -2, -4 and -8 partitions, read
-// off the 8-byte sorted keys (pstat[b*8 + q] heads, [b*8 + 4 + q] singletons).
-__global__ void __launch_bounds__(256) k_bwt_prefix_stats(SlabDev d) {
+// Group heads and singletons of the prefix-1, -2, -4 (and -8) partitions,
+// read off the first sort's keys (key_bits = 32 packed, 64 otherwise):
+// pstat[b*8 + q] heads, pstat[b*8 + 4 + q] singletons of prefix 2^q bytes.
+__global__ void __launch_bounds__(256) k_bwt_prefix_stats(SlabDev d, Layout L, int key_bits,
+                                                          int nq) {
   int b, lt;
   int valid = tile_valid(d, blockIdx.x, d.sort_len, &b, &lt);
   if (valid == 0) return;
@@ -204,17 +243,19 @@ __global__ void __launch_bounds__(256) k_bwt_prefix_stats(SlabDev d) {
   int cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   for (int e = threadIdx.x; e < valid; e += blockDim.x) {
     const int j = lt + e;
-    const uint64_t k = K[j];
-    const uint64_t kp = j > 0 ? K[j - 1] : 0;
-    const uint64_t kn = j + 1 < m ? K[j + 1] : 0;
+    const uint64_t k = key_of(L, K[j]);
+    const uint64_t kp = j > 0 ? key_of(L, K[j - 1]) : 0;
+    const uint64_t kn = j + 1 < m ? key_of(L, K[j + 1]) : 0;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-      const int sh = 64 - 8 * (1 << q);
-      const uint64_t a = sh > 0 ? k >> sh : k;
-      const bool hd = j == 0 || a != (sh > 0 ? kp >> sh : kp);
-      const bool tl = j + 1 == m || a != (sh > 0 ? kn >> sh : kn);
-      cnt[q] += hd;
-      cnt[4 + q] += hd && tl;
+      if (q < nq) {
+        const int sh = key_bits - 8 * (1 << q);
+        const uint64_t a = sh > 0 ? k >> sh : k;
+        const bool hd = j == 0 || a != (sh > 0 ? kp >> sh : kp);
+        const bool tl = j + 1 == m || a != (sh > 0 ? kn >> sh : kn);
+        cnt[q] += hd;
+        cnt[4 + q] += hd && tl;
+      }
     }
   }
 #pragma unroll
@@ -225,10 +266,11 @@ __global__ void __launch_bounds__(256) k_bwt_prefix_stats(SlabDev d) {
   }
 }
 
-// The oracle's accounting of rounds h = 1, 2, 4 (round h runs while the
-// partition has a non-singleton group and the previous round split one), and
-// the prefix-4 group count as the fixed-point reference of the first round.
-__global__ void k_bwt_prefix_account(SlabDev d) {
+// The oracle's accounting of the rounds h = 1, 2, (4) that the first sort
+// stands for (round h runs while the partition has a non-singleton group and
+// the previous round split one), and the group count of the prefix before
+// the first sort's as the fixed-point reference of the first ranking.
+__global__ void k_bwt_prefix_account(SlabDev d, int nq) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= d.nblocks) return;
   const int m = d.m[b];
@@ -236,7 +278,7 @@ __global__ void k_bwt_prefix_account(SlabDev d) {
   const int32_t *ps = d.pstat + b * 8;
   int64_t A = 0;
   bool stop = false;
-  for (int q = 0; q < 3 && !stop; q++) {
+  for (int q = 0; q < nq - 1 && !stop; q++) {
     const int G = ps[q], S = ps[4 + q];
     if (G == m) break;
     A += m - S;
@@ -244,11 +286,11 @@ __global__ void k_bwt_prefix_account(SlabDev d) {
     if (ps[q + 1] == G || 2 * h >= m) stop = true;
   }
   d.active_sum[b] = A;
-  d.ngroups[b] = ps[2];
+  d.ngroups[b] = ps[nq - 2];
 }
 
-// Initial keys: the first 8 bytes of each rotation.
-__global__ void __launch_bounds__(256) k_bwt_keys0(SlabDev d) {
+// First keys: the first 4 (packed) or 8 bytes of each rotation.
+__global__ void __launch_bounds__(256) k_bwt_keys0(SlabDev d, int packed) {
   __shared__ uint8_t sb[kTile + 8];
   int b, lt;
   int valid = tile_valid(d, blockIdx.x, d.sort_len, &b, &lt);
@@ -265,56 +307,86 @@ __global__ void __launch_bounds__(256) k_bwt_keys0(SlabDev d) {
   uint32_t *V = d.vals[0] + d.off[b] + lt;
   for (int e = threadIdx.x; e < valid; e += blockDim.x) {
     uint64_t k = 0;
+    if (packed) {
 #pragma unroll
-    for (int q = 0; q < 8; q++) k = (k << 8) | sb[e + q];
-    K[e] = k;
-    V[e] = (uint32_t)(lt + e);
+      for (int q = 0; q < 4; q++) k = (k << 8) | sb[e + q];
+      K[e] = (k << 32) | (uint32_t)(lt + e);
+    } else {
+#pragma unroll
+      for (int q = 0; q < 8; q++) k = (k << 8) | sb[e + q];
+      K[e] = k;
+      V[e] = (uint32_t)(lt + e);
+    }
   }
 }
 
-// Group heads after a sort: per tile, the last head position and head count.
-__global__ void __launch_bounds__(256) k_bwt_rank_tiles(SlabDev d) {
-  __shared__ int red[3][8];
+// ---------------------------------------------------------------- ranking
+// After a sort, the sorted (key, rotation) pairs of a block sit at
+// [off, off + len); element k belongs at SA position P[k] (k itself after the
+// first sort; the k-th active position in later rounds).  A group starts
+// where the key changes; its head is the SA position of its first element.
+// Elements are read warp-striped (warp w owns [512w, 512w + 512), item i of
+// lane l is element 512w + 32i + l) so every load is coalesced.
+constexpr int kWarpSpan = kTile / kSortWarps;  // 512
+
+__device__ __forceinline__ uint64_t key_at(const uint64_t *K, int k) { return K[k]; }
+
+// Per tile: last head (SA position), head count, singleton count, active
+// (non-singleton) count.
+__global__ void __launch_bounds__(256) k_bwt_flags(SlabDev d, Layout L, int initial) {
+  __shared__ int red[4][kSortWarps];
   int b, lt;
-  int valid = tile_valid(d, blockIdx.x, d.sort_len, &b, &lt);
+  const int valid = tile_valid(d, blockIdx.x, d.sort_len, &b, &lt);
   if (valid == 0) return;
-  const uint64_t *K = d.keys[d.sort_ctl[0]] + d.off[b];
-  const int m = d.sort_len[b];
-  int last = -1, cnt = 0, sing = 0;
-  for (int e = threadIdx.x; e < valid; e += blockDim.x) {
-    int j = lt + e;
-    bool hd = j == 0 || K[j] != K[j - 1];
-    if (hd) {
-      last = max(last, j);
-      cnt++;
-      sing += j + 1 == m || K[j + 1] != K[j];
+  const int len = d.sort_len[b];
+  const int64_t off = d.off[b];
+  const uint64_t *K = d.keys[d.sort_ctl[0]] + off;
+  const int32_t *P = d.kpos[d.sort_ctl[3]] + off;
+  const int w = warp_id(), ln = lane_id();
+  int last = -1, heads = 0, sing = 0;
+#pragma unroll 4
+  for (int i = 0; i < kTileItems; i++) {
+    const int e = w * kWarpSpan + i * 32 + ln;
+    if (e < valid) {
+      const int k = lt + e;
+      const uint64_t key = key_of(L, K[k]);
+      const bool hd = k == 0 || key != key_of(L, K[k - 1]);
+      if (hd) {
+        const bool tl = k + 1 == len || key_of(L, K[k + 1]) != key;
+        last = max(last, initial ? k : P[k]);
+        heads++;
+        sing += tl;
+      }
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
     last = max(last, __shfl_xor_sync(0xffffffffu, last, o));
-    cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    heads += __shfl_xor_sync(0xffffffffu, heads, o);
     sing += __shfl_xor_sync(0xffffffffu, sing, o);
   }
-  if (lane_id() == 0) {
-    red[0][warp_id()] = last;
-    red[1][warp_id()] = cnt;
-    red[2][warp_id()] = sing;
+  if (ln == 0) {
+    red[0][w] = last;
+    red[1][w] = heads;
+    red[2][w] = sing;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    int l = -1, c = 0, sg = 0;
-    for (int w = 0; w < 8; w++) {
-      l = max(l, red[0][w]);
-      c += red[1][w];
-      sg += red[2][w];
+    int l = -1, h = 0, sg = 0;
+    for (int q = 0; q < kSortWarps; q++) {
+      l = max(l, red[0][q]);
+      h += red[1][q];
+      sg += red[2][q];
     }
     d.tile_a[blockIdx.x] = l;
-    d.tile_b[blockIdx.x] = c;
+    d.tile_b[blockIdx.x] = h;
     d.tile_c[blockIdx.x] = sg;
+    d.tile_d[blockIdx.x] = valid - sg;  // elements in groups of size >= 2
   }
 }
 
-// Per block: carry of the last head into each tile; group count; stop test.
+// Per block: carry of the last head into each tile, compaction offsets of
+// the active elements, and the stop test: no active element left, no group
+// split by this round (the rest are equal rotations), or prefix >= m.
 __global__ void __launch_bounds__(256) k_bwt_rank_block(SlabDev d, int64_t prefix_len) {
   __shared__ int scratch[40];
   __shared__ int sx[256];
@@ -323,107 +395,169 @@ __global__ void __launch_bounds__(256) k_bwt_rank_block(SlabDev d, int64_t prefi
   if (len <= 0) return;
   const int nt = (len + kTile - 1) / kTile;
   const int t0 = (int)(d.off[b] / kTile);
-  int carry = -1, count = 0, singles = 0;
+  int carry = -1, heads = 0, singles = 0, active = 0;
   for (int base = 0; base < nt; base += 256) {
-    int k = base + threadIdx.x;
-    int v = k < nt ? d.tile_a[t0 + k] : -1;
-    int c = k < nt ? d.tile_b[t0 + k] : 0;
-    int sg = k < nt ? d.tile_c[t0 + k] : 0;
-    int inc = block_incl_max(v, scratch, -1);
+    const int k = base + threadIdx.x;
+    const int v = k < nt ? d.tile_a[t0 + k] : -1;
+    const int h = k < nt ? d.tile_b[t0 + k] : 0;
+    const int sg = k < nt ? d.tile_c[t0 + k] : 0;
+    const int ac = k < nt ? d.tile_d[t0 + k] : 0;
+    const int inc = block_incl_max(v, scratch, -1);
     sx[threadIdx.x] = inc;
     __syncthreads();
-    int ex = threadIdx.x == 0 ? carry : max(carry, sx[threadIdx.x - 1]);
+    const int ex = threadIdx.x == 0 ? carry : max(carry, sx[threadIdx.x - 1]);
     if (k < nt) d.tile_a[t0 + k] = ex;
-    int c2 = max(carry, sx[255]);
+    const int c2 = max(carry, sx[255]);
     __syncthreads();
     carry = c2;
     int tot;
-    block_excl_sum(c, scratch, &tot);
-    count += tot;
+    block_excl_sum(h, scratch, &tot);
+    heads += tot;
     block_excl_sum(sg, scratch, &tot);
     singles += tot;
+    const int ao = block_excl_sum(ac, scratch, &tot);
+    if (k < nt) d.tile_d[t0 + k] = active + ao;
+    active += tot;
   }
   if (threadIdx.x == 0) {
-    int m = d.m[b];
-    bool fin = count == m || count == d.ngroups[b] || prefix_len >= m;
-    d.ngroups[b] = count;
+    const int m = d.m[b];
+    const bool fin = active == 0 || heads == d.ngroups[b] || prefix_len >= m;
+    d.ngroups[b] = heads - singles;  // groups among the rotations still active
     if (fin) {
       d.done[b] = 1;
+      d.act_len[b] = 0;
     } else {
+      d.act_len[b] = active;
       atomicAdd(&d.sort_ctl[2], 1);
-      d.active_sum[b] += m - singles;  // rotations entering the next round
+      d.active_sum[b] += active;  // rotations entering the next round
     }
   }
 }
 
-// Write SA, HEAD and ISA for the sorted positions of each block still sorting.
-__global__ void __launch_bounds__(256) k_bwt_rank_apply(SlabDev d) {
-  __shared__ int scratch[40];
-  __shared__ int wl[8];
+// Write SA and ISA for the sorted elements, and compact the elements of
+// groups of size >= 2 (for blocks still sorting) into the other key/value/
+// position buffers, keyed by their new head (rank of i+h added next round).
+__global__ void __launch_bounds__(256) k_bwt_apply(SlabDev d, Layout L, int initial, int kb) {
+  __shared__ int wlast[kSortWarps];
+  __shared__ int wact[kSortWarps];
   int b, lt;
-  int valid = tile_valid(d, blockIdx.x, d.sort_len, &b, &lt);
+  const int valid = tile_valid(d, blockIdx.x, d.sort_len, &b, &lt);
   if (valid == 0) return;
-  const int cur = d.sort_ctl[0];
+  const int len = d.sort_len[b];
   const int64_t off = d.off[b];
+  const int cur = d.sort_ctl[0], pc = d.sort_ctl[3];
   const uint64_t *K = d.keys[cur] + off;
   const uint32_t *V = d.vals[cur] + off;
-  const int p0 = threadIdx.x * kTileItems;
-  int ls = -1;
-  for (int k = 0; k < kTileItems; k++) {
-    int e = p0 + k;
-    if (e >= valid) break;
-    int j = lt + e;
-    if (j == 0 || K[j] != K[j - 1]) ls = j;
+  const int32_t *P = d.kpos[pc] + off;
+  const bool compact = d.done[b] == 0;
+  const int w = warp_id(), ln = lane_id();
+  // pass 1: per warp, last head and active count
+  int last = -1, act = 0;
+#pragma unroll 4
+  for (int i = 0; i < kTileItems; i++) {
+    const int e = w * kWarpSpan + i * 32 + ln;
+    if (e < valid) {
+      const int k = lt + e;
+      const uint64_t key = key_of(L, K[k]);
+      const bool hd = k == 0 || key != key_of(L, K[k - 1]);
+      const bool tl = k + 1 == len || key_of(L, K[k + 1]) != key;
+      if (hd) last = max(last, initial ? k : P[k]);
+      act += !(hd && tl);
+    }
   }
-  int inc = block_incl_max(ls, scratch, -1);
-  int ex = __shfl_up_sync(0xffffffffu, inc, 1);
-  if (lane_id() == 31) wl[warp_id()] = inc;
+  for (int o = 16; o > 0; o >>= 1) {
+    last = max(last, __shfl_xor_sync(0xffffffffu, last, o));
+    act += __shfl_xor_sync(0xffffffffu, act, o);
+  }
+  if (ln == 0) {
+    wlast[w] = last;
+    wact[w] = act;
+  }
   __syncthreads();
-  if (lane_id() == 0) ex = warp_id() == 0 ? -1 : wl[warp_id() - 1];
-  int cur_head = max(ex, d.tile_a[blockIdx.x]);
-  for (int k = 0; k < kTileItems; k++) {
-    int e = p0 + k;
-    if (e >= valid) break;
-    int j = lt + e;
-    if (j == 0 || K[j] != K[j - 1]) cur_head = j;
-    int i = (int)V[j];
-    d.sa[off + j] = i;
-    d.head[off + j] = cur_head;
-    d.isa[off + i] = cur_head;
+  int carry = d.tile_a[blockIdx.x];
+  int aoff = d.tile_d[blockIdx.x];
+  for (int q = 0; q < w; q++) {
+    carry = max(carry, wlast[q]);
+    aoff += wact[q];
+  }
+  uint64_t *KO = d.keys[cur ^ 1] + off;
+  uint32_t *VO = d.vals[cur ^ 1] + off;
+  int32_t *PO = d.kpos[pc ^ 1] + off;
+  int32_t *SA = d.sa + off;
+  int32_t *IS = d.isa + off;
+  const unsigned lt_mask = (1u << ln) - 1u;
+  // pass 2: heads by a running max, writes, compaction
+#pragma unroll 4
+  for (int i = 0; i < kTileItems; i++) {
+    const int e = w * kWarpSpan + i * 32 + ln;
+    const bool ok = e < valid;
+    int pos = 0, hdpos = -1;
+    uint32_t val = 0;
+    bool active = false;
+    if (ok) {
+      const int k = lt + e;
+      const uint64_t item = K[k];
+      const uint64_t key = key_of(L, item);
+      const bool hd = k == 0 || key != key_of(L, K[k - 1]);
+      const bool tl = k + 1 == len || key_of(L, K[k + 1]) != key;
+      pos = initial ? k : P[k];
+      val = L.packed ? (uint32_t)(item & ((1ull << L.low) - 1)) : V[k];
+      if (hd) hdpos = pos;
+      active = !(hd && tl);
+    }
+    const int head = max(carry, warp_incl_max(hdpos));
+    carry = __shfl_sync(0xffffffffu, head, 31);
+    const unsigned am = __ballot_sync(0xffffffffu, active);
+    if (ok) {
+      SA[pos] = (int32_t)val;
+      IS[val] = head;
+      if (compact && active) {
+        const int r = aoff + __popc(am & lt_mask);
+        if (L.packed) {
+          KO[r] = ((uint64_t)(uint32_t)head << (2 * kb)) | val;
+        } else {
+          KO[r] = (uint64_t)(uint32_t)head << kb;
+          VO[r] = val;
+        }
+        PO[r] = pos;
+      }
+    }
+    aoff += __popc(am);
   }
 }
 
-// Round keys: (HEAD[j] << kb) | ISA[(SA[j] + h) mod m]; singletons get 0.
-__global__ void __launch_bounds__(256) k_bwt_round_keys(SlabDev d, int h, int kb) {
+__global__ void k_bwt_flip(SlabDev d) {
+  d.sort_ctl[0] ^= 1;
+  d.sort_ctl[3] ^= 1;
+}
+
+// Round keys for the compacted active rotations: add the rank of i+h.
+__global__ void __launch_bounds__(256) k_bwt_round_keys(SlabDev d, int h, int packed, int kb) {
   const int t = blockIdx.x;
   const int b = d.tile_block[t];
   const int64_t off = d.off[b];
   const int lt = (int)((int64_t)t * kTile - off);
-  const int m = d.m[b];
-  const bool dn = d.done[b] != 0;
-  if (lt == 0 && threadIdx.x == 0) d.sort_len[b] = dn ? 0 : m;
-  if (dn) return;
-  int valid = min(kTile, m - lt);
+  const int len = d.act_len[b];
+  if (lt == 0 && threadIdx.x == 0) d.sort_len[b] = len;
+  const int valid = min(kTile, len - lt);
   if (valid <= 0) return;
+  const int m = d.m[b];
   const int cur = d.sort_ctl[0];
-  uint64_t *K = d.keys[cur] + off;
-  uint32_t *V = d.vals[cur] + off;
-  const int32_t *SA = d.sa + off;
-  const int32_t *HD = d.head + off;
+  uint64_t *K = d.keys[cur] + off + lt;
+  const uint32_t *V = d.vals[cur] + off + lt;
   const int32_t *IS = d.isa + off;
+  const uint64_t mask = (1ull << kb) - 1;
   for (int e = threadIdx.x; e < valid; e += blockDim.x) {
-    int j = lt + e;
-    int i = SA[j];
-    int hd = HD[j];
-    bool single = hd == j && (j + 1 == m || HD[j + 1] == j + 1);
-    uint32_t k2 = 0;
-    if (!single) {
-      int i2 = i + h;
+    if (packed) {
+      const uint64_t item = K[e];
+      int i2 = (int)(item & mask) + h;
       if (i2 >= m) i2 -= m;
-      k2 = (uint32_t)IS[i2];
+      K[e] = item | ((uint64_t)(uint32_t)IS[i2] << kb);
+    } else {
+      int i2 = (int)V[e] + h;
+      if (i2 >= m) i2 -= m;
+      K[e] |= (uint32_t)IS[i2];
     }
-    K[j] = ((uint64_t)(uint32_t)hd << kb) | k2;
-    V[j] = (uint32_t)i;
   }
 }
 
@@ -439,34 +573,47 @@ void stage_bwt(const SlabDev &d, int max_m, cudaStream_t st) {
   }
   int kb = 1;
   while ((1ll << kb) <= (int64_t)max_m) kb++;
+  const int packed = 3 * kb <= 64;
   k_bwt_init<<<(d.nblocks + 127) / 128, 128, 0, st>>>(d);
   BZ_LAUNCH_CHECK();
   if (max_m <= 1) return;
-  k_bwt_keys0<<<d.ntiles, 256, 0, st>>>(d);
+  k_bwt_keys0<<<d.ntiles, 256, 0, st>>>(d, packed);
   BZ_LAUNCH_CHECK();
-  radix_sort(d, 64, st);
-  k_bwt_prefix_stats<<<d.ntiles, 256, 0, st>>>(d);
+  // first sort: 4-byte prefixes in the high half of packed items, or 8-byte keys
+  const Layout first = {packed, packed ? 32 : 0};
+  const Layout round = {packed, packed ? kb : 0};
+  if (packed)
+    radix_sort(d, 32, 64, 0, st);
+  else
+    radix_sort(d, 0, 64, 1, st);
+  const int nq = packed ? 3 : 4;  // prefixes 1,2,4 (,8) bytes
+  k_bwt_prefix_stats<<<d.ntiles, 256, 0, st>>>(d, first, packed ? 32 : 64, nq);
   BZ_LAUNCH_CHECK();
-  k_bwt_prefix_account<<<(d.nblocks + 127) / 128, 128, 0, st>>>(d);
+  k_bwt_prefix_account<<<(d.nblocks + 127) / 128, 128, 0, st>>>(d, nq);
   BZ_LAUNCH_CHECK();
-  int64_t prefix = 8;
-  for (int round = 0;; round++) {
+  int64_t prefix = packed ? 4 : 8;
+  for (int initial = 1;; initial = 0) {
+    const Layout L = initial ? first : round;
     BZ_CUDA(cudaMemsetAsync(d.sort_ctl + 2, 0, sizeof(int32_t), st));
-    k_bwt_rank_tiles<<<d.ntiles, 256, 0, st>>>(d);
+    k_bwt_flags<<<d.ntiles, 256, 0, st>>>(d, L, initial);
     BZ_LAUNCH_CHECK();
     k_bwt_rank_block<<<d.nblocks, 256, 0, st>>>(d, prefix);
     BZ_LAUNCH_CHECK();
-    k_bwt_rank_apply<<<d.ntiles, 256, 0, st>>>(d);
+    k_bwt_apply<<<d.ntiles, 256, 0, st>>>(d, L, initial, kb);
+    BZ_LAUNCH_CHECK();
+    k_bwt_flip<<<1, 1, 0, st>>>(d);
     BZ_LAUNCH_CHECK();
     if (prefix >= max_m) break;
     BZ_CUDA(cudaMemcpyAsync(d.h_flags, d.sort_ctl + 2, sizeof(int32_t), cudaMemcpyDeviceToHost,
                             st));
     BZ_CUDA(cudaStreamSynchronize(st));
     if (d.h_flags[0] == 0) break;
-    int h = (int)prefix;
-    k_bwt_round_keys<<<d.ntiles, 256, 0, st>>>(d, h, kb);
+    k_bwt_round_keys<<<d.ntiles, 256, 0, st>>>(d, (int)prefix, packed, kb);
     BZ_LAUNCH_CHECK();
-    radix_sort(d, 2 * kb, st);
+    if (packed)
+      radix_sort(d, kb, 3 * kb, 0, st);
+    else
+      radix_sort(d, 0, 2 * kb, 1, st);
     prefix *= 2;
   }
 }

@@ -95,7 +95,7 @@ struct EngineKey {
 };
 std::mutex g_eng_mu;
 std::map<EngineKey, std::unique_ptr<Compressor>> g_engines;
-int g_slab = 32, g_workers = 3;
+int g_slab = 128, g_workers = 3;
 bool g_timing = false;
 thread_local StageTimes g_last_stats;
 
@@ -122,7 +122,7 @@ Compressor &engine_for(int64_t block_bytes) {
 }
 
 void compress_any(const uint8_t *in, size_t n, int level, int block_bytes, bool on_device,
-                  std::vector<uint8_t> &out) {
+                  ByteSink &out) {
   BZ_REQUIRE(block_bytes > 0 && block_bytes <= (1 << 24), kErrArg,
              "block_bytes must be in (0, 16 MiB]");
   BZ_REQUIRE(n == 0 || in != nullptr, kErrArg, "null input");
@@ -161,7 +161,7 @@ size_t bz2g_rle1_bound(size_t n) { return (size_t)rle1_bound((int64_t)n); }
 size_t bz2g_compress_bound(size_t n, int block_bytes) {
   if (block_bytes <= 0) block_bytes = 900000;
   size_t nb = (n + block_bytes - 1) / block_bytes;
-  return 64 + nb * 20000 + (rle1_bound((int64_t)n) + nb * 16) * kMaxCodeLen / 8 + 16;
+  return stream_bound((int64_t)n, (int64_t)nb);
 }
 
 int bz2g_set_engine(int slab_blocks, int workers) {
@@ -177,13 +177,10 @@ int bz2g_compress(const uint8_t *in, size_t n, int level, int block_bytes, uint8
                   size_t *out_len) {
   return guard([&] {
     BZ_REQUIRE(out && out_len, kErrArg, "null output pointer");
-    std::vector<uint8_t> v;
-    compress_any(in, n, level, block_bytes, false, v);
-    uint8_t *p = (uint8_t *)std::malloc(std::max<size_t>(v.size(), 1));
-    BZ_REQUIRE(p, kErrAlloc, "malloc failed");
-    std::memcpy(p, v.data(), v.size());
-    *out = p;
-    *out_len = v.size();
+    ByteSink s;
+    compress_any(in, n, level, block_bytes, false, s);
+    *out_len = s.size;
+    *out = s.release();
   });
 }
 
@@ -191,13 +188,10 @@ int bz2g_compress_device(const uint8_t *d_in, size_t n, int level, int block_byt
                          uint8_t **out, size_t *out_len) {
   return guard([&] {
     BZ_REQUIRE(out && out_len, kErrArg, "null output pointer");
-    std::vector<uint8_t> v;
-    compress_any(d_in, n, level, block_bytes, true, v);
-    uint8_t *p = (uint8_t *)std::malloc(std::max<size_t>(v.size(), 1));
-    BZ_REQUIRE(p, kErrAlloc, "malloc failed");
-    std::memcpy(p, v.data(), v.size());
-    *out = p;
-    *out_len = v.size();
+    ByteSink s;
+    compress_any(d_in, n, level, block_bytes, true, s);
+    *out_len = s.size;
+    *out = s.release();
   });
 }
 
@@ -205,11 +199,19 @@ int bz2g_compress_into(const uint8_t *in, size_t n, int level, int block_bytes, 
                        size_t cap, size_t *out_len) {
   return guard([&] {
     BZ_REQUIRE(out && out_len, kErrArg, "null output pointer");
-    std::vector<uint8_t> v;
-    compress_any(in, n, level, block_bytes, false, v);
-    BZ_REQUIRE(v.size() <= cap, kErrTooLarge, "output buffer too small");
-    std::memcpy(out, v.data(), v.size());
-    *out_len = v.size();
+    ByteSink s(out, cap);
+    compress_any(in, n, level, block_bytes, false, s);
+    *out_len = s.size;
+  });
+}
+
+int bz2g_compress_device_into(const uint8_t *d_in, size_t n, int level, int block_bytes,
+                              uint8_t *out, size_t cap, size_t *out_len) {
+  return guard([&] {
+    BZ_REQUIRE(out && out_len, kErrArg, "null output pointer");
+    ByteSink s(out, cap);
+    compress_any(d_in, n, level, block_bytes, true, s);
+    *out_len = s.size;
   });
 }
 
@@ -223,10 +225,11 @@ int bz2g_set_timing(int on) {
 
 int bz2g_last_stats(double *out, int n) {
   const StageTimes &t = g_last_stats;
-  const double v[] = {(double)t.blocks, (double)t.n, (double)t.m,  (double)t.A,
-                      (double)t.s,      (double)t.g, (double)t.bits, t.rle1,
-                      t.bwt,            t.mtf,       t.rle2,       t.huffman,
-                      t.sizes,          t.place};
+  const double v[] = {(double)t.blocks, (double)t.n,   (double)t.m,  (double)t.A,
+                      (double)t.s,      (double)t.g,   (double)t.bits, t.rle1,
+                      t.bwt,            t.mtf,         t.rle2,       t.huffman,
+                      t.sizes,          t.place,       (double)t.scatter_launches,
+                      t.scatter_ms,     t.scatter_bytes};
   const int k = (int)(sizeof(v) / sizeof(v[0]));
   for (int i = 0; i < n && i < k; i++) out[i] = v[i];
   return k;

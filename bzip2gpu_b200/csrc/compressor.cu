@@ -30,10 +30,17 @@ struct Compressor::Worker {
   int64_t *h_act = nullptr;    // [max_blocks] A
   uint32_t *h_crc = nullptr;
   cudaEvent_t ev[8] = {};
+  cudaEvent_t kt_ev[2 * kMaxTimedLaunches] = {};
+  int kt_n = 0;
+  int kt_bpe[kMaxTimedLaunches] = {};
+  uint64_t *h_kt = nullptr;
   ~Worker() {
     if (st) cudaStreamSynchronize(st);
     for (auto &e : ev)
       if (e) cudaEventDestroy(e);
+    for (auto &e : kt_ev)
+      if (e) cudaEventDestroy(e);
+    if (h_kt) cudaFreeHost(h_kt);
     delete ws;
     if (h_out) cudaFreeHost(h_out);
     if (h_sizes) cudaFreeHost(h_sizes);
@@ -59,50 +66,110 @@ Compressor::Compressor(const CompressorConfig &cfg) : cfg_(cfg) {
     BZ_CUDA(cudaMallocHost((void **)&w->h_cnt, sizeof(int32_t) * 3 * cfg_.slab_blocks));
     BZ_CUDA(cudaMallocHost((void **)&w->h_act, sizeof(int64_t) * cfg_.slab_blocks));
     for (auto &e : w->ev) BZ_CUDA(cudaEventCreate(&e));
+    for (auto &e : w->kt_ev) BZ_CUDA(cudaEventCreate(&e));
+    BZ_CUDA(cudaMallocHost((void **)&w->h_kt, 8 * kMaxTimedLaunches));
+    w->ws->dev.kt_ev = w->kt_ev;
+    w->ws->dev.kt_n = &w->kt_n;
+    w->ws->dev.kt_bpe = w->kt_bpe;
     workers_.push_back(std::move(w));
   }
 }
 
 Compressor::~Compressor() = default;
 
-void append_eos(std::vector<uint8_t> &out, int64_t bit, uint32_t crc) {
-  // 48-bit end-of-stream magic then the 32-bit combined CRC, MSB first
-  // (src/compression/compress.cu:366-375).
+ByteSink::ByteSink(uint8_t *p, size_t c) : data(p), size(0), cap(c), owned(false) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) == cudaSuccess)
+    pinned = a.type == cudaMemoryTypeHost;
+  else
+    cudaGetLastError();
+}
+
+ByteSink::~ByteSink() {
+  if (owned) std::free(data);
+}
+
+void ByteSink::reserve(size_t c) {
+  BZ_REQUIRE(owned || c <= cap, kErrTooLarge, "output buffer too small");
+  if (!owned || c <= cap) return;
+  // large buffers are mapped lazily: untouched pages cost nothing
+  uint8_t *p = (uint8_t *)std::realloc(data, c);
+  BZ_REQUIRE(p, kErrAlloc, "host output allocation failed");
+  data = p;
+  cap = c;
+}
+
+uint8_t *ByteSink::release() {
+  uint8_t *p = data;
+  if (size < cap && size > 0) {
+    uint8_t *q = (uint8_t *)std::realloc(p, size);
+    if (q) p = q;
+  }
+  data = nullptr;
+  size = cap = 0;
+  return p;
+}
+
+size_t stream_bound(int64_t n, int64_t nblocks) {
+  // header <= 20000 bytes per block (selectors <= 6 bits each, tables);
+  // payload <= 17 bits per symbol, symbols <= RLE1 bytes + 1
+  return 64 + (size_t)nblocks * 20000 + (size_t)(rle1_bound(n) + nblocks * 16) * kMaxCodeLen / 8;
+}
+
+namespace {
+// 48-bit end-of-stream magic then the 32-bit combined CRC, MSB first, then
+// padding to a byte (src/compression/compress.cu:366-376).
+void put_eos(ByteSink &out, size_t base, int64_t bit, uint32_t crc) {
   const uint64_t magic = 0x177245385090ull;
   auto put = [&](uint64_t v, int nb) {
     for (int k = nb - 1; k >= 0; k--) {
-      size_t byte = (size_t)(bit >> 3);
-      if (byte >= out.size()) out.push_back(0);
-      if ((v >> k) & 1) out[byte] |= (uint8_t)(0x80u >> (bit & 7));
+      size_t byte = base + (size_t)(bit >> 3);
+      if (byte >= out.size) out.data[out.size++] = 0;
+      if ((v >> k) & 1) out.data[byte] |= (uint8_t)(0x80u >> (bit & 7));
       bit++;
     }
   };
   put(magic, 48);
   put(crc, 32);
 }
+}  // namespace
 
 void Compressor::compress(const uint8_t *const *ptrs, const int *lens, int nblocks, int level,
-                          std::vector<uint8_t> &out, StageTimes *times) {
+                          ByteSink &out, StageTimes *times) {
   run(ptrs, lens, nblocks, level, false, out, times);
 }
 
 void Compressor::compress_device(const uint8_t *const *d_ptrs, const int *lens, int nblocks,
-                                 int level, std::vector<uint8_t> &out, StageTimes *times) {
+                                 int level, ByteSink &out, StageTimes *times) {
   run(d_ptrs, lens, nblocks, level, true, out, times);
 }
 
+void Compressor::compress(const uint8_t *const *ptrs, const int *lens, int nblocks, int level,
+                          std::vector<uint8_t> &out, StageTimes *times) {
+  ByteSink s;
+  compress(ptrs, lens, nblocks, level, s, times);
+  out.insert(out.end(), s.data, s.data + s.size);
+}
+
 void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, int level,
-                     bool on_device, std::vector<uint8_t> &out, StageTimes *times) {
-  for (int b = 0; b < nblocks; b++)
+                     bool on_device, ByteSink &out, StageTimes *times) {
+  int64_t ntot = 0;
+  for (int b = 0; b < nblocks; b++) {
     BZ_REQUIRE(lens[b] > 0 && lens[b] <= cfg_.max_block_bytes, kErrArg,
                "block length outside (0, max_block_bytes]");
+    ntot += lens[b];
+  }
   if (level < 1) level = 1;
   if (level > 9) level = 9;
-  const size_t base = out.size();
-  out.push_back('B');
-  out.push_back('Z');
-  out.push_back('h');
-  out.push_back((uint8_t)('0' + level));
+  const size_t base = out.size;
+  const size_t bound = stream_bound(ntot, nblocks);
+  if (out.owned) out.reserve(base + bound);
+  BZ_REQUIRE(base + 14 <= out.cap, kErrTooLarge, "output buffer too small");
+  out.data[base + 0] = 'B';
+  out.data[base + 1] = 'Z';
+  out.data[base + 2] = 'h';
+  out.data[base + 3] = (uint8_t)('0' + level);
+  out.size = base + 4;
   const int B = cfg_.slab_blocks;
   const int nslabs = (nblocks + B - 1) / B;
 
@@ -143,6 +210,9 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
           BZ_CUDA(cudaMemcpyAsync(d.raw + plan.raw_off[i], ptrs[b0 + i], lens[b0 + i], kind, w.st));
       }
       const bool tm = times != nullptr && cfg_.time_stages;
+      w.ws->dev.kt_on = tm;
+      w.kt_n = 0;
+      if (tm) BZ_CUDA(cudaMemsetAsync(d.kt_elems, 0, 8 * kMaxTimedLaunches, w.st));
       if (tm) BZ_CUDA(cudaEventRecord(w.ev[0], w.st));
       stage_rle1_crc(d, w.st);
       if (tm) BZ_CUDA(cudaEventRecord(w.ev[1], w.st));
@@ -167,6 +237,8 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
         BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 2 * B, d.n_sel, 4 * nb, cudaMemcpyDeviceToHost, w.st));
         BZ_CUDA(cudaMemcpyAsync(w.h_act, d.active_sum, 8 * nb, cudaMemcpyDeviceToHost, w.st));
       }
+      if (tm && w.kt_n > 0)
+        BZ_CUDA(cudaMemcpyAsync(w.h_kt, d.kt_elems, 8 * w.kt_n, cudaMemcpyDeviceToHost, w.st));
       BZ_CUDA(cudaStreamSynchronize(w.st));
       int64_t total = 0;
       for (int i = 0; i < nb; i++) total += w.h_sizes[i] + w.h_sizes[B + i];
@@ -197,11 +269,29 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
       const int64_t w0 = start / 32;
       const int64_t nwords = (end + 31) / 32 - w0;
       BZ_REQUIRE(nwords <= w.ws->out_words, kErrInternal, "slab output exceeds buffer");
+      const size_t at = base + (size_t)(4 * w0);
+      const int64_t nbytes = (end + 7) / 8 - 4 * w0;
+      BZ_REQUIRE(at + (size_t)nbytes + 10 <= out.cap, kErrTooLarge, "output buffer too small");
       stage_place(d, start, w0, nwords, w.st);
       if (tm) BZ_CUDA(cudaEventRecord(w.ev[7], w.st));
-      const int64_t nbytes = (end + 7) / 8 - 4 * w0;
-      BZ_CUDA(cudaMemcpyAsync(w.h_out, d.out, nbytes, cudaMemcpyDeviceToHost, w.st));
-      BZ_CUDA(cudaStreamSynchronize(w.st));
+      // The slab owns its bytes from 4*w0 + 4 on; its first word is shared
+      // with the previous slab's last one and is OR-ed in slab order below.
+      const int64_t head = std::min<int64_t>(4, nbytes);
+      BZ_CUDA(cudaMemcpyAsync(w.h_out, d.out, head, cudaMemcpyDeviceToHost, w.st));
+      if (nbytes > head) {
+        if (out.pinned) {
+          BZ_CUDA(cudaMemcpyAsync(out.data + at + head, (const uint8_t *)d.out + head,
+                                  nbytes - head, cudaMemcpyDeviceToHost, w.st));
+          BZ_CUDA(cudaStreamSynchronize(w.st));
+        } else {
+          BZ_CUDA(cudaMemcpyAsync(w.h_out + head, (const uint8_t *)d.out + head, nbytes - head,
+                                  cudaMemcpyDeviceToHost, w.st));
+          BZ_CUDA(cudaStreamSynchronize(w.st));
+          std::memcpy(out.data + at + head, w.h_out + head, nbytes - head);
+        }
+      } else {
+        BZ_CUDA(cudaStreamSynchronize(w.st));
+      }
       if (tm) {
         float ms[7];
         for (int q = 0; q < 6; q++) BZ_CUDA(cudaEventElapsedTime(&ms[q], w.ev[q], w.ev[q + 1]));
@@ -214,16 +304,25 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
         tsum.huffman += ms[4];
         tsum.sizes += ms[5];
         tsum.place += ms[6];
+        for (int q = 0; q < w.kt_n; q++) {
+          if (w.h_kt[q] == 0) continue;  // skipped pass (one digit value only)
+          float t = 0;
+          BZ_CUDA(cudaEventElapsedTime(&t, w.kt_ev[2 * q], w.kt_ev[2 * q + 1]));
+          tsum.scatter_launches++;
+          tsum.scatter_ms += t;
+          tsum.scatter_bytes += (double)w.h_kt[q] * w.kt_bpe[q];
+        }
       }
       {
         std::unique_lock<std::mutex> g(mu);
         cv.wait(g, [&] { return next_append == k || err; });
         if (err) return;
-        const size_t at = base + (size_t)(4 * w0);
-        size_t ov = out.size() > at ? out.size() - at : 0;
-        ov = std::min<size_t>(ov, (size_t)nbytes);
-        for (size_t i = 0; i < ov; i++) out[at + i] |= w.h_out[i];
-        out.insert(out.end(), w.h_out + ov, w.h_out + nbytes);
+        // bytes [at, out.size) hold the previous slab's tail (<= 4 bytes)
+        for (int64_t i = 0; i < head; i++) {
+          if (at + i < out.size) out.data[at + i] |= w.h_out[i];
+          else out.data[at + i] = w.h_out[i];
+        }
+        out.size = at + (size_t)nbytes;
         next_append++;
         cv.notify_all();
       }
@@ -245,19 +344,10 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
   if (nw >= 1) guarded(*workers_[0]);
   for (auto &t : th) t.join();
   if (err) {
-    out.resize(base);
+    out.size = base;
     std::rethrow_exception(err);
   }
-  // the stream's byte vector relative to `base`
-  std::vector<uint8_t> tail;
-  if (base == 0) {
-    append_eos(out, bit, stream_crc);
-  } else {
-    tail.assign(out.begin() + base, out.end());
-    append_eos(tail, bit, stream_crc);
-    out.resize(base);
-    out.insert(out.end(), tail.begin(), tail.end());
-  }
+  put_eos(out, base, bit, stream_crc);
   if (times) *times = tsum;
 }
 

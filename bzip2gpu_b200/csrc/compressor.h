@@ -19,13 +19,33 @@ struct StageTimes {
   // totals over all blocks, for the HBM byte model
   // B = n + 10m + 28A + 14s + 5g + bits/8
   int64_t blocks = 0, n = 0, m = 0, A = 0, s = 0, g = 0, bits = 0;
+  // radix scatter launches (when timing is enabled): count, summed device
+  // ms, and algorithmic bytes (each element's item read and written once)
+  int64_t scatter_launches = 0;
+  double scatter_ms = 0, scatter_bytes = 0;
 };
 
 struct CompressorConfig {
-  int slab_blocks = 32;
+  int slab_blocks = 128;
   int workers = 3;
   int64_t max_block_bytes = 900000;
   bool time_stages = false;
+};
+
+// Destination of a stream: a malloc'd buffer that this library grows (and
+// the caller may take over and free()), or a caller buffer of fixed capacity.
+struct ByteSink {
+  uint8_t *data = nullptr;
+  size_t size = 0, cap = 0;
+  bool owned = true;
+  bool pinned = false;  // data is page-locked: device copies land in it directly
+  ByteSink() = default;
+  ByteSink(uint8_t *p, size_t c);  // caller buffer
+  ~ByteSink();
+  ByteSink(const ByteSink &) = delete;
+  ByteSink &operator=(const ByteSink &) = delete;
+  void reserve(size_t c);          // owned only
+  uint8_t *release();              // hand the owned buffer to the caller
 };
 
 class Compressor {
@@ -33,27 +53,30 @@ class Compressor {
   explicit Compressor(const CompressorConfig &cfg);
   ~Compressor();
   // Compress the blocks (host memory; pinned memory makes the copies
-  // asynchronous) into one stream with header digit `level`; appends to out.
+  // asynchronous) into one stream with header digit `level`, written at
+  // out.size onward.
   void compress(const uint8_t *const *ptrs, const int *lens, int nblocks, int level,
-                std::vector<uint8_t> &out, StageTimes *times = nullptr);
+                ByteSink &out, StageTimes *times = nullptr);
   // Same, with the blocks already in device memory (raw bytes of block b at
   // d_ptrs[b]).
   void compress_device(const uint8_t *const *d_ptrs, const int *lens, int nblocks, int level,
-                       std::vector<uint8_t> &out, StageTimes *times = nullptr);
+                       ByteSink &out, StageTimes *times = nullptr);
+  // Convenience for callers holding a std::vector (appends).
+  void compress(const uint8_t *const *ptrs, const int *lens, int nblocks, int level,
+                std::vector<uint8_t> &out, StageTimes *times = nullptr);
   const CompressorConfig &config() const { return cfg_; }
   int device() const { return device_; }
 
  private:
   struct Worker;
   void run(const uint8_t *const *ptrs, const int *lens, int nblocks, int level, bool on_device,
-           std::vector<uint8_t> &out, StageTimes *times);
+           ByteSink &out, StageTimes *times);
   CompressorConfig cfg_;
   int device_ = 0;
   std::vector<std::unique_ptr<Worker>> workers_;
 };
 
-// Append the end-of-stream marker and combined CRC at bit offset `bit` of
-// `out` (whose last byte may be partial), then pad to a byte.
-void append_eos(std::vector<uint8_t> &out, int64_t bit, uint32_t stream_crc);
+// Upper bound of the stream size for n bytes in nblocks blocks.
+size_t stream_bound(int64_t n, int64_t nblocks);
 
 }  // namespace bz2g

@@ -85,7 +85,8 @@ Workspace::Workspace(int mb, int64_t mr, int64_t me, int mt, int mrt, int mgt)
     dev.mtf = (uint8_t *)alloc(E);
     dev.sa = (int32_t *)alloc(E * 4);
     dev.isa = (int32_t *)alloc(E * 4);
-    dev.head = (int32_t *)alloc(E * 4);
+    dev.kpos[0] = (int32_t *)alloc(E * 4);
+    dev.kpos[1] = (int32_t *)alloc(E * 4);
     dev.keys[0] = (uint64_t *)alloc(E * 8);
     dev.keys[1] = (uint64_t *)alloc(E * 8);
     dev.vals[0] = (uint32_t *)alloc(E * 4);
@@ -101,6 +102,7 @@ Workspace::Workspace(int mb, int64_t mr, int64_t me, int mt, int mrt, int mgt)
     dev.tile_a = (int32_t *)alloc(T * 4);
     dev.tile_b = (int32_t *)alloc(T * 4);
     dev.tile_c = (int32_t *)alloc(T * 4);
+    dev.tile_d = (int32_t *)alloc(T * 4);
     dev.tile_hist = (uint32_t *)alloc((int64_t)mt * 256 * 4);
     dev.tile_last = (int32_t *)alloc((int64_t)mt * 256 * 4);
     dev.gt_bits = (uint32_t *)alloc(((int64_t)mgt + 1) * 4);
@@ -121,6 +123,7 @@ Workspace::Workspace(int mb, int64_t mr, int64_t me, int mt, int mrt, int mgt)
     dev.sort_len = (int32_t *)alloc(B * 4);
     dev.done = (int32_t *)alloc(B * 4);
     dev.ngroups = (int32_t *)alloc(B * 4);
+    dev.act_len = (int32_t *)alloc(B * 4);
     dev.active_sum = (int64_t *)alloc(B * 8);
     dev.pstat = (int32_t *)alloc(B * 8 * 4);
     dev.hdr_bits = (int64_t *)alloc(B * 8);
@@ -128,6 +131,7 @@ Workspace::Workspace(int mb, int64_t mr, int64_t me, int mt, int mrt, int mgt)
     dev.blk_start = (int64_t *)alloc(B * 8);
     dev.sort_ctl = (int32_t *)alloc(64);
     dev.stream = (uint64_t *)alloc(64);
+    dev.kt_elems = (uint64_t *)alloc(8 * kMaxTimedLaunches);
     // plan arrays: 3 int64 per block + ints
     pinned_plan_bytes = (size_t)B * 3 * 8 + ((size_t)B * 4 + mrt * 2 + mt + mgt * 2) * 4 + 1024;
     plan_dev_ = alloc(pinned_plan_bytes);

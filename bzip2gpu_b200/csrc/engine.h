@@ -4,7 +4,7 @@
 // element layout, so a kernel finds a block's data at off[b]):
 //   raw      uint8   block b at raw_off[b] (16-byte aligned), raw_len[b] bytes
 //   rle1     uint8   block b at off[b], m[b] bytes           (off[b] % kTile == 0)
-//   sa, isa, head    int32 at off[b], m[b] entries (block-local indices)
+//   sa, isa, kpos[2] int32 at off[b], m[b] entries (block-local indices)
 //   keys[2]  uint64, vals[2] uint32: radix sort ping-pong, same layout
 //   last     uint8   BWT last column, same layout
 //   mtf      uint8   same layout
@@ -47,14 +47,15 @@ struct SlabDev {
   const int *raw_len, *rt_block, *rt_start, *rt_first, *tile_block, *gt_block, *gt_first, *gt_begin;
   // data
   uint8_t *raw, *rle1, *last, *mtf;
-  int32_t *sa, *isa, *head;
+  int32_t *sa, *isa;
+  int32_t *kpos[2];                    // BWT: sorted-array position of each active rotation
   uint64_t *keys[2];
   uint32_t *vals[2];
   uint16_t *rle2;
   uint8_t *sel, *sel_mtf;
   uint32_t *out;
   // per-tile scratch
-  int32_t *tile_a, *tile_b, *tile_c;  // [ntiles] or [n_raw_tiles]
+  int32_t *tile_a, *tile_b, *tile_c, *tile_d;  // [ntiles] or [n_raw_tiles]
   uint32_t *tile_hist;                 // [ntiles * 256]
   int32_t *tile_last;                  // [ntiles * 256]
   uint32_t *gt_bits;                   // [n_group_tiles]
@@ -66,17 +67,29 @@ struct SlabDev {
   uint8_t *len;                        // [nblocks * 6 * 258]
   int32_t *code;                       // [nblocks * 6 * 258]
   int32_t *rfreq;                      // [nblocks * 6 * 258]
-  int32_t *sort_len, *done, *ngroups;  // BWT control
+  int32_t *sort_len, *done, *ngroups;  // BWT control (ngroups: groups among active rotations)
+  int32_t *act_len;                    // BWT: active rotations entering the next round
   int64_t *active_sum;                 // A: rotations in non-singleton groups, summed over rounds
   int32_t *pstat;                      // [nblocks * 8]: heads and singletons at prefix 1,2,4,8
   int64_t *hdr_bits, *pay_bits, *blk_start;
   // radix sort control
-  int32_t *sort_ctl;                   // [0]=cur buffer, [1]=nontrivial flag, [2]=blocks still sorting
+  int32_t *sort_ctl;                   // [0]=cur key buffer, [1]=nontrivial flag,
+                                       // [2]=blocks still sorting, [3]=cur kpos buffer
   int32_t *h_flags;                    // pinned host mirror of small counters
   // stream state: [0] = bit offset (u64), [1] = stream crc, [2] = slab first word,
   // [3] = slab word count
   uint64_t *stream;
+  // optional per-launch timing of the radix scatter (host-side fields, only
+  // read on the host): events around each launch, the elements each launch
+  // moved (device counters) and its bytes per element
+  int kt_on;
+  cudaEvent_t *kt_ev;       // [2 * kMaxTimedLaunches]
+  int *kt_n;                // launches recorded in this slab
+  int *kt_bpe;              // [kMaxTimedLaunches]
+  uint64_t *kt_elems;       // device [kMaxTimedLaunches]
 };
+
+constexpr int kMaxTimedLaunches = 96;
 
 // Owns the device buffers of a slab context (sized for a maximum slab).
 class Workspace {

@@ -98,96 +98,112 @@ __global__ void __launch_bounds__(kGroupTile) k_huff_select(SlabDev d) {
 }
 
 // bzip2's length-limited Huffman lengths (src/compression/huffman.cu:13-124),
-// one lane per table; heap, weight and parent arrays live in shared memory.
+// one warp per table.  Lane 0 runs the heap: its entries carry their node's
+// weight in the high half (weight << 32 | node), so a sift step reads a
+// sibling pair with one 16-byte shared load; comparisons use the weight half
+// only, with the reference's strict '<', so ties resolve exactly as there.
+// All lanes then walk the parent links for the code lengths.
 constexpr int kHeapN = kMaxAlpha + 2;
 constexpr int kNodeN = kMaxAlpha * 2;
 
-__global__ void __launch_bounds__(32) k_huff_lengths(SlabDev d) {
-  __shared__ int32_t heap_s[kMaxGroups][kHeapN];
-  __shared__ int32_t weight_s[kMaxGroups][kNodeN];
-  __shared__ int32_t parent_s[kMaxGroups][kNodeN];
+__device__ __forceinline__ uint32_t hw(uint64_t e) { return (uint32_t)(e >> 32); }
+
+__global__ void __launch_bounds__(kMaxGroups * 32) k_huff_lengths(SlabDev d) {
+  __shared__ __align__(16) uint64_t heap_s[kMaxGroups][kHeapN + 2];
+  __shared__ int32_t leafw_s[kMaxGroups][kMaxAlpha + 1];
+  __shared__ int16_t parent_s[kMaxGroups][kNodeN];
   const int b = blockIdx.x;
-  const int t = threadIdx.x;
+  const int t = warp_id();
+  const int ln = lane_id();
   const int ngrp = d.n_groups[b];
   if (t >= ngrp) return;
   const int alpha = d.n_in_use[b] + 2;
-  int32_t *heap = heap_s[t];
-  int32_t *weight = weight_s[t];
-  int32_t *parent = parent_s[t];
+  uint64_t *heap = heap_s[t];
+  int32_t *leafw = leafw_s[t];
+  int16_t *parent = parent_s[t];
   const int32_t *freq = d.rfreq + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
   uint8_t *len = d.len + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
-  for (int i = 0; i < alpha; i++) {
+  for (int i = ln; i < alpha; i += 32) {
     int f = freq[i];
-    weight[i + 1] = (f == 0 ? 1 : f) << 8;
+    leafw[i + 1] = (f == 0 ? 1 : f) << 8;
   }
+  __syncwarp();
   for (;;) {
-    int n_nodes = alpha, n_heap = 0;
-    heap[0] = 0;
-    weight[0] = 0;
-    parent[0] = -2;
-    for (int i = 1; i <= alpha; i++) {
-      parent[i] = -1;
-      n_heap++;
-      heap[n_heap] = i;
-      int zz = n_heap, tmp = heap[zz];
-      while (weight[tmp] < weight[heap[zz >> 1]]) {
-        heap[zz] = heap[zz >> 1];
-        zz >>= 1;
-      }
-      heap[zz] = tmp;
-    }
-    while (n_heap > 1) {
-      int n1 = 0, n2 = 0;
-      for (int pick = 0; pick < 2; pick++) {
-        int top = heap[1];
-        heap[1] = heap[n_heap];
-        n_heap--;
-        int zz = 1, tmp = heap[zz];
-        const int wt = weight[tmp];
-        for (;;) {
-          int yy = zz << 1;
-          if (yy > n_heap) break;
-          if (yy < n_heap && weight[heap[yy + 1]] < weight[heap[yy]]) yy++;
-          if (wt < weight[heap[yy]]) break;
-          heap[zz] = heap[yy];
-          zz = yy;
+    if (ln == 0) {
+      int n_nodes = alpha, n_heap = 0;
+      heap[0] = 0;  // sentinel: weight 0
+      for (int i = 1; i <= alpha; i++) {
+        parent[i] = -1;
+        n_heap++;
+        const uint64_t e = ((uint64_t)(uint32_t)leafw[i] << 32) | (uint32_t)i;
+        int zz = n_heap;
+        uint64_t up = heap[zz >> 1];
+        while (hw(e) < hw(up)) {
+          heap[zz] = up;
+          zz >>= 1;
+          up = heap[zz >> 1];
         }
-        heap[zz] = tmp;
-        if (pick == 0) n1 = top;
-        else n2 = top;
+        heap[zz] = e;
       }
-      n_nodes++;
-      parent[n1] = parent[n2] = n_nodes;
-      int32_t w1 = weight[n1], w2 = weight[n2];
-      int32_t d1 = w1 & 0xff, d2 = w2 & 0xff;
-      weight[n_nodes] = (int32_t)(((uint32_t)(w1 & 0xffffff00) + (uint32_t)(w2 & 0xffffff00)) |
-                                  (uint32_t)(1 + (d1 > d2 ? d1 : d2)));
-      parent[n_nodes] = -1;
-      n_heap++;
-      heap[n_heap] = n_nodes;
-      int zz = n_heap, tmp = heap[zz];
-      while (weight[tmp] < weight[heap[zz >> 1]]) {
-        heap[zz] = heap[zz >> 1];
-        zz >>= 1;
+      while (n_heap > 1) {
+        uint64_t pick[2];
+        for (int q = 0; q < 2; q++) {
+          pick[q] = heap[1];
+          const uint64_t tmp = heap[n_heap];
+          n_heap--;
+          int zz = 1;
+          for (;;) {
+            int yy = zz << 1;
+            if (yy > n_heap) break;
+            const ulonglong2 pr = *reinterpret_cast<const ulonglong2 *>(&heap[yy]);
+            uint64_t c = pr.x;
+            if (yy < n_heap && hw(pr.y) < hw(pr.x)) {
+              yy++;
+              c = pr.y;
+            }
+            if (hw(tmp) < hw(c)) break;
+            heap[zz] = c;
+            zz = yy;
+          }
+          heap[zz] = tmp;
+        }
+        const uint32_t w1 = hw(pick[0]), w2 = hw(pick[1]);
+        const int n1 = (int)(uint32_t)pick[0], n2 = (int)(uint32_t)pick[1];
+        n_nodes++;
+        parent[n1] = parent[n2] = (int16_t)n_nodes;
+        const uint32_t d1 = w1 & 0xff, d2 = w2 & 0xff;
+        const uint32_t wn = ((w1 & 0xffffff00u) + (w2 & 0xffffff00u)) | (1 + (d1 > d2 ? d1 : d2));
+        parent[n_nodes] = -1;
+        n_heap++;
+        const uint64_t e = ((uint64_t)wn << 32) | (uint32_t)n_nodes;
+        int zz = n_heap;
+        uint64_t up = heap[zz >> 1];
+        while (hw(e) < hw(up)) {
+          heap[zz] = up;
+          zz >>= 1;
+          up = heap[zz >> 1];
+        }
+        heap[zz] = e;
       }
-      heap[zz] = tmp;
     }
+    __syncwarp();
     bool too_long = false;
-    for (int i = 1; i <= alpha; i++) {
+    for (int i = ln + 1; i <= alpha; i += 32) {
       int j = 0, k = i;
       while (parent[k] >= 0) {
         k = parent[k];
         j++;
       }
       len[i - 1] = (uint8_t)j;
-      if (j > kMaxCodeLen) too_long = true;
+      too_long |= j > kMaxCodeLen;
     }
-    if (!too_long) break;
-    for (int i = 1; i <= alpha; i++) {
-      int j = weight[i] >> 8;
+    if (!__any_sync(0xffffffffu, too_long)) break;
+    for (int i = ln + 1; i <= alpha; i += 32) {
+      int j = leafw[i] >> 8;
       j = 1 + (j / 2);
-      weight[i] = j << 8;
+      leafw[i] = j << 8;
     }
+    __syncwarp();
   }
 }
 
@@ -221,7 +237,7 @@ void stage_huffman(const SlabDev &d, cudaStream_t st) {
     BZ_CUDA(cudaMemsetAsync(d.rfreq, 0, sizeof(int32_t) * kMaxGroups * kMaxAlpha * d.nblocks, st));
     k_huff_select<<<d.n_group_tiles, kGroupTile, 0, st>>>(d);
     BZ_LAUNCH_CHECK();
-    k_huff_lengths<<<d.nblocks, 32, 0, st>>>(d);
+    k_huff_lengths<<<d.nblocks, kMaxGroups * 32, 0, st>>>(d);
     BZ_LAUNCH_CHECK();
   }
   k_huff_codes<<<d.nblocks, 32, 0, st>>>(d);

@@ -7,8 +7,8 @@
 // is the in-use symbols ordered by their last occurrence before that point
 // (most recent first), symbols not seen yet in ascending order.  So each tile
 // records the last position of every symbol, a per-block prefix-max over
-// tiles gives each tile's starting list, and one warp per tile then runs the
-// sequential MTF with the 256-entry list spread over the lanes' registers.
+// tiles gives each tile's starting list, and inside a tile the same fact,
+// applied lane by lane, gives each lane its own starting list.
 #include "engine.h"
 
 namespace bz2g {
@@ -66,13 +66,23 @@ __global__ void __launch_bounds__(256) k_mtf_block_scan(SlabDev d) {
   }
 }
 
-// One warp per tile: starting list from the last-occurrence table, then the
-// sequential move-to-front.  Lane l holds list entries 8l .. 8l+7.
+// One warp per tile.  The tile's starting list comes from the
+// last-occurrence table.  Lane k owns the 128 symbols [128k, 128k+128): it
+// records their distinct values most recent first (its "partial list"); the
+// warp then derives each lane's starting list in turn (list k = partial k-1
+// followed by list k-1 without those symbols), and every lane runs the
+// sequential move-to-front over its own symbols with its own list.
+constexpr int kSub = kTile / 32;      // symbols per lane
+constexpr int kListStride = 260;      // bytes per lane list (bank spread)
+constexpr int kPartStride = kSub + 4;
+
 __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d) {
   __shared__ int key[256];
-  __shared__ int list[256];
-  __shared__ uint8_t sL[kTile];
-  __shared__ uint8_t sO[kTile];
+  __shared__ __align__(16) uint8_t sL[kTile];
+  __shared__ __align__(4) uint8_t lists[32 * kListStride];
+  __shared__ __align__(4) uint8_t part[32 * kPartStride];
+  __shared__ uint32_t pmask[32][8];
+  __shared__ int pcount[32];
   const int t = blockIdx.x;
   const int b = d.tile_block[t];
   const int64_t off = d.off[b];
@@ -82,54 +92,104 @@ __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d) {
   if (valid <= 0) return;
   const int ln = lane_id();
   uint32_t pw[8];
+  int nuse = 0;
 #pragma unroll
-  for (int w = 0; w < 8; w++) pw[w] = d.present[b * 8 + w];
+  for (int w = 0; w < 8; w++) {
+    pw[w] = d.present[b * 8 + w];
+    nuse += __popc(pw[w]);
+  }
   // key: last position before this tile, or (-1 - c) for unseen symbols
   for (int c = ln; c < 256; c += 32) {
     int lp = d.tile_last[(size_t)t * 256 + c];
     bool use = (pw[c >> 5] >> (c & 31)) & 1u;
     key[c] = !use ? INT32_MIN : (lp >= 0 ? lp : -1 - c);
-    list[c] = -1;
   }
   const uint4 *src = reinterpret_cast<const uint4 *>(d.last + off + lt);
   for (int w = ln; w < (valid + 15) / 16; w += 32) reinterpret_cast<uint4 *>(sL)[w] = src[w];
+#pragma unroll
+  for (int w = 0; w < 8; w++) pmask[ln][w] = 0;
   __syncwarp();
   for (int c = ln; c < 256; c += 32) {
     int kc = key[c];
     if (kc == INT32_MIN) continue;
     int r = 0;
     for (int c2 = 0; c2 < 256; c2++) r += key[c2] > kc;
-    list[r] = c;
+    lists[r] = (uint8_t)c;  // list of lane 0
+  }
+  // partial lists
+  const int a0 = ln * kSub;
+  const int a1 = min(valid, a0 + kSub);
+  {
+    int cnt = 0;
+    uint8_t *pp = part + ln * kPartStride;
+    for (int i = a1 - 1; i >= a0; i--) {
+      const int c = sL[i];
+      const uint32_t bit = 1u << (c & 31);
+      const uint32_t mw = pmask[ln][c >> 5];
+      if (!(mw & bit)) {
+        pmask[ln][c >> 5] = mw | bit;
+        pp[cnt++] = (uint8_t)c;
+      }
+    }
+    pcount[ln] = cnt;
   }
   __syncwarp();
-  int e0 = list[ln * 8 + 0], e1 = list[ln * 8 + 1], e2 = list[ln * 8 + 2], e3 = list[ln * 8 + 3];
-  int e4 = list[ln * 8 + 4], e5 = list[ln * 8 + 5], e6 = list[ln * 8 + 6], e7 = list[ln * 8 + 7];
-  for (int e = 0; e < valid; e++) {
-    const int c = sL[e];
-    int slot = e0 == c ? 0 : e1 == c ? 1 : e2 == c ? 2 : e3 == c ? 3
-             : e4 == c ? 4 : e5 == c ? 5 : e6 == c ? 6 : e7 == c ? 7 : -1;
-    unsigned bal = __ballot_sync(0xffffffffu, slot >= 0);
-    int owner = __ffs(bal) - 1;
-    int os = __shfl_sync(0xffffffffu, slot, owner);
-    if (ln == 0) sO[e] = (uint8_t)(owner * 8 + os);
-    int carry = __shfl_up_sync(0xffffffffu, e7, 1);
-    if (ln == 0) carry = c;
-    if ((int)ln < owner) {
-      e7 = e6; e6 = e5; e5 = e4; e4 = e3; e3 = e2; e2 = e1; e1 = e0; e0 = carry;
-    } else if ((int)ln == owner) {
-      if (os >= 7) e7 = e6;
-      if (os >= 6) e6 = e5;
-      if (os >= 5) e5 = e4;
-      if (os >= 4) e4 = e3;
-      if (os >= 3) e3 = e2;
-      if (os >= 2) e2 = e1;
-      if (os >= 1) e1 = e0;
-      e0 = carry;
+  // lane lists, in turn: list k = partial(k-1) ++ (list k-1 minus partial(k-1))
+  for (int k = 1; k < 32; k++) {
+    const uint8_t *prevl = lists + (k - 1) * kListStride;
+    uint8_t *cur = lists + k * kListStride;
+    const int pc = pcount[k - 1];
+    const uint8_t *pp = part + (k - 1) * kPartStride;
+    for (int q = ln; q < pc; q += 32) cur[q] = pp[q];
+    uint8_t keepv[8];
+    int nk = 0;
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int j = ln * 8 + q;
+      uint8_t c = 0;
+      bool keep = false;
+      if (j < nuse) {
+        c = prevl[j];
+        keep = !((pmask[k - 1][c >> 5] >> (c & 31)) & 1u);
+      }
+      keepv[q] = c;
+      nk += keep;
+    }
+    int inc = warp_incl_sum(nk);
+    int o = pc + inc - nk;
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int j = ln * 8 + q;
+      if (j < nuse) {
+        const uint8_t c = keepv[q];
+        if (!((pmask[k - 1][c >> 5] >> (c & 31)) & 1u)) cur[o++] = c;
+      }
+    }
+    __syncwarp();
+  }
+  // each lane: sequential move-to-front over its symbols, in place in sL
+  {
+    uint8_t *lst = lists + ln * kListStride;
+    for (int i = a0; i < a1; i++) {
+      const uint8_t c = sL[i];
+      uint8_t carry = c;
+      int q = 0;
+      uint8_t tmp = lst[0];
+      lst[0] = carry;
+      while (tmp != c && q < 255) {
+        carry = tmp;
+        q++;
+        tmp = lst[q];
+        lst[q] = carry;
+      }
+      sL[i] = (uint8_t)q;
     }
   }
   __syncwarp();
-  uint8_t *dst = d.mtf + off + lt;
-  for (int e = ln; e < valid; e += 32) dst[e] = sO[e];
+  uint4 *dst = reinterpret_cast<uint4 *>(d.mtf + off + lt);
+  const int full = valid / 16;
+  for (int w = ln; w < full; w += 32) dst[w] = reinterpret_cast<const uint4 *>(sL)[w];
+  for (int i = full * 16 + ln; i < valid; i += 32) d.mtf[off + lt + i] = sL[i];
 }
 
 }  // namespace

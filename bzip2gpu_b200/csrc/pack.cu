@@ -43,55 +43,107 @@ struct BitSink {
   }
 };
 
-// Selector MTF and header size; one warp per block.
-__global__ void k_sel_mtf_hdr(SlabDev d) {
+// Per block: selector MTF (src/compression/compress.cu:119-137) and the
+// header size.  256 threads split the selectors into chunks; the MTF list at
+// a chunk's start is the tables ordered by their last use before it (most
+// recent first, unused ones in index order), read off a prefix max over the
+// threads of each table's last position, so every chunk then runs its MTF on
+// its own.
+constexpr int kHdrThreads = 256;
+
+__device__ __forceinline__ int sel_chunk(int nsel, int *a, int *e) {
+  const int per = (nsel + kHdrThreads - 1) / kHdrThreads;
+  *a = min(nsel, (int)threadIdx.x * per);
+  *e = min(nsel, *a + per);
+  return per;
+}
+
+__device__ int64_t table_bits(const uint8_t *len, int alpha) {
+  int cur = len[0];
+  int64_t tb = 5;
+  for (int v = 0; v < alpha; v++) {
+    int tg = len[v];
+    tb += 2 * abs(tg - cur) + 1;
+    cur = tg;
+  }
+  return tb;
+}
+
+__device__ int used_ranges(const uint32_t *pres) {
+  int r = 0;
+  for (int q = 0; q < 16; q++) r += ((pres[q >> 1] >> ((q & 1) * 16)) & 0xffffu) != 0;
+  return r;
+}
+
+__global__ void __launch_bounds__(kHdrThreads) k_sel_mtf_hdr(SlabDev d) {
+  __shared__ int scratch[40];
+  __shared__ int64_t tbits[kMaxGroups];
   const int b = blockIdx.x;
   const int ngrp = d.n_groups[b];
   const int nsel = d.n_sel[b];
   const int alpha = d.n_in_use[b] + 2;
   const uint8_t *sel = d.sel + d.off[b] / 32;
   uint8_t *smtf = d.sel_mtf + d.off[b] / 32;
-  const int ln = threadIdx.x;
-  // table delta bits: lane t < ngrp
-  int64_t tb = 0;
-  if (ln < ngrp) {
-    const uint8_t *len = d.len + ((size_t)b * kMaxGroups + ln) * kMaxAlpha;
-    int cur = len[0];
-    tb = 5;
-    for (int v = 0; v < alpha; v++) {
-      int tg = len[v];
-      tb += 2 * abs(tg - cur) + 1;
-      cur = tg;
+  int a, e;
+  sel_chunk(nsel, &a, &e);
+  int last[kMaxGroups];
+#pragma unroll
+  for (int t = 0; t < kMaxGroups; t++) last[t] = -1;
+  for (int i = a; i < e; i++) {
+    const int v = sel[i];
+#pragma unroll
+    for (int t = 0; t < kMaxGroups; t++)
+      if (v == t) last[t] = i;
+  }
+  int prev[kMaxGroups];
+#pragma unroll
+  for (int t = 0; t < kMaxGroups; t++) {
+    int inc = block_incl_max(last[t], scratch, -1);
+    int ex = __shfl_up_sync(0xffffffffu, inc, 1);
+    __shared__ int wl[kHdrThreads / 32];
+    if (lane_id() == 31) wl[warp_id()] = inc;
+    __syncthreads();
+    if (lane_id() == 0) ex = warp_id() == 0 ? -1 : wl[warp_id() - 1];
+    prev[t] = ex;
+    __syncthreads();
+  }
+  // starting list: used tables by last use (latest first), then unused ones
+  uint8_t pos[kMaxGroups];
+  {
+    int key[kMaxGroups];
+    for (int t = 0; t < ngrp; t++) key[t] = prev[t] >= 0 ? prev[t] : -1 - t;
+    for (int t = 0; t < ngrp; t++) {
+      int r = 0;
+      for (int u = 0; u < ngrp; u++) r += key[u] > key[t];
+      pos[r] = (uint8_t)t;
     }
   }
-  for (int o = 16; o > 0; o >>= 1) tb += __shfl_xor_sync(0xffffffffu, tb, o);
-  // used 16-symbol ranges
-  int ranges = 0;
-  if (ln < 16) {
-    uint32_t w = d.present[b * 8 + (ln >> 1)];
-    uint32_t half = (ln & 1) ? (w >> 16) : (w & 0xffffu);
-    ranges = half != 0;
-  }
-  for (int o = 16; o > 0; o >>= 1) ranges += __shfl_xor_sync(0xffffffffu, ranges, o);
-  if (ln == 0) {
-    uint8_t pos[kMaxGroups];
-    for (int i = 0; i < ngrp; i++) pos[i] = (uint8_t)i;
-    int64_t unary = 0;
-    for (int i = 0; i < nsel; i++) {
-      uint8_t v = sel[i];
-      int j = 0;
-      uint8_t tmp = pos[0];
-      while (v != tmp) {
-        j++;
-        uint8_t t2 = tmp;
-        tmp = pos[j];
-        pos[j] = t2;
-      }
-      pos[0] = tmp;
-      smtf[i] = (uint8_t)j;
-      unary += j + 1;
+  int unary = 0;
+  for (int i = a; i < e; i++) {
+    const uint8_t v = sel[i];
+    int j = 0;
+    uint8_t tmp = pos[0];
+    while (v != tmp) {
+      j++;
+      uint8_t t2 = tmp;
+      tmp = pos[j];
+      pos[j] = t2;
     }
-    d.hdr_bits[b] = 48 + 32 + 1 + 24 + 16 + 16 * ranges + 3 + 15 + unary + tb;
+    pos[0] = tmp;
+    smtf[i] = (uint8_t)j;
+    unary += j + 1;
+  }
+  int total_unary;
+  block_excl_sum(unary, scratch, &total_unary);
+  if ((int)threadIdx.x < ngrp)
+    tbits[threadIdx.x] =
+        table_bits(d.len + ((size_t)b * kMaxGroups + threadIdx.x) * kMaxAlpha, alpha);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int64_t tb = 0;
+    for (int t = 0; t < ngrp; t++) tb += tbits[t];
+    const int ranges = used_ranges(d.present + b * 8);
+    d.hdr_bits[b] = 48 + 32 + 1 + 24 + 16 + 16 * ranges + 3 + 15 + (int64_t)total_unary + tb;
   }
 }
 
@@ -149,47 +201,75 @@ __global__ void k_block_starts(SlabDev d, int64_t slab_start) {
 }
 
 // Block header at its stream position (src/compression/compress.cu:290-353).
-__global__ void k_write_header(SlabDev d, int64_t w0) {
-  if (threadIdx.x != 0) return;
+// Thread 0 writes the fixed fields; every thread writes the unary selector
+// codes of its chunk at an offset from a block scan; threads t < nGroups
+// write table t's delta-coded lengths.
+__global__ void __launch_bounds__(kHdrThreads) k_write_header(SlabDev d, int64_t w0) {
+  __shared__ int scratch[40];
+  __shared__ int64_t tbits[kMaxGroups];
   const int b = blockIdx.x;
   const int ngrp = d.n_groups[b];
   const int nsel = d.n_sel[b];
   const int alpha = d.n_in_use[b] + 2;
   const uint32_t *pres = d.present + b * 8;
-  BitSink w;
-  w.init(d.out, d.blk_start[b] - w0 * 32);
-  w.put(0x314159u, 24);
-  w.put(0x265359u, 24);
-  w.put(d.crc[b], 32);
-  w.put(0, 1);
-  w.put((uint32_t)d.orig_ptr[b], 24);
-  uint32_t l1 = 0;
-  for (int r = 0; r < 16; r++) {
-    uint32_t half = (pres[r >> 1] >> ((r & 1) * 16)) & 0xffffu;
-    if (half) l1 |= 1u << (15 - r);
-  }
-  w.put(l1, 16);
-  for (int r = 0; r < 16; r++) {
-    uint32_t half = (pres[r >> 1] >> ((r & 1) * 16)) & 0xffffu;
-    if (!half) continue;
-    uint32_t l2 = 0;
-    for (int q = 0; q < 16; q++)
-      if ((half >> q) & 1u) l2 |= 1u << (15 - q);
-    w.put(l2, 16);
-  }
-  w.put((uint32_t)ngrp, 3);
-  w.put((uint32_t)nsel, 15);
   const uint8_t *smtf = d.sel_mtf + d.off[b] / 32;
-  for (int i = 0; i < nsel; i++) {
-    int j = smtf[i];
-    w.put(((1u << j) - 1u) << 1, j + 1);
+  const int ranges = used_ranges(pres);
+  const int64_t fixed = 48 + 32 + 1 + 24 + 16 + 16 * ranges + 3 + 15;
+  const int64_t base = d.blk_start[b] - w0 * 32;
+  if (threadIdx.x == 0) {
+    BitSink w;
+    w.init(d.out, base);
+    w.put(0x314159u, 24);
+    w.put(0x265359u, 24);
+    w.put(d.crc[b], 32);
+    w.put(0, 1);
+    w.put((uint32_t)d.orig_ptr[b], 24);
+    uint32_t l1 = 0;
+    for (int r = 0; r < 16; r++)
+      if ((pres[r >> 1] >> ((r & 1) * 16)) & 0xffffu) l1 |= 1u << (15 - r);
+    w.put(l1, 16);
+    for (int r = 0; r < 16; r++) {
+      uint32_t half = (pres[r >> 1] >> ((r & 1) * 16)) & 0xffffu;
+      if (!half) continue;
+      uint32_t l2 = 0;
+      for (int q = 0; q < 16; q++)
+        if ((half >> q) & 1u) l2 |= 1u << (15 - q);
+      w.put(l2, 16);
+    }
+    w.put((uint32_t)ngrp, 3);
+    w.put((uint32_t)nsel, 15);
+    w.flush();
   }
-  for (int t = 0; t < ngrp; t++) {
+  int a, e;
+  sel_chunk(nsel, &a, &e);
+  int mine = 0;
+  for (int i = a; i < e; i++) mine += smtf[i] + 1;
+  int total;
+  const int off = block_excl_sum(mine, scratch, &total);
+  if (e > a) {
+    BitSink w;
+    w.init(d.out, base + fixed + off);
+    for (int i = a; i < e; i++) {
+      const int j = smtf[i];
+      w.put(((1u << j) - 1u) << 1, j + 1);
+    }
+    w.flush();
+  }
+  if ((int)threadIdx.x < ngrp)
+    tbits[threadIdx.x] =
+        table_bits(d.len + ((size_t)b * kMaxGroups + threadIdx.x) * kMaxAlpha, alpha);
+  __syncthreads();
+  if ((int)threadIdx.x < ngrp) {
+    const int t = threadIdx.x;
+    int64_t at = base + fixed + total;
+    for (int u = 0; u < t; u++) at += tbits[u];
     const uint8_t *len = d.len + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
+    BitSink w;
+    w.init(d.out, at);
     int cur = len[0];
     w.put((uint32_t)cur, 5);
     for (int v = 0; v < alpha; v++) {
-      int tg = len[v];
+      const int tg = len[v];
       while (cur < tg) {
         w.put(2, 2);
         cur++;
@@ -200,8 +280,8 @@ __global__ void k_write_header(SlabDev d, int64_t w0) {
       }
       w.put(0, 1);
     }
+    w.flush();
   }
-  w.flush();
 }
 
 // Payload: one thread per 50-symbol group.
@@ -264,7 +344,7 @@ __global__ void __launch_bounds__(kGroupTile) k_pack_words(SlabDev d, uint32_t *
 }  // namespace
 
 void stage_sizes(const SlabDev &d, cudaStream_t st) {
-  k_sel_mtf_hdr<<<d.nblocks, 32, 0, st>>>(d);
+  k_sel_mtf_hdr<<<d.nblocks, kHdrThreads, 0, st>>>(d);
   BZ_LAUNCH_CHECK();
   k_pay_bits<<<d.n_group_tiles, kGroupTile, 0, st>>>(d);
   BZ_LAUNCH_CHECK();
@@ -284,7 +364,7 @@ void stage_place(const SlabDev &d, int64_t slab_start_bit, int64_t w0, int64_t n
   BZ_CUDA(cudaMemsetAsync(d.out, 0, sizeof(uint32_t) * nwords, st));
   k_block_starts<<<1, 32, 0, st>>>(d, slab_start_bit);
   BZ_LAUNCH_CHECK();
-  k_write_header<<<d.nblocks, 32, 0, st>>>(d, w0);
+  k_write_header<<<d.nblocks, kHdrThreads, 0, st>>>(d, w0);
   BZ_LAUNCH_CHECK();
   k_write_payload<<<d.n_group_tiles, kGroupTile, 0, st>>>(d, w0);
   BZ_LAUNCH_CHECK();

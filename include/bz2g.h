@@ -55,6 +55,10 @@ int bz2g_compress_device(const uint8_t *d_in, size_t n, int level, int block_byt
  * it does not fit; bz2g_compress_bound gives a sufficient size). */
 int bz2g_compress_into(const uint8_t *in, size_t n, int level, int block_bytes, uint8_t *out,
                        size_t cap, size_t *out_len);
+/* As bz2g_compress_device into a caller host buffer (page-locked memory
+ * receives the device copies directly). */
+int bz2g_compress_device_into(const uint8_t *d_in, size_t n, int level, int block_bytes,
+                              uint8_t *out, size_t cap, size_t *out_len);
 size_t bz2g_compress_bound(size_t n, int block_bytes);
 void bz2g_free(void *p);
 
@@ -67,8 +71,9 @@ int bz2g_set_engine(int slab_blocks, int workers);
  * CUDA events around every stage of the following whole-stream calls.
  * bz2g_last_stats fills out[0..n) with, for the last whole-stream call on
  * this thread: blocks, sum n, sum m, sum A, sum s, sum groups, payload bits,
- * then device ms of RLE1+CRC, BWT, MTF, RLE2, Huffman, sizes, placement;
- * returns the number of fields.  bz2g_launch_count: kernels launched by this
+ * then device ms of RLE1+CRC, BWT, MTF, RLE2, Huffman, sizes, placement,
+ * then the radix-scatter kernel's timed launches, their summed device ms and
+ * their algorithmic bytes (items read + written); returns the field count.  bz2g_launch_count: kernels launched by this
  * library since it was loaded. */
 int bz2g_set_timing(int on);
 int bz2g_last_stats(double *out, int n);

@@ -78,6 +78,15 @@ def test_bwt_cases(torch_cuda, case):
     assert np.array_equal(got, oracle.bwt(a))
 
 
+@pytest.mark.parametrize("case", ["uniform_2_2M", "markov4_2_2M"])
+def test_bwt_large_m_unpacked_layout(torch_cuda, case):
+    # m >= 2^21 takes the 64-bit key + 32-bit rotation layout of the sort
+    a = {"uniform_2_2M": B.gen_uniform(2200000, 77),
+         "markov4_2_2M": B.gen_markov(2200000, 78, np.arange(4, dtype=np.uint8), 0.5, 0.0, 4, 4)}[case]
+    got = B.bwt(dev(torch_cuda, a)).cpu().numpy()
+    assert np.array_equal(got, oracle.bwt(a))
+
+
 # -------------------------------------------------------------------- MTF
 @pytest.mark.parametrize("A", [256, 4])
 def test_mtf_reference_vectors(torch_cuda, A):
