@@ -33,6 +33,7 @@ namespace {
 constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;
 constexpr int kSortWarps = kTileThreads / 32;  // 8
+constexpr int kWarpSpan = kTile / kSortWarps;   // elements per warp in a tile (512)
 constexpr size_t kScatterSmem =
     (size_t)kTile * 8 + (size_t)kTile * 4 + (size_t)kSortWarps * kRadix * 4 + 2 * kRadix * 4;
 
@@ -47,6 +48,12 @@ __device__ __forceinline__ uint64_t key_of(const Layout L, uint64_t item) {
   return L.packed ? item >> L.low : item;
 }
 
+// Tile of this CTA: blockIdx.x, or the blockIdx.x-th entry of a list of the
+// tiles that hold work (doubling rounds).
+__device__ __forceinline__ int tile_id(const int32_t *list) {
+  return list ? list[blockIdx.x] : (int)blockIdx.x;
+}
+
 __device__ __forceinline__ int tile_valid(const SlabDev &d, int t, const int32_t *lens, int *b_out,
                                           int *lt_out) {
   int b = d.tile_block[t];
@@ -57,10 +64,11 @@ __device__ __forceinline__ int tile_valid(const SlabDev &d, int t, const int32_t
   return v < 0 ? 0 : (v > kTile ? kTile : v);
 }
 
-__global__ void __launch_bounds__(256) k_radix_hist(SlabDev d, int shift) {
+__global__ void __launch_bounds__(256) k_radix_hist(SlabDev d, int shift, const int32_t *list) {
   __shared__ uint32_t cnt[kRadix];
+  const int t = tile_id(list);
   int b, lt;
-  int valid = tile_valid(d, blockIdx.x, d.sort_len, &b, &lt);
+  int valid = tile_valid(d, t, d.sort_len, &b, &lt);
   if (valid == 0) return;
   cnt[threadIdx.x] = 0;
   __syncthreads();
@@ -68,7 +76,7 @@ __global__ void __launch_bounds__(256) k_radix_hist(SlabDev d, int shift) {
   for (int e = threadIdx.x; e < valid; e += blockDim.x)
     atomicAdd(&cnt[(uint32_t)(K[e] >> shift) & (kRadix - 1)], 1u);
   __syncthreads();
-  d.tile_hist[(size_t)blockIdx.x * kRadix + threadIdx.x] = cnt[threadIdx.x];
+  d.tile_hist[(size_t)t * kRadix + threadIdx.x] = cnt[threadIdx.x];
 }
 
 // Per block: turn tile digit counts into global scatter bases.
@@ -99,47 +107,54 @@ __global__ void __launch_bounds__(256) k_radix_scan(SlabDev d) {
 // (lane l, item i <-> element w*512 + i*32 + l) so that ranking item by item
 // with __match_any_sync keeps the original order; the tile is sorted locally
 // in shared memory, then written so that equal digits go out contiguously.
-__global__ void __launch_bounds__(256) k_radix_scatter(SlabDev d, int shift, int has_vals,
-                                                       int timed) {
+// All of a thread's loads are issued before the ranking starts.
+template <bool kVals>
+__global__ void __launch_bounds__(256, kVals ? 2 : 3)
+    k_radix_scatter(SlabDev d, int shift, int timed, const int32_t *list) {
   if (!d.sort_ctl[1]) return;
+  const int t = tile_id(list);
   int b, lt;
-  int valid = tile_valid(d, blockIdx.x, d.sort_len, &b, &lt);
+  const int valid = tile_valid(d, t, d.sort_len, &b, &lt);
   if (valid == 0) return;
   if (timed >= 0 && threadIdx.x == 0)
     atomicAdd((unsigned long long *)&d.kt_elems[timed], (unsigned long long)valid);
   extern __shared__ __align__(16) uint8_t smem[];
   uint64_t *sk = reinterpret_cast<uint64_t *>(smem);
   uint32_t *sv = reinterpret_cast<uint32_t *>(sk + kTile);
-  uint32_t *wcnt = sv + kTile;                 // [warp][digit]
+  uint32_t *wcnt = kVals ? sv + kTile : reinterpret_cast<uint32_t *>(sk + kTile);  // [warp][digit]
   uint32_t *lbase = wcnt + kSortWarps * kRadix;  // local digit base
-  uint32_t *goff = lbase + kRadix;             // global digit base for this tile
+  uint32_t *goff = lbase + kRadix;               // global digit base for this tile
   const int cur = d.sort_ctl[0];
   const uint64_t *K = d.keys[cur] + d.off[b] + lt;
   const uint32_t *V = d.vals[cur] + d.off[b] + lt;
   const int w = warp_id(), ln = lane_id();
-  if (!has_vals) {  // keys only: the value array area holds the counters
-    wcnt = reinterpret_cast<uint32_t *>(sk + kTile);
-    lbase = wcnt + kSortWarps * kRadix;
-    goff = lbase + kRadix;
-  }
-  for (int i = threadIdx.x; i < kSortWarps * kRadix; i += blockDim.x) wcnt[i] = 0;
-  goff[threadIdx.x] = d.tile_hist[(size_t)blockIdx.x * kRadix + threadIdx.x];
-  __syncthreads();
 
   uint64_t key[kTileItems];
   uint32_t val[kTileItems];
-  uint32_t rank[kTileItems];
+#pragma unroll
+  for (int i = 0; i < kTileItems; i++) {
+    const int e = w * kWarpSpan + i * 32 + ln;
+    key[i] = e < valid ? K[e] : 0;
+    if (kVals) val[i] = e < valid ? V[e] : 0;
+  }
+  for (int i = threadIdx.x; i < kSortWarps * kRadix; i += blockDim.x) wcnt[i] = 0;
+  goff[threadIdx.x] = d.tile_hist[(size_t)t * kRadix + threadIdx.x];
+  __syncthreads();
+
+  uint32_t rank2[kTileItems / 2];  // two 16-bit ranks per register (ranks < 512)
   const unsigned lt_mask = (1u << ln) - 1u;
 #pragma unroll
   for (int i = 0; i < kTileItems; i++) {
-    int e = w * 512 + i * 32 + ln;
-    bool ok = e < valid;
-    key[i] = ok ? K[e] : 0;
-    val[i] = ok && has_vals ? V[e] : 0;
-    int dg = ok ? (int)((key[i] >> shift) & (kRadix - 1)) : kRadix + 1;
-    unsigned peers = __match_any_sync(0xffffffffu, dg);
-    uint32_t before = ok ? wcnt[w * kRadix + dg] : 0;
-    rank[i] = before + __popc(peers & lt_mask);
+    const int e = w * kWarpSpan + i * 32 + ln;
+    const bool ok = e < valid;
+    const int dg = ok ? (int)((key[i] >> shift) & (kRadix - 1)) : kRadix + 1;
+    const unsigned peers = __match_any_sync(0xffffffffu, dg);
+    const uint32_t before = ok ? wcnt[w * kRadix + dg] : 0;
+    const uint32_t r = before + __popc(peers & lt_mask);
+    if (i & 1)
+      rank2[i >> 1] |= r << 16;
+    else
+      rank2[i >> 1] = r;
     __syncwarp();
     if (ok && (peers & lt_mask) == 0) wcnt[w * kRadix + dg] = before + __popc(peers);
     __syncwarp();
@@ -156,29 +171,29 @@ __global__ void __launch_bounds__(256) k_radix_scatter(SlabDev d, int shift, int
     }
     __shared__ uint32_t scratch[40];
     uint32_t tot;
-    uint32_t ex = block_excl_sum(run, scratch, &tot);
-    lbase[dg] = ex;
+    lbase[dg] = block_excl_sum(run, scratch, &tot);
   }
   __syncthreads();
 #pragma unroll
   for (int i = 0; i < kTileItems; i++) {
-    int e = w * 512 + i * 32 + ln;
+    const int e = w * kWarpSpan + i * 32 + ln;
     if (e < valid) {
-      int dg = (int)((key[i] >> shift) & (kRadix - 1));
-      uint32_t pos = lbase[dg] + wcnt[w * kRadix + dg] + rank[i];
+      const int dg = (int)((key[i] >> shift) & (kRadix - 1));
+      const uint32_t r = (i & 1) ? rank2[i >> 1] >> 16 : rank2[i >> 1] & 0xffffu;
+      const uint32_t pos = lbase[dg] + wcnt[w * kRadix + dg] + r;
       sk[pos] = key[i];
-      if (has_vals) sv[pos] = val[i];
+      if (kVals) sv[pos] = val[i];
     }
   }
   __syncthreads();
   uint64_t *KO = d.keys[cur ^ 1];
   uint32_t *VO = d.vals[cur ^ 1];
   for (int k = threadIdx.x; k < valid; k += blockDim.x) {
-    uint64_t kk = sk[k];
-    int dg = (int)((kk >> shift) & (kRadix - 1));
-    uint32_t g = goff[dg] + (uint32_t)k - lbase[dg];
+    const uint64_t kk = sk[k];
+    const int dg = (int)((kk >> shift) & (kRadix - 1));
+    const uint32_t g = goff[dg] + (uint32_t)k - lbase[dg];
     KO[g] = kk;
-    if (has_vals) VO[g] = sv[k];
+    if (kVals) VO[g] = sv[k];
   }
 }
 
@@ -187,12 +202,15 @@ __global__ void k_radix_flip(SlabDev d) {
   d.sort_ctl[1] = 0;
 }
 
-// Stable sort of each block's elements by key bits [lo, hi).
-void radix_sort(const SlabDev &d, int lo, int hi, int has_vals, cudaStream_t st) {
+// Stable sort of each block's elements by key bits [lo, hi), over `grid`
+// tiles (all tiles, or the listed ones).
+void radix_sort(const SlabDev &d, int lo, int hi, int has_vals, cudaStream_t st, int grid,
+                const int32_t *list) {
   const size_t smem = has_vals ? kScatterSmem : (size_t)kTile * 8 + (size_t)kSortWarps * kRadix * 4 +
                                                     2 * kRadix * 4;
+  if (grid <= 0) return;
   for (int shift = lo; shift < hi; shift += kRadixBits) {
-    k_radix_hist<<<d.ntiles, 256, 0, st>>>(d, shift);
+    k_radix_hist<<<grid, 256, 0, st>>>(d, shift, list);
     BZ_LAUNCH_CHECK();
     k_radix_scan<<<d.nblocks, 256, 0, st>>>(d);
     BZ_LAUNCH_CHECK();
@@ -202,7 +220,10 @@ void radix_sort(const SlabDev &d, int lo, int hi, int has_vals, cudaStream_t st)
       d.kt_bpe[timed] = has_vals ? 24 : 16;
       BZ_CUDA(cudaEventRecord(d.kt_ev[2 * timed], st));
     }
-    k_radix_scatter<<<d.ntiles, 256, smem, st>>>(d, shift, has_vals, timed);
+    if (has_vals)
+      k_radix_scatter<true><<<grid, 256, smem, st>>>(d, shift, timed, list);
+    else
+      k_radix_scatter<false><<<grid, 256, smem, st>>>(d, shift, timed, list);
     BZ_LAUNCH_CHECK();
     if (timed >= 0) BZ_CUDA(cudaEventRecord(d.kt_ev[2 * timed + 1], st));
     k_radix_flip<<<1, 1, 0, st>>>(d);
@@ -327,16 +348,16 @@ __global__ void __launch_bounds__(256) k_bwt_keys0(SlabDev d, int packed) {
 // where the key changes; its head is the SA position of its first element.
 // Elements are read warp-striped (warp w owns [512w, 512w + 512), item i of
 // lane l is element 512w + 32i + l) so every load is coalesced.
-constexpr int kWarpSpan = kTile / kSortWarps;  // 512
-
 __device__ __forceinline__ uint64_t key_at(const uint64_t *K, int k) { return K[k]; }
 
 // Per tile: last head (SA position), head count, singleton count, active
 // (non-singleton) count.
-__global__ void __launch_bounds__(256) k_bwt_flags(SlabDev d, Layout L, int initial) {
+__global__ void __launch_bounds__(256) k_bwt_flags(SlabDev d, Layout L, int initial,
+                                                   const int32_t *list) {
   __shared__ int red[4][kSortWarps];
+  const int t = tile_id(list);
   int b, lt;
-  const int valid = tile_valid(d, blockIdx.x, d.sort_len, &b, &lt);
+  const int valid = tile_valid(d, t, d.sort_len, &b, &lt);
   if (valid == 0) return;
   const int len = d.sort_len[b];
   const int64_t off = d.off[b];
@@ -377,10 +398,10 @@ __global__ void __launch_bounds__(256) k_bwt_flags(SlabDev d, Layout L, int init
       h += red[1][q];
       sg += red[2][q];
     }
-    d.tile_a[blockIdx.x] = l;
-    d.tile_b[blockIdx.x] = h;
-    d.tile_c[blockIdx.x] = sg;
-    d.tile_d[blockIdx.x] = valid - sg;  // elements in groups of size >= 2
+    d.tile_a[t] = l;
+    d.tile_b[t] = h;
+    d.tile_c[t] = sg;
+    d.tile_d[t] = valid - sg;  // elements in groups of size >= 2
   }
 }
 
@@ -429,6 +450,7 @@ __global__ void __launch_bounds__(256) k_bwt_rank_block(SlabDev d, int64_t prefi
     } else {
       d.act_len[b] = active;
       atomicAdd(&d.sort_ctl[2], 1);
+      atomicAdd(&d.sort_ctl[4], (active + kTile - 1) / kTile);
       d.active_sum[b] += active;  // rotations entering the next round
     }
   }
@@ -437,11 +459,13 @@ __global__ void __launch_bounds__(256) k_bwt_rank_block(SlabDev d, int64_t prefi
 // Write SA and ISA for the sorted elements, and compact the elements of
 // groups of size >= 2 (for blocks still sorting) into the other key/value/
 // position buffers, keyed by their new head (rank of i+h added next round).
-__global__ void __launch_bounds__(256) k_bwt_apply(SlabDev d, Layout L, int initial, int kb) {
+__global__ void __launch_bounds__(256) k_bwt_apply(SlabDev d, Layout L, int initial, int kb,
+                                                   const int32_t *list) {
   __shared__ int wlast[kSortWarps];
   __shared__ int wact[kSortWarps];
+  const int t = tile_id(list);
   int b, lt;
-  const int valid = tile_valid(d, blockIdx.x, d.sort_len, &b, &lt);
+  const int valid = tile_valid(d, t, d.sort_len, &b, &lt);
   if (valid == 0) return;
   const int len = d.sort_len[b];
   const int64_t off = d.off[b];
@@ -474,8 +498,8 @@ __global__ void __launch_bounds__(256) k_bwt_apply(SlabDev d, Layout L, int init
     wact[w] = act;
   }
   __syncthreads();
-  int carry = d.tile_a[blockIdx.x];
-  int aoff = d.tile_d[blockIdx.x];
+  int carry = d.tile_a[t];
+  int aoff = d.tile_d[t];
   for (int q = 0; q < w; q++) {
     carry = max(carry, wlast[q]);
     aoff += wact[q];
@@ -526,19 +550,32 @@ __global__ void __launch_bounds__(256) k_bwt_apply(SlabDev d, Layout L, int init
   }
 }
 
+// Next round: sort_len = active rotations; list the tiles that hold them.
+__global__ void k_bwt_tile_list(SlabDev d) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= d.nblocks) return;
+  const int len = d.act_len[b];
+  d.sort_len[b] = len;
+  if (len <= 0) return;
+  const int nt = (len + kTile - 1) / kTile;
+  const int at = atomicAdd(&d.sort_ctl[5], nt);
+  const int t0 = (int)(d.off[b] / kTile);
+  for (int k = 0; k < nt; k++) d.tile_list[at + k] = t0 + k;
+}
+
 __global__ void k_bwt_flip(SlabDev d) {
   d.sort_ctl[0] ^= 1;
   d.sort_ctl[3] ^= 1;
 }
 
 // Round keys for the compacted active rotations: add the rank of i+h.
-__global__ void __launch_bounds__(256) k_bwt_round_keys(SlabDev d, int h, int packed, int kb) {
-  const int t = blockIdx.x;
+__global__ void __launch_bounds__(256) k_bwt_round_keys(SlabDev d, int h, int packed, int kb,
+                                                        const int32_t *list) {
+  const int t = tile_id(list);
   const int b = d.tile_block[t];
   const int64_t off = d.off[b];
   const int lt = (int)((int64_t)t * kTile - off);
-  const int len = d.act_len[b];
-  if (lt == 0 && threadIdx.x == 0) d.sort_len[b] = len;
+  const int len = d.sort_len[b];
   const int valid = min(kTile, len - lt);
   if (valid <= 0) return;
   const int m = d.m[b];
@@ -567,8 +604,10 @@ bool smem_configured = false;
 
 void stage_bwt(const SlabDev &d, int max_m, cudaStream_t st) {
   if (!smem_configured) {
-    BZ_CUDA(cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kScatterSmem));
+    BZ_CUDA(cudaFuncSetAttribute(k_radix_scatter<true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScatterSmem));
+    BZ_CUDA(cudaFuncSetAttribute(k_radix_scatter<false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScatterSmem));
     smem_configured = true;
   }
   int kb = 1;
@@ -583,37 +622,44 @@ void stage_bwt(const SlabDev &d, int max_m, cudaStream_t st) {
   const Layout first = {packed, packed ? 32 : 0};
   const Layout round = {packed, packed ? kb : 0};
   if (packed)
-    radix_sort(d, 32, 64, 0, st);
+    radix_sort(d, 32, 64, 0, st, d.ntiles, nullptr);
   else
-    radix_sort(d, 0, 64, 1, st);
+    radix_sort(d, 0, 64, 1, st, d.ntiles, nullptr);
   const int nq = packed ? 3 : 4;  // prefixes 1,2,4 (,8) bytes
   k_bwt_prefix_stats<<<d.ntiles, 256, 0, st>>>(d, first, packed ? 32 : 64, nq);
   BZ_LAUNCH_CHECK();
   k_bwt_prefix_account<<<(d.nblocks + 127) / 128, 128, 0, st>>>(d, nq);
   BZ_LAUNCH_CHECK();
   int64_t prefix = packed ? 4 : 8;
+  int grid = d.ntiles;
+  const int32_t *list = nullptr;
   for (int initial = 1;; initial = 0) {
     const Layout L = initial ? first : round;
     BZ_CUDA(cudaMemsetAsync(d.sort_ctl + 2, 0, sizeof(int32_t), st));
-    k_bwt_flags<<<d.ntiles, 256, 0, st>>>(d, L, initial);
+    BZ_CUDA(cudaMemsetAsync(d.sort_ctl + 4, 0, 2 * sizeof(int32_t), st));
+    k_bwt_flags<<<grid, 256, 0, st>>>(d, L, initial, list);
     BZ_LAUNCH_CHECK();
     k_bwt_rank_block<<<d.nblocks, 256, 0, st>>>(d, prefix);
     BZ_LAUNCH_CHECK();
-    k_bwt_apply<<<d.ntiles, 256, 0, st>>>(d, L, initial, kb);
+    k_bwt_apply<<<grid, 256, 0, st>>>(d, L, initial, kb, list);
     BZ_LAUNCH_CHECK();
     k_bwt_flip<<<1, 1, 0, st>>>(d);
     BZ_LAUNCH_CHECK();
     if (prefix >= max_m) break;
-    BZ_CUDA(cudaMemcpyAsync(d.h_flags, d.sort_ctl + 2, sizeof(int32_t), cudaMemcpyDeviceToHost,
+    k_bwt_tile_list<<<(d.nblocks + 127) / 128, 128, 0, st>>>(d);
+    BZ_LAUNCH_CHECK();
+    BZ_CUDA(cudaMemcpyAsync(d.h_flags, d.sort_ctl + 2, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost,
                             st));
     BZ_CUDA(cudaStreamSynchronize(st));
     if (d.h_flags[0] == 0) break;
-    k_bwt_round_keys<<<d.ntiles, 256, 0, st>>>(d, (int)prefix, packed, kb);
+    grid = d.h_flags[2];  // tiles holding active rotations
+    list = d.tile_list;
+    k_bwt_round_keys<<<grid, 256, 0, st>>>(d, (int)prefix, packed, kb, list);
     BZ_LAUNCH_CHECK();
     if (packed)
-      radix_sort(d, kb, 3 * kb, 0, st);
+      radix_sort(d, kb, 3 * kb, 0, st, grid, list);
     else
-      radix_sort(d, 0, 2 * kb, 1, st);
+      radix_sort(d, 0, 2 * kb, 1, st, grid, list);
     prefix *= 2;
   }
 }

@@ -103,6 +103,7 @@ Workspace::Workspace(int mb, int64_t mr, int64_t me, int mt, int mrt, int mgt)
     dev.tile_b = (int32_t *)alloc(T * 4);
     dev.tile_c = (int32_t *)alloc(T * 4);
     dev.tile_d = (int32_t *)alloc(T * 4);
+    dev.tile_list = (int32_t *)alloc(T * 4);
     dev.tile_hist = (uint32_t *)alloc((int64_t)mt * 256 * 4);
     dev.tile_last = (int32_t *)alloc((int64_t)mt * 256 * 4);
     dev.gt_bits = (uint32_t *)alloc(((int64_t)mgt + 1) * 4);

@@ -69,12 +69,14 @@ struct SlabDev {
   int32_t *rfreq;                      // [nblocks * 6 * 258]
   int32_t *sort_len, *done, *ngroups;  // BWT control (ngroups: groups among active rotations)
   int32_t *act_len;                    // BWT: active rotations entering the next round
+  int32_t *tile_list;                  // BWT: tiles holding active rotations [ntiles]
   int64_t *active_sum;                 // A: rotations in non-singleton groups, summed over rounds
   int32_t *pstat;                      // [nblocks * 8]: heads and singletons at prefix 1,2,4,8
   int64_t *hdr_bits, *pay_bits, *blk_start;
   // radix sort control
   int32_t *sort_ctl;                   // [0]=cur key buffer, [1]=nontrivial flag,
-                                       // [2]=blocks still sorting, [3]=cur kpos buffer
+                                       // [2]=blocks still sorting, [3]=cur kpos buffer,
+                                       // [4]=tiles of the next round, [5]=tile list fill
   int32_t *h_flags;                    // pinned host mirror of small counters
   // stream state: [0] = bit offset (u64), [1] = stream crc, [2] = slab first word,
   // [3] = slab word count

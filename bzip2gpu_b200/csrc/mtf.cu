@@ -73,13 +73,13 @@ __global__ void __launch_bounds__(256) k_mtf_block_scan(SlabDev d) {
 // followed by list k-1 without those symbols), and every lane runs the
 // sequential move-to-front over its own symbols with its own list.
 constexpr int kSub = kTile / 32;      // symbols per lane
-constexpr int kListStride = 260;      // bytes per lane list (bank spread)
+constexpr int kListStride = 264;      // bytes per lane list (8-aligned, bank spread)
 constexpr int kPartStride = kSub + 4;
 
 __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d) {
   __shared__ int key[256];
   __shared__ __align__(16) uint8_t sL[kTile];
-  __shared__ __align__(4) uint8_t lists[32 * kListStride];
+  __shared__ __align__(16) uint8_t lists[32 * kListStride];
   __shared__ __align__(4) uint8_t part[32 * kPartStride];
   __shared__ uint32_t pmask[32][8];
   __shared__ int pcount[32];
@@ -167,20 +167,32 @@ __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d) {
     }
     __syncwarp();
   }
-  // each lane: sequential move-to-front over its symbols, in place in sL
+  // each lane: sequential move-to-front over its symbols, in place in sL.
+  // The list is handled eight entries at a time: entry 8i+q is byte q of
+  // little-endian word i.  A word without the symbol shifts up one byte (its
+  // top byte carries into the next word); in the word holding it, the bytes
+  // below it shift up and it leaves.
   {
-    uint8_t *lst = lists + ln * kListStride;
+    uint64_t *lw = reinterpret_cast<uint64_t *>(lists + ln * kListStride);
+    const uint64_t ones = 0x0101010101010101ull, highs = 0x8080808080808080ull;
     for (int i = a0; i < a1; i++) {
-      const uint8_t c = sL[i];
-      uint8_t carry = c;
+      const uint32_t c = sL[i];
+      const uint64_t bc = ones * c;
+      uint64_t carry = c;
       int q = 0;
-      uint8_t tmp = lst[0];
-      lst[0] = carry;
-      while (tmp != c && q < 255) {
-        carry = tmp;
-        q++;
-        tmp = lst[q];
-        lst[q] = carry;
+      for (int wi = 0; wi < 32; wi++) {
+        const uint64_t wv = lw[wi];
+        const uint64_t x = wv ^ bc;
+        const uint64_t z = (x - ones) & ~x & highs;  // lowest set bit marks the first match
+        if (z) {
+          const int j = (__ffsll((long long)z) - 1) >> 3;
+          const uint64_t low = j == 7 ? ~0ull : ((1ull << (8 * (j + 1))) - 1);
+          lw[wi] = (wv & ~low) | (((wv << 8) | carry) & low);
+          q = wi * 8 + j;
+          break;
+        }
+        lw[wi] = (wv << 8) | carry;
+        carry = wv >> 56;
       }
       sL[i] = (uint8_t)q;
     }

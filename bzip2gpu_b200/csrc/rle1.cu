@@ -119,27 +119,39 @@ __global__ void __launch_bounds__(256) k_rle1_scan_tiles(SlabDev d) {
   }
 
   // CRC of the tile, right-aligned into a virtual 4096-byte tile (leading
-  // zeros leave a zero-init CRC unchanged)
-  if (warp_id() == 0) {
+  // zeros leave a zero-init CRC unchanged): 16 bytes per lane, a shuffle tree
+  // per warp (512 bytes), then warp 0 joins the eight warp CRCs.
+  __shared__ uint32_t wcrc[8];
+  {
     const int pad = kRawTile - len;
     uint32_t r = 0;
-    const int v0 = lane_id() * 128;
-    for (int v = max(v0, pad); v < v0 + 128; v++) {
+    const int v0 = warp_id() * 512 + lane_id() * 16;
+    for (int v = max(v0, pad); v < v0 + 16; v++) {
       uint32_t byte = sb[v - pad];
       r = (r << 8) ^ tbl[(r >> 24) ^ byte];
     }
 #pragma unroll
     for (int k = 0; k < 5; k++) {
-      int dd = 1 << k;
-      uint32_t o = __shfl_down_sync(0xffffffffu, r, dd);
-      if ((lane_id() & (2 * dd - 1)) == 0) r = gf_mul(r, c_xpow[7 + k]) ^ o;
+      const int dd = 1 << k;
+      const uint32_t o = __shfl_down_sync(0xffffffffu, r, dd);
+      if ((lane_id() & (2 * dd - 1)) == 0) r = gf_mul(r, c_xpow[4 + k]) ^ o;  // x^(8*16*dd)
+    }
+    if (lane_id() == 0) wcrc[warp_id()] = r;
+  }
+  __syncthreads();
+  if (warp_id() == 0) {
+    uint32_t r = lane_id() < 8 ? wcrc[lane_id()] : 0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const int dd = 1 << k;
+      const uint32_t o = __shfl_down_sync(0xffffffffu, r, dd);
+      if ((lane_id() & (2 * dd - 1)) == 0) r = gf_mul(r, c_xpow[9 + k]) ^ o;  // x^(8*512*dd)
     }
     if (lane_id() == 0) {
       uint64_t after = (uint64_t)(n - (st + len));
       atomicXor(&d.crc_acc[b], gf_mul(r, xpow8(after)));
     }
   }
-  __syncthreads();
   if (threadIdx.x == 0) {
     int f = INT32_MAX, l = -1;
     for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
