@@ -20,7 +20,7 @@ import numpy as np
 
 __all__ = [
     "Bz2gError", "lib", "lib_path", "compress", "compress_device", "compress_bound",
-    "set_engine", "compress_into", "compress_device_into", "rle1", "crc32", "bwt", "mtf", "symbols_table", "rle2", "huffman_build",
+    "set_engine", "compress_into", "compress_device_into", "compress_batch", "rle1", "crc32", "bwt", "mtf", "symbols_table", "rle2", "huffman_build",
     "huffman_encode", "count_frequencies", "gen_markov", "gen_uniform", "MAX_GROUPS",
     "MAX_ALPHA",
 ]
@@ -41,6 +41,8 @@ _SIGS = {
     "bz2g_compress_into": (_i, [_vp, _sz, _i, _i, _vp, _sz, _c.POINTER(_sz)]),
     "bz2g_compress_device_into": (_i, [_vp, _sz, _i, _i, _vp, _sz, _c.POINTER(_sz)]),
     "bz2g_compress_bound": (_sz, [_sz, _i]),
+    "bz2g_compress_batch": (_i, [_i, _vp, _vp, _vp, _vp, _i, _vp, _sz, _vp]),
+    "bz2g_compress_batch_bound": (_sz, [_i, _vp, _vp, _vp]),
     "bz2g_free": (None, [_vp]),
     "bz2g_set_engine": (_i, [_i, _i]),
     "bz2g_set_timing": (_i, [_i]),
@@ -171,6 +173,37 @@ def compress_device(d_in, level: int = 9, block_bytes: int = 900000) -> bytes:
         return ctypes.string_at(out, ln.value)
     finally:
         lib().bz2g_free(out)
+
+
+def compress_batch(inputs, levels, block_bytes=None, out=None, on_device=False):
+    """Batched form: a list of inputs (host arrays/bytes, or CUDA tensors with
+    on_device=True) -> list of .bz2 streams (memoryviews into one buffer).
+    Block size per input: block_bytes[i], or levels[i] * 100000."""
+    count = len(inputs)
+    keep = []
+    ptrs = (ctypes.c_void_p * max(count, 1))()
+    sizes = (ctypes.c_size_t * max(count, 1))()
+    lv = (ctypes.c_int * max(count, 1))(*[int(x) for x in levels])
+    bb = None
+    if block_bytes is not None:
+        bb = (ctypes.c_int * max(count, 1))(*[int(x) for x in block_bytes])
+    for i, x in enumerate(inputs):
+        if on_device:
+            ptrs[i], sizes[i] = x.data_ptr(), x.numel()
+        else:
+            a, p = _host_view(x)
+            keep.append(a)
+            ptrs[i], sizes[i] = p, a.size
+    cap = lib().bz2g_compress_batch_bound(count, sizes, lv, bb)
+    if out is None:
+        out = np.empty(cap, np.uint8)
+    optr = out.data_ptr() if hasattr(out, "data_ptr") else out.ctypes.data
+    ocap = out.numel() if hasattr(out, "numel") else out.nbytes
+    offs = (ctypes.c_size_t * (count + 1))()
+    _check(lib().bz2g_compress_batch(count, ptrs, sizes, lv, bb, int(on_device), optr, ocap,
+                                     offs))
+    buf = memoryview(out.numpy() if hasattr(out, "numpy") else out)
+    return [buf[offs[i]:offs[i + 1]] for i in range(count)]
 
 
 def compress_bound(n: int, block_bytes: int = 900000) -> int:

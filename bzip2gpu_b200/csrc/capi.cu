@@ -217,6 +217,43 @@ int bz2g_compress_device_into(const uint8_t *d_in, size_t n, int level, int bloc
 
 void bz2g_free(void *p) { std::free(p); }
 
+size_t bz2g_compress_batch_bound(int count, const size_t *sizes, const int *levels,
+                                 const int *block_bytes) {
+  size_t tot = 0;
+  for (int i = 0; i < count; i++) {
+    int bb = block_bytes && block_bytes[i] > 0 ? block_bytes[i]
+                                               : 100000 * std::min(std::max(levels[i], 1), 9);
+    size_t nb = (sizes[i] + bb - 1) / bb;
+    tot += stream_bound((int64_t)sizes[i], (int64_t)nb);
+  }
+  return tot + 64;
+}
+
+int bz2g_compress_batch(int count, const uint8_t *const *inputs, const size_t *sizes,
+                        const int *levels, const int *block_bytes, int on_device, uint8_t *out,
+                        size_t cap, size_t *offsets) {
+  return guard([&] {
+    BZ_REQUIRE(count >= 0 && (count == 0 || (inputs && sizes && levels)) && out && offsets,
+               kErrArg, "bad arguments");
+    std::vector<Compressor::Item> items(count);
+    int64_t maxb = 1;
+    for (int i = 0; i < count; i++) {
+      const int lvl = std::min(std::max(levels[i], 1), 9);
+      const int bb = block_bytes && block_bytes[i] > 0 ? block_bytes[i] : 100000 * lvl;
+      BZ_REQUIRE(bb <= (1 << 24), kErrArg, "block_bytes above 16 MiB");
+      items[i] = {inputs[i], (int64_t)sizes[i], lvl, bb};
+      maxb = std::max<int64_t>(maxb, bb);
+    }
+    Compressor &c = engine_for(maxb);
+    ByteSink sink(out, cap);
+    std::vector<size_t> offs;
+    g_last_stats = StageTimes();
+    const_cast<CompressorConfig &>(c.config()).time_stages = g_timing;
+    c.compress_batch(items.data(), count, on_device != 0, sink, offs, &g_last_stats);
+    for (int i = 0; i <= count; i++) offsets[i] = offs[i];
+  });
+}
+
 int bz2g_set_timing(int on) {
   std::lock_guard<std::mutex> g(g_eng_mu);
   g_timing = on != 0;

@@ -351,4 +351,205 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
   if (times) *times = tsum;
 }
 
+
+// ------------------------------------------------------------ batched form
+void Compressor::compress_batch(const Item *items, int count, bool on_device, ByteSink &out,
+                                std::vector<size_t> &offsets, StageTimes *times) {
+  struct Blk {
+    int item, k;
+    const uint8_t *ptr;
+    int len;
+    int64_t arena_word = 0, bits = 0;
+    uint32_t crc = 0;
+  };
+  std::vector<Blk> blks;
+  int64_t ntot = 0;
+  for (int i = 0; i < count; i++) {
+    const Item &it = items[i];
+    BZ_REQUIRE(it.n >= 0 && (it.n == 0 || it.ptr), kErrArg, "bad batch item");
+    BZ_REQUIRE(it.block_bytes > 0 && it.block_bytes <= cfg_.max_block_bytes, kErrArg,
+               "batch item block size outside (0, max_block_bytes]");
+    for (int64_t o = 0, k = 0; o < it.n; o += it.block_bytes, k++)
+      blks.push_back({i, (int)k, it.ptr + o, (int)std::min<int64_t>(it.block_bytes, it.n - o)});
+    ntot += it.n;
+  }
+  const int nb = (int)blks.size();
+  // the work queue: longest blocks first, so slabs hold similar lengths
+  std::vector<int> order(nb);
+  for (int i = 0; i < nb; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return blks[a].len > blks[b].len; });
+  const int B = cfg_.slab_blocks;
+  const int nslabs = (nb + B - 1) / B;
+  // arena: every block's bits, word-aligned
+  int64_t arena_words = 16;
+  for (const Blk &b : blks) arena_words += (int64_t)(stream_bound(b.len, 1) + 3) / 4 + 1;
+  uint32_t *arena = nullptr;
+  BZ_CUDA(cudaMalloc((void **)&arena, sizeof(uint32_t) * arena_words));
+  struct Free {
+    void *p;
+    ~Free() {
+      if (p) cudaFree(p);
+    }
+  } free_arena{arena};
+
+  std::mutex mu;
+  std::exception_ptr err;
+  std::atomic<int> next_slab{0};
+  int64_t arena_used = 0;
+  StageTimes tsum;
+
+  auto work = [&](Worker &w) {
+    BZ_CUDA(cudaSetDevice(device_));
+    SlabPlan plan;
+    std::vector<int> lens(B);
+    for (;;) {
+      {
+        std::lock_guard<std::mutex> g(mu);
+        if (err) return;
+      }
+      const int k = next_slab.fetch_add(1);
+      if (k >= nslabs) return;
+      const int s0 = k * B, ns = std::min(B, nb - s0);
+      for (int i = 0; i < ns; i++) lens[i] = blks[order[s0 + i]].len;
+      plan.build(lens.data(), ns);
+      w.ws->upload_plan(plan, w.st);
+      const SlabDev &d = w.ws->dev;
+      const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+      for (int i = 0; i < ns; i++)
+        BZ_CUDA(cudaMemcpyAsync(d.raw + plan.raw_off[i], blks[order[s0 + i]].ptr, lens[i], kind,
+                                w.st));
+      w.ws->dev.kt_on = 0;
+      stage_rle1_crc(d, w.st);
+      stage_bwt(d, plan.max_m_bound, w.st);
+      stage_mtf(d, w.st);
+      stage_rle2(d, w.st);
+      stage_huffman(d, w.st);
+      stage_sizes(d, w.st);
+      BZ_CUDA(cudaMemcpyAsync(w.h_sizes, d.hdr_bits, sizeof(int64_t) * ns, cudaMemcpyDeviceToHost,
+                              w.st));
+      BZ_CUDA(cudaMemcpyAsync(w.h_sizes + B, d.pay_bits, sizeof(int64_t) * ns,
+                              cudaMemcpyDeviceToHost, w.st));
+      BZ_CUDA(cudaMemcpyAsync(w.h_crc, d.crc, sizeof(uint32_t) * ns, cudaMemcpyDeviceToHost, w.st));
+      if (times) {
+        BZ_CUDA(cudaMemcpyAsync(w.h_cnt, d.m, 4 * ns, cudaMemcpyDeviceToHost, w.st));
+        BZ_CUDA(cudaMemcpyAsync(w.h_cnt + B, d.s, 4 * ns, cudaMemcpyDeviceToHost, w.st));
+        BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 2 * B, d.n_sel, 4 * ns, cudaMemcpyDeviceToHost, w.st));
+        BZ_CUDA(cudaMemcpyAsync(w.h_act, d.active_sum, 8 * ns, cudaMemcpyDeviceToHost, w.st));
+      }
+      BZ_CUDA(cudaStreamSynchronize(w.st));
+      int64_t words = 0;
+      int64_t base;
+      {
+        std::lock_guard<std::mutex> g(mu);
+        for (int i = 0; i < ns; i++) words += (w.h_sizes[i] + w.h_sizes[B + i] + 31) / 32;
+        base = arena_used;
+        arena_used += words;
+        BZ_REQUIRE(arena_used <= arena_words, kErrInternal, "batch arena overflow");
+        int64_t at = base;
+        for (int i = 0; i < ns; i++) {
+          Blk &bk = blks[order[s0 + i]];
+          const int64_t bits = w.h_sizes[i] + w.h_sizes[B + i];
+          bk.arena_word = at;
+          bk.bits = bits;
+          bk.crc = w.h_crc[i];
+          at += (bits + 31) / 32;
+        }
+        if (times)
+          for (int i = 0; i < ns; i++) {
+            tsum.blocks++;
+            tsum.n += lens[i];
+            tsum.m += w.h_cnt[i];
+            tsum.s += w.h_cnt[B + i];
+            tsum.g += w.h_cnt[2 * B + i];
+            tsum.A += w.h_act[i];
+            tsum.bits += w.h_sizes[B + i];
+          }
+      }
+      // block starts (bits) in the arena, staged through the sizes buffer
+      for (int i = 0; i < ns; i++) w.h_sizes[i] = blks[order[s0 + i]].arena_word * 32;
+      BZ_CUDA(cudaMemcpyAsync(d.blk_start, w.h_sizes, sizeof(int64_t) * ns, cudaMemcpyHostToDevice,
+                              w.st));
+      stage_place_arena(d, arena, base, words, w.st);
+      BZ_CUDA(cudaStreamSynchronize(w.st));
+    }
+  };
+
+  if (nslabs > 0) {
+    const int nw = std::min<int>((int)workers_.size(), nslabs);
+    std::vector<std::thread> th;
+    auto guarded = [&](Worker &w) {
+      try {
+        work(w);
+      } catch (...) {
+        std::lock_guard<std::mutex> g(mu);
+        if (!err) err = std::current_exception();
+      }
+    };
+    for (int i = 1; i < nw; i++) th.emplace_back(guarded, std::ref(*workers_[i]));
+    guarded(*workers_[0]);
+    for (auto &t : th) t.join();
+    if (err) std::rethrow_exception(err);
+  }
+
+  // stream layout: item i occupies [offsets[i], offsets[i+1]) of the output
+  const size_t base = out.size;
+  offsets.assign(count + 1, base);
+  std::vector<int64_t> first_blk(count + 1, 0);
+  for (int i = 0, b = 0; i < count; i++) {
+    first_blk[i] = b;
+    while (b < nb && blks[b].item == i) b++;
+    first_blk[i + 1] = b;
+  }
+  std::vector<int64_t> h_src(std::max(nb, 1)), h_dst(std::max(nb, 1)), h_bits(std::max(nb, 1));
+  std::vector<int64_t> end_bit(count);
+  std::vector<uint32_t> scrc(count, 0);
+  size_t pos = 0;  // bytes from base
+  for (int i = 0; i < count; i++) {
+    int64_t bit = 32;
+    for (int64_t b = first_blk[i]; b < first_blk[i + 1]; b++) {
+      h_src[b] = blks[b].arena_word;
+      h_dst[b] = (int64_t)pos * 8 + bit;
+      h_bits[b] = blks[b].bits;
+      bit += blks[b].bits;
+      scrc[i] = ((scrc[i] << 1) | (scrc[i] >> 31)) ^ blks[b].crc;
+    }
+    end_bit[i] = bit;
+    offsets[i] = base + pos;
+    pos += (size_t)((bit + 80 + 7) / 8);
+  }
+  offsets[count] = base + pos;
+  if (out.owned) out.reserve(base + pos + 8);
+  BZ_REQUIRE(base + pos <= out.cap, kErrTooLarge, "output buffer too small");
+  const int64_t owords = (int64_t)(pos + 3) / 4 + 1;
+  uint32_t *d_out = nullptr;
+  int64_t *d_meta = nullptr;
+  cudaStream_t st = workers_[0]->st;
+  BZ_CUDA(cudaMalloc((void **)&d_out, sizeof(uint32_t) * owords));
+  Free free_out{d_out};
+  BZ_CUDA(cudaMalloc((void **)&d_meta, sizeof(int64_t) * 3 * std::max(nb, 1)));
+  Free free_meta{d_meta};
+  BZ_CUDA(cudaMemsetAsync(d_out, 0, sizeof(uint32_t) * owords, st));
+  BZ_CUDA(cudaMemcpyAsync(d_meta, h_src.data(), 8 * nb, cudaMemcpyHostToDevice, st));
+  BZ_CUDA(cudaMemcpyAsync(d_meta + nb, h_dst.data(), 8 * nb, cudaMemcpyHostToDevice, st));
+  BZ_CUDA(cudaMemcpyAsync(d_meta + 2 * nb, h_bits.data(), 8 * nb, cudaMemcpyHostToDevice, st));
+  launch_splice(arena, d_meta, d_meta + nb, d_meta + 2 * nb, nb, d_out, st);
+  BZ_CUDA(cudaMemcpyAsync(out.data + base, d_out, pos, cudaMemcpyDeviceToHost, st));
+  BZ_CUDA(cudaStreamSynchronize(st));
+  out.size = base + pos;
+  // stream headers and end-of-stream markers
+  for (int i = 0; i < count; i++) {
+    int lvl = items[i].level < 1 ? 1 : (items[i].level > 9 ? 9 : items[i].level);
+    uint8_t *p = out.data + offsets[i];
+    p[0] = 'B';
+    p[1] = 'Z';
+    p[2] = 'h';
+    p[3] = (uint8_t)('0' + lvl);
+    ByteSink view(out.data + offsets[i], offsets[i + 1] - offsets[i]);
+    view.size = (size_t)((end_bit[i] + 7) / 8);
+    put_eos(view, 0, end_bit[i], scrc[i]);
+  }
+  if (times) *times = tsum;
+}
+
 }  // namespace bz2g

@@ -64,6 +64,19 @@ class Compressor {
   // Convenience for callers holding a std::vector (appends).
   void compress(const uint8_t *const *ptrs, const int *lens, int nblocks, int level,
                 std::vector<uint8_t> &out, StageTimes *times = nullptr);
+  // Batched form: every item becomes its own stream (header digit
+  // item.level, blocks of item.block_bytes raw bytes); all blocks of all
+  // items run through shared slabs in order of decreasing length, and the
+  // streams are written back to back into out (offsets: count + 1 entries).
+  // Each stream equals compress() of that item alone.
+  struct Item {
+    const uint8_t *ptr;
+    int64_t n;
+    int level;
+    int block_bytes;
+  };
+  void compress_batch(const Item *items, int count, bool on_device, ByteSink &out,
+                      std::vector<size_t> &offsets, StageTimes *times = nullptr);
   const CompressorConfig &config() const { return cfg_; }
   int device() const { return device_; }
 

@@ -140,6 +140,13 @@ void stage_place(const SlabDev &d, int64_t slab_start_bit, int64_t w0, int64_t n
 // Kernel launches issued by this library so far.
 int64_t launch_count();
 
+// Batched form: blocks placed word-aligned in an arena (d.blk_start filled by
+// the caller), then spliced to their bit positions in the output streams.
+void stage_place_arena(const SlabDev &d, uint32_t *arena, int64_t w0, int64_t nwords,
+                       cudaStream_t st);
+void launch_splice(const uint32_t *arena, const int64_t *src_word, const int64_t *dst_bit,
+                   const int64_t *nbits, int nblocks, uint32_t *out, cudaStream_t st);
+
 // Individual pieces used by the per-stage C-ABI.
 void launch_crc_only(const SlabDev &d, cudaStream_t st);
 void launch_pack_words(const SlabDev &d, uint32_t *words, cudaStream_t st);

@@ -370,6 +370,54 @@ void stage_place(const SlabDev &d, int64_t slab_start_bit, int64_t w0, int64_t n
   BZ_LAUNCH_CHECK();
 }
 
+// Blocks at word-aligned places of their own in `arena` (d.blk_start already
+// holds each block's first bit); zeroes arena words [w0, w0 + nwords) first.
+void stage_place_arena(const SlabDev &d, uint32_t *arena, int64_t w0, int64_t nwords,
+                       cudaStream_t st) {
+  BZ_CUDA(cudaMemsetAsync(arena + w0, 0, sizeof(uint32_t) * nwords, st));
+  SlabDev a = d;
+  a.out = arena;
+  k_write_header<<<a.nblocks, kHdrThreads, 0, st>>>(a, 0);
+  BZ_LAUNCH_CHECK();
+  k_write_payload<<<a.n_group_tiles, kGroupTile, 0, st>>>(a, 0);
+  BZ_LAUNCH_CHECK();
+}
+
+// Copy each block's bits (word-aligned in the arena) to its bit position in
+// the output streams; the output is zeroed, and the first and last word of a
+// block are OR-ed in because neighbours share them.
+__global__ void __launch_bounds__(256) k_splice(const uint32_t *arena, const int64_t *src_word,
+                                                const int64_t *dst_bit, const int64_t *nbits,
+                                                uint32_t *out) {
+  const int b = blockIdx.x;
+  const int64_t L = nbits[b];
+  if (L <= 0) return;
+  const int64_t D = dst_bit[b];
+  const uint32_t *src = arena + src_word[b];
+  const int64_t srcw = (L + 31) >> 5;
+  const int64_t w_first = D >> 5, w_last = (D + L - 1) >> 5;
+  for (int64_t w = w_first + threadIdx.x; w <= w_last; w += blockDim.x) {
+    const int64_t s = w * 32 - D;  // source bit of this word's first bit
+    const int64_t a = s >= 0 ? s >> 5 : -1;
+    const int sh = (int)(s - a * 32);
+    const uint32_t x0 = (a >= 0 && a < srcw) ? bswap32(src[a]) : 0u;
+    const uint32_t x1 = (a + 1 >= 0 && a + 1 < srcw) ? bswap32(src[a + 1]) : 0u;
+    const uint32_t v = sh == 0 ? x0 : ((x0 << sh) | (x1 >> (32 - sh)));
+    if (w == w_first || w == w_last) {
+      if (v) atomicOr(out + w, bswap32(v));
+    } else {
+      out[w] = bswap32(v);
+    }
+  }
+}
+
+void launch_splice(const uint32_t *arena, const int64_t *src_word, const int64_t *dst_bit,
+                   const int64_t *nbits, int nblocks, uint32_t *out, cudaStream_t st) {
+  if (nblocks <= 0) return;
+  k_splice<<<nblocks, 256, 0, st>>>(arena, src_word, dst_bit, nbits, out);
+  BZ_LAUNCH_CHECK();
+}
+
 void launch_pack_words(const SlabDev &d, uint32_t *words, cudaStream_t st) {
   k_pack_words<<<d.n_group_tiles, kGroupTile, 0, st>>>(d, words);
   BZ_LAUNCH_CHECK();

@@ -62,6 +62,20 @@ int bz2g_compress_device_into(const uint8_t *d_in, size_t n, int level, int bloc
 size_t bz2g_compress_bound(size_t n, int block_bytes);
 void bz2g_free(void *p);
 
+/* Batched form: `count` independent inputs, each compressed into its own
+ * .bz2 stream (header digit levels[i], blocks of block_bytes[i] raw bytes,
+ * or levels[i] * 100000 when block_bytes is NULL or the entry is 0).  All
+ * blocks of all inputs share the GPU in one length-ordered queue; stream i is
+ * written to out[offsets[i], offsets[i+1]) and equals bz2g_compress of input
+ * i alone.  inputs are host pointers, or device pointers if on_device.
+ * No counterpart in the reference (it compresses one stream per call,
+ * include/compression.h:86-87). */
+int bz2g_compress_batch(int count, const uint8_t *const *inputs, const size_t *sizes,
+                        const int *levels, const int *block_bytes, int on_device, uint8_t *out,
+                        size_t cap, size_t *offsets);
+size_t bz2g_compress_batch_bound(int count, const size_t *sizes, const int *levels,
+                                 const int *block_bytes);
+
 /* Engine shape used by the whole-stream calls on this thread's device:
  * blocks per slab and worker streams.  0 keeps the current value. */
 int bz2g_set_engine(int slab_blocks, int workers);
