@@ -21,6 +21,7 @@ on a bounded sample of the same workload with all host threads.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -29,6 +30,8 @@ import sys
 import threading
 import time
 from pathlib import Path
+
+import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
@@ -169,6 +172,69 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def run_batch(args):
+    """Batched form vs plain form on the many-inputs workload: inputs of
+    log-uniform size 1 KiB .. 8 MiB, alphabet 2..256, alpha 0.05 .. 5, level
+    1..9 (blocks of level * 100,000 bytes), 1 % runs; inputs resident in HBM,
+    streams delivered to page-locked host memory."""
+    world, rank, local = dist_setup(args.gpus)
+    import torch
+
+    import bzip2gpu_b200 as B
+    import bzip2gpu_b200.workloads as W
+
+    items = W.batch_inputs(count=args.batch_count, seed=0xB2C2 + 7919 * rank)
+    sizes = [x.data.size for x in items]
+    levels = [x.level for x in items]
+    total = sum(sizes)
+    flat = torch.from_numpy(np.concatenate([x.data for x in items])).cuda()
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    d_in = [flat[offs[i]:offs[i + 1]] for i in range(len(items))]
+    cap = B.lib().bz2g_compress_batch_bound(len(items), (ctypes.c_size_t * len(items))(*sizes),
+                                           (ctypes.c_int * len(items))(*levels), None)
+    h_out = torch.empty(cap, dtype=torch.uint8, pin_memory=True)
+    B.set_timing(False)
+
+    def plain():
+        n = 0
+        for x, lv in zip(d_in, levels):
+            n += B.compress_device_into(x, h_out[n:], lv, lv * 100000)
+        return n
+
+    def batched():
+        st = B.compress_batch(d_in, levels, out=h_out, on_device=True)
+        return sum(len(v) for v in st)
+
+    ref = [bytes(s) for s in B.compress_batch(d_in, levels, on_device=True)]
+    for _ in range(args.warmup):
+        plain()
+        batched()
+    res = {}
+    for name, fn in (("plain", plain), ("batched", batched)):
+        barrier(world)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            nbytes = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        dt = max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
+        res[name] = {"MB/s": round(total * world * args.steps / dt / 1e6, 2),
+                     "ms_per_step": round(dt / args.steps * 1e3, 2), "stream_bytes": int(nbytes)}
+    # the batched streams are the per-input streams
+    for i, (x, lv) in enumerate(zip(d_in, levels)):
+        k = B.compress_device_into(x, h_out, lv, lv * 100000)
+        assert bytes(h_out[:k].numpy()) == ref[i]
+    if rank == 0:
+        print(json.dumps({"workload": "many inputs (1 KiB..8 MiB; levels 1..9)",
+                          "inputs": len(items), "bytes": int(total), "n_gpus": world,
+                          "steps": args.steps, "warmup": args.warmup, "forms": res,
+                          "batched_over_plain": round(res["batched"]["MB/s"] / res["plain"]["MB/s"], 3),
+                          "bit_exact": True}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -180,9 +246,13 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--slab", type=int, default=0)
     ap.add_argument("--workers", type=int, default=0)
+    ap.add_argument("--workload", default="large", choices=["large", "batch"])
+    ap.add_argument("--batch-count", type=int, default=2048)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch":
+        return run_batch(args)
 
     world, rank, local = dist_setup(args.gpus)
     import torch
@@ -225,6 +295,11 @@ def main():
     assert olen == len(out) and bytes(h_out[:olen].numpy()) == out
     launches = (B.launch_count() - l0) // max(args.steps, 1)
     stats = B.last_stats()
+    # the batched form on the same stream (one input: blocks in one queue)
+    bt, bout = timed(lambda: B.compress_batch([d_in], [9], [900000], out=h_out, on_device=True))
+    assert bytes(bout[0]) == out
+    bt = max_over_ranks(bt, world)
+    batched_value = n * world * args.steps / bt / 1e6
     dt = max_over_ranks(dt, world)
     value = n * world * args.steps / dt / 1e6
 
@@ -289,6 +364,8 @@ def main():
                        "level": 9, "form": "plain", "l2": "input larger than L2",
                        "blocks": int(stats["blocks"]), "ratio": round(ratio, 4)},
             "e2e": e2e, "roofline": roof, "pipeline_roofline": pipeline, "cpu_baseline": cpu,
+            "forms": {"plain": round(value, 2), "batched": round(batched_value, 2),
+                      "learned": None},
             "clocks": clk.summary(), "gpu_launches": int(launches),
             "stats": {k: stats[k] for k in ("n", "m", "A", "s", "g", "bits")},
             "stage_ms_sum_over_slabs_last_step": stage_ms,

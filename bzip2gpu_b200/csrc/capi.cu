@@ -99,25 +99,32 @@ int g_slab = 128, g_workers = 3;
 bool g_timing = false;
 thread_local StageTimes g_last_stats;
 
+// The device's engine if its shape matches and its blocks are large enough;
+// otherwise a new one (at least 900,000-byte blocks) replaces it.
 Compressor &engine_for(int64_t block_bytes) {
   int dev = 0;
   BZ_CUDA(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> g(g_eng_mu);
-  EngineKey k{dev, g_slab, g_workers, block_bytes};
-  auto it = g_engines.find(k);
-  if (it != g_engines.end()) return *it->second;
-  // one engine per device: drop engines of other shapes on this device
+  for (auto &e : g_engines)
+    if (e.first.dev == dev && e.first.slab == g_slab && e.first.workers == g_workers &&
+        e.first.maxb >= block_bytes)
+      return *e.second;
+  int64_t maxb = std::max<int64_t>(block_bytes, 900000);
   for (auto i = g_engines.begin(); i != g_engines.end();) {
-    if (i->first.dev == dev) i = g_engines.erase(i);
-    else ++i;
+    if (i->first.dev == dev) {
+      maxb = std::max<int64_t>(maxb, i->first.maxb);
+      i = g_engines.erase(i);
+    } else {
+      ++i;
+    }
   }
   CompressorConfig cfg;
   cfg.slab_blocks = g_slab;
   cfg.workers = g_workers;
-  cfg.max_block_bytes = block_bytes;
+  cfg.max_block_bytes = maxb;
   auto c = std::make_unique<Compressor>(cfg);
   Compressor &ref = *c;
-  g_engines[k] = std::move(c);
+  g_engines[EngineKey{dev, g_slab, g_workers, maxb}] = std::move(c);
   return ref;
 }
 

@@ -75,7 +75,32 @@ Compressor::Compressor(const CompressorConfig &cfg) : cfg_(cfg) {
   }
 }
 
-Compressor::~Compressor() = default;
+Compressor::~Compressor() {
+  for (uint32_t *c : arena_chunks_) cudaFree(c);
+}
+
+// A run of `words` arena words for one slab (caller holds the batch lock):
+// the current chunk if it has room, else the next one, allocated once and
+// kept for later calls.
+uint32_t *Compressor::arena_take(int64_t words, size_t *chunk, int64_t *used, int64_t *base) {
+  const int64_t cw = std::max<int64_t>(kArenaChunkWords, words);
+  if (*chunk < arena_chunks_.size() && *used + words > arena_chunk_words_[*chunk]) {
+    (*chunk)++;
+    *used = 0;
+  }
+  while (*chunk < arena_chunks_.size() && words > arena_chunk_words_[*chunk]) (*chunk)++;
+  if (*chunk >= arena_chunks_.size()) {
+    uint32_t *p = nullptr;
+    BZ_CUDA(cudaMalloc((void **)&p, sizeof(uint32_t) * cw));
+    arena_chunks_.push_back(p);
+    arena_chunk_words_.push_back(cw);
+    *chunk = arena_chunks_.size() - 1;
+    *used = 0;
+  }
+  *base = *used;
+  *used += words;
+  return arena_chunks_[*chunk];
+}
 
 ByteSink::ByteSink(uint8_t *p, size_t c) : data(p), size(0), cap(c), owned(false) {
   cudaPointerAttributes a;
@@ -153,6 +178,7 @@ void Compressor::compress(const uint8_t *const *ptrs, const int *lens, int nbloc
 
 void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, int level,
                      bool on_device, ByteSink &out, StageTimes *times) {
+  std::lock_guard<std::mutex> call_lock(call_mu_);
   int64_t ntot = 0;
   for (int b = 0; b < nblocks; b++) {
     BZ_REQUIRE(lens[b] > 0 && lens[b] <= cfg_.max_block_bytes, kErrArg,
@@ -355,11 +381,13 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
 // ------------------------------------------------------------ batched form
 void Compressor::compress_batch(const Item *items, int count, bool on_device, ByteSink &out,
                                 std::vector<size_t> &offsets, StageTimes *times) {
+  std::lock_guard<std::mutex> call_lock(call_mu_);
   struct Blk {
     int item, k;
     const uint8_t *ptr;
     int len;
     int64_t arena_word = 0, bits = 0;
+    const uint32_t *src = nullptr;
     uint32_t crc = 0;
   };
   std::vector<Blk> blks;
@@ -381,22 +409,13 @@ void Compressor::compress_batch(const Item *items, int count, bool on_device, By
                    [&](int a, int b) { return blks[a].len > blks[b].len; });
   const int B = cfg_.slab_blocks;
   const int nslabs = (nb + B - 1) / B;
-  // arena: every block's bits, word-aligned
-  int64_t arena_words = 16;
-  for (const Blk &b : blks) arena_words += (int64_t)(stream_bound(b.len, 1) + 3) / 4 + 1;
-  uint32_t *arena = nullptr;
-  BZ_CUDA(cudaMalloc((void **)&arena, sizeof(uint32_t) * arena_words));
-  struct Free {
-    void *p;
-    ~Free() {
-      if (p) cudaFree(p);
-    }
-  } free_arena{arena};
+  // arena: every block's bits, word-aligned, in chunks kept by the engine
+  size_t chunk = 0;
+  int64_t chunk_used = 0;
 
   std::mutex mu;
   std::exception_ptr err;
   std::atomic<int> next_slab{0};
-  int64_t arena_used = 0;
   StageTimes tsum;
 
   auto work = [&](Worker &w) {
@@ -416,9 +435,18 @@ void Compressor::compress_batch(const Item *items, int count, bool on_device, By
       w.ws->upload_plan(plan, w.st);
       const SlabDev &d = w.ws->dev;
       const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-      for (int i = 0; i < ns; i++)
-        BZ_CUDA(cudaMemcpyAsync(d.raw + plan.raw_off[i], blks[order[s0 + i]].ptr, lens[i], kind,
+      // one copy per run of blocks that are adjacent both in the source and in
+      // the slab (16-byte multiples)
+      for (int i = 0; i < ns;) {
+        int j = i + 1;
+        while (j < ns && blks[order[s0 + j]].ptr == blks[order[s0 + j - 1]].ptr + lens[j - 1] &&
+               plan.raw_off[j] == plan.raw_off[j - 1] + lens[j - 1])
+          j++;
+        const int64_t bytes = plan.raw_off[j - 1] + lens[j - 1] - plan.raw_off[i];
+        BZ_CUDA(cudaMemcpyAsync(d.raw + plan.raw_off[i], blks[order[s0 + i]].ptr, bytes, kind,
                                 w.st));
+        i = j;
+      }
       w.ws->dev.kt_on = 0;
       stage_rle1_crc(d, w.st);
       stage_bwt(d, plan.max_m_bound, w.st);
@@ -440,17 +468,17 @@ void Compressor::compress_batch(const Item *items, int count, bool on_device, By
       BZ_CUDA(cudaStreamSynchronize(w.st));
       int64_t words = 0;
       int64_t base;
+      uint32_t *arena;
       {
         std::lock_guard<std::mutex> g(mu);
         for (int i = 0; i < ns; i++) words += (w.h_sizes[i] + w.h_sizes[B + i] + 31) / 32;
-        base = arena_used;
-        arena_used += words;
-        BZ_REQUIRE(arena_used <= arena_words, kErrInternal, "batch arena overflow");
+        arena = arena_take(words, &chunk, &chunk_used, &base);
         int64_t at = base;
         for (int i = 0; i < ns; i++) {
           Blk &bk = blks[order[s0 + i]];
           const int64_t bits = w.h_sizes[i] + w.h_sizes[B + i];
           bk.arena_word = at;
+          bk.src = arena + at;
           bk.bits = bits;
           bk.crc = w.h_crc[i];
           at += (bits + 31) / 32;
@@ -492,6 +520,12 @@ void Compressor::compress_batch(const Item *items, int count, bool on_device, By
     if (err) std::rethrow_exception(err);
   }
 
+  struct Free {
+    void *p;
+    ~Free() {
+      if (p) cudaFree(p);
+    }
+  };
   // stream layout: item i occupies [offsets[i], offsets[i+1]) of the output
   const size_t base = out.size;
   offsets.assign(count + 1, base);
@@ -508,7 +542,7 @@ void Compressor::compress_batch(const Item *items, int count, bool on_device, By
   for (int i = 0; i < count; i++) {
     int64_t bit = 32;
     for (int64_t b = first_blk[i]; b < first_blk[i + 1]; b++) {
-      h_src[b] = blks[b].arena_word;
+      h_src[b] = (int64_t)(uintptr_t)blks[b].src;
       h_dst[b] = (int64_t)pos * 8 + bit;
       h_bits[b] = blks[b].bits;
       bit += blks[b].bits;
@@ -533,7 +567,7 @@ void Compressor::compress_batch(const Item *items, int count, bool on_device, By
   BZ_CUDA(cudaMemcpyAsync(d_meta, h_src.data(), 8 * nb, cudaMemcpyHostToDevice, st));
   BZ_CUDA(cudaMemcpyAsync(d_meta + nb, h_dst.data(), 8 * nb, cudaMemcpyHostToDevice, st));
   BZ_CUDA(cudaMemcpyAsync(d_meta + 2 * nb, h_bits.data(), 8 * nb, cudaMemcpyHostToDevice, st));
-  launch_splice(arena, d_meta, d_meta + nb, d_meta + 2 * nb, nb, d_out, st);
+  launch_splice(d_meta, d_meta + nb, d_meta + 2 * nb, nb, d_out, st);
   BZ_CUDA(cudaMemcpyAsync(out.data + base, d_out, pos, cudaMemcpyDeviceToHost, st));
   BZ_CUDA(cudaStreamSynchronize(st));
   out.size = base + pos;

@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <memory>
+#include <mutex>
 #include <vector>
 
 namespace bz2g {
@@ -84,9 +85,14 @@ class Compressor {
   struct Worker;
   void run(const uint8_t *const *ptrs, const int *lens, int nblocks, int level, bool on_device,
            ByteSink &out, StageTimes *times);
+  uint32_t *arena_take(int64_t words, size_t *chunk, int64_t *used, int64_t *base);
+  static constexpr int64_t kArenaChunkWords = int64_t(1) << 28;  // 1 GiB
   CompressorConfig cfg_;
   int device_ = 0;
   std::vector<std::unique_ptr<Worker>> workers_;
+  std::mutex call_mu_;                         // one call at a time per engine
+  std::vector<uint32_t *> arena_chunks_;       // batched form: block bits
+  std::vector<int64_t> arena_chunk_words_;
 };
 
 // Upper bound of the stream size for n bytes in nblocks blocks.

@@ -144,8 +144,9 @@ int64_t launch_count();
 // the caller), then spliced to their bit positions in the output streams.
 void stage_place_arena(const SlabDev &d, uint32_t *arena, int64_t w0, int64_t nwords,
                        cudaStream_t st);
-void launch_splice(const uint32_t *arena, const int64_t *src_word, const int64_t *dst_bit,
-                   const int64_t *nbits, int nblocks, uint32_t *out, cudaStream_t st);
+// src_addr: device address of each block's first word.
+void launch_splice(const int64_t *src_addr, const int64_t *dst_bit, const int64_t *nbits,
+                   int nblocks, uint32_t *out, cudaStream_t st);
 
 // Individual pieces used by the per-stage C-ABI.
 void launch_crc_only(const SlabDev &d, cudaStream_t st);

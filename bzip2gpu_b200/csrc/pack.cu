@@ -386,14 +386,13 @@ void stage_place_arena(const SlabDev &d, uint32_t *arena, int64_t w0, int64_t nw
 // Copy each block's bits (word-aligned in the arena) to its bit position in
 // the output streams; the output is zeroed, and the first and last word of a
 // block are OR-ed in because neighbours share them.
-__global__ void __launch_bounds__(256) k_splice(const uint32_t *arena, const int64_t *src_word,
-                                                const int64_t *dst_bit, const int64_t *nbits,
-                                                uint32_t *out) {
+__global__ void __launch_bounds__(256) k_splice(const int64_t *src_addr, const int64_t *dst_bit,
+                                                const int64_t *nbits, uint32_t *out) {
   const int b = blockIdx.x;
   const int64_t L = nbits[b];
   if (L <= 0) return;
   const int64_t D = dst_bit[b];
-  const uint32_t *src = arena + src_word[b];
+  const uint32_t *src = reinterpret_cast<const uint32_t *>(src_addr[b]);
   const int64_t srcw = (L + 31) >> 5;
   const int64_t w_first = D >> 5, w_last = (D + L - 1) >> 5;
   for (int64_t w = w_first + threadIdx.x; w <= w_last; w += blockDim.x) {
@@ -411,10 +410,10 @@ __global__ void __launch_bounds__(256) k_splice(const uint32_t *arena, const int
   }
 }
 
-void launch_splice(const uint32_t *arena, const int64_t *src_word, const int64_t *dst_bit,
-                   const int64_t *nbits, int nblocks, uint32_t *out, cudaStream_t st) {
+void launch_splice(const int64_t *src_addr, const int64_t *dst_bit, const int64_t *nbits,
+                   int nblocks, uint32_t *out, cudaStream_t st) {
   if (nblocks <= 0) return;
-  k_splice<<<nblocks, 256, 0, st>>>(arena, src_word, dst_bit, nbits, out);
+  k_splice<<<nblocks, 256, 0, st>>>(src_addr, dst_bit, nbits, out);
   BZ_LAUNCH_CHECK();
 }
 
