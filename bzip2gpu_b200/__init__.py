@@ -22,11 +22,13 @@ __all__ = [
     "Bz2gError", "lib", "lib_path", "compress", "compress_device", "compress_bound",
     "set_engine", "compress_into", "compress_device_into", "compress_batch", "rle1", "crc32", "bwt", "mtf", "symbols_table", "rle2", "huffman_build",
     "huffman_encode", "count_frequencies", "gen_markov", "gen_uniform", "MAX_GROUPS",
-    "MAX_ALPHA",
+    "MAX_ALPHA", "SELECTOR_PARAMS", "selector_load", "set_selector", "get_selector",
+    "selector_logits", "huffman_build_learned", "selector_dataset",
 ]
 
 MAX_GROUPS = 6
 MAX_ALPHA = 258
+SELECTOR_PARAMS = 139792
 _LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libbz2gpu_b200.so"
 _lib = None
 
@@ -61,6 +63,22 @@ _SIGS = {
     "bz2g_gen_markov": (_i, [_c.c_uint64, _vp, _i, _c.c_double, _c.c_double, _i, _i, _vp,
                              _c.c_int64, _i, _vp]),
     "bz2g_gen_uniform": (_i, [_c.c_uint64, _vp, _c.c_int64, _i, _vp]),
+    "bz2g_selector_load": (_i, [_vp, _sz]),
+    "bz2g_set_selector": (_i, [_i]),
+    "bz2g_get_selector": (_i, []),
+    "bz2g_selector_logits": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
+    "bz2g_huffman_build_learned": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _c.POINTER(_i),
+                                        _c.POINTER(_i), _vp]),
+    "bz2g_selector_dataset": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _c.c_int64,
+                                   _c.POINTER(_c.c_int64)]),
+    "bz2g_mlp_features": (_i, [_vp, _c.c_int64, _vp, _vp, _vp]),
+    "bz2g_mlp_work_bytes": (_sz, [_i]),
+    "bz2g_mlp_grads": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "bz2g_mlp_forward": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp, _vp]),
+    "bz2g_mlp_adam": (_i, [_vp, _vp, _vp, _vp, _vp, _c.c_float, _c.c_float, _c.c_float,
+                           _c.c_float, _i, _vp]),
+    "bz2g_mlp_to_bf16": (_i, [_vp, _vp, _vp]),
+    "bz2g_mlp_status": (_i, [_vp]),
 }
 
 
@@ -220,7 +238,7 @@ def set_timing(on: bool) -> None:
 
 STAT_FIELDS = ("blocks", "n", "m", "A", "s", "g", "bits", "ms_rle1", "ms_bwt", "ms_mtf",
                "ms_rle2", "ms_huffman", "ms_sizes", "ms_place", "scatter_launches",
-               "scatter_ms", "scatter_bytes")
+               "scatter_ms", "scatter_bytes", "learned_blocks")
 
 
 def last_stats() -> dict:
@@ -370,3 +388,72 @@ def gen_uniform(n: int, seed: int, out=None, device: bool = False, stream=None):
     _check(lib().bz2g_gen_uniform(seed & (2**64 - 1), ptr, n, int(on_dev),
                                   _stream(stream) if on_dev else None))
     return out
+
+
+# ------------------------------------------------- learned table selector
+def selector_load(params) -> None:
+    """Load selector parameters (flat fp32, SELECTOR_PARAMS values; layout in
+    include/bz2g.h) on the current device."""
+    p = np.ascontiguousarray(params, dtype=np.float32).reshape(-1)
+    _check(lib().bz2g_selector_load(p.ctypes.data, p.size))
+
+
+def set_selector(mode) -> None:
+    """Table selector of the whole-stream calls: "plain" (0, the reference's),
+    "learned" (1) or "one_pass" (2: the plain selector with a single
+    selection pass, the learned form's measurement baseline)."""
+    m = {"plain": 0, "learned": 1, "one_pass": 2}.get(mode, mode)
+    _check(lib().bz2g_set_selector(int(m)))
+
+
+def get_selector() -> str:
+    return ("plain", "learned", "one_pass")[lib().bz2g_get_selector()]
+
+
+def selector_logits(d_syms, d_params, stream=None):
+    """The fused tensor-core selector over a symbol stream treated as one
+    six-table block: (logits [groups, 6] float32 tensor, choices uint8 tensor)."""
+    import torch
+    s = d_syms.numel()
+    g = (s + 49) // 50
+    lg = torch.empty((g, 6), dtype=torch.float32, device=d_syms.device)
+    sel = torch.empty(g, dtype=torch.uint8, device=d_syms.device)
+    _check(lib().bz2g_selector_logits(_ptr(d_syms), s, _ptr(d_params), _ptr(lg), _ptr(sel),
+                                      _stream(stream)))
+    return lg, sel
+
+
+def huffman_build_learned(d_syms, n_in_use: int, d_params, stream=None):
+    """huffman_build with the learned selector: (len, code, selectors, n_groups,
+    the MLP's own choices)."""
+    s = d_syms.numel()
+    ln = np.zeros((MAX_GROUPS, MAX_ALPHA), np.uint8)
+    code = np.zeros((MAX_GROUPS, MAX_ALPHA), np.int32)
+    nsel = max((s + 49) // 50, 1)
+    sel = np.zeros(nsel, np.uint8)
+    msel = np.zeros(nsel, np.uint8)
+    ns, ng = _i(), _i()
+    _check(lib().bz2g_huffman_build_learned(_ptr(d_syms), s, n_in_use, _ptr(d_params),
+                                            ln.ctypes.data, code.ctypes.data, sel.ctypes.data,
+                                            msel.ctypes.data, ctypes.byref(ns), ctypes.byref(ng),
+                                            _stream(stream)))
+    return ln, code, sel[: ns.value], ng.value, msel[: ns.value]
+
+
+def selector_dataset(d_inputs, levels, cap: int):
+    """Training groups of the inputs (CUDA uint8 tensors): (group symbols
+    [G, 50] uint16 tensor, plain-selector labels [G] uint8 tensor, groups
+    available)."""
+    import torch
+    n = len(d_inputs)
+    ptrs = (ctypes.c_void_p * max(n, 1))(*[t.data_ptr() for t in d_inputs])
+    sizes = (ctypes.c_size_t * max(n, 1))(*[t.numel() for t in d_inputs])
+    lv = (ctypes.c_int * max(n, 1))(*[int(x) for x in levels])
+    syms = torch.empty((cap, 50), dtype=torch.int16, device="cuda")
+    labels = torch.empty(cap, dtype=torch.uint8, device="cuda")
+    got = ctypes.c_int64()
+    _check(lib().bz2g_selector_dataset(n, ptrs, sizes, lv, _ptr(syms), _ptr(labels), cap,
+                                       ctypes.byref(got)))
+    k = min(cap, got.value)
+    return syms[:k], labels[:k], got.value
+

@@ -14,6 +14,7 @@
 #include "../../include/bz2g.h"
 #include "compressor.h"
 #include "engine.h"
+#include "selector.h"
 
 namespace bz2g {
 namespace {
@@ -99,6 +100,37 @@ int g_slab = 128, g_workers = 3;
 bool g_timing = false;
 thread_local StageTimes g_last_stats;
 
+// Learned table selector: packed weights per device and the selector mode of
+// the whole-stream calls (0 = the reference's plain selector, 1 = learned,
+// 2 = the plain selector with one selection pass, a measurement baseline).
+std::mutex g_sel_mu;
+std::map<int, uint8_t *> g_sel_packed;
+int g_sel_mode = 0;
+
+int current_passes() {
+  std::lock_guard<std::mutex> g(g_sel_mu);
+  return g_sel_mode == 2 ? 1 : kIters;
+}
+
+const uint8_t *current_selector() {
+  std::lock_guard<std::mutex> g(g_sel_mu);
+  if (g_sel_mode != 1) return nullptr;
+  int dev = 0;
+  BZ_CUDA(cudaGetDevice(&dev));
+  auto it = g_sel_packed.find(dev);
+  BZ_REQUIRE(it != g_sel_packed.end(), kErrArg,
+             "learned selector enabled but no weights loaded on this device");
+  return it->second;
+}
+
+// Packed weights from fp32 parameters in device memory (temporary buffer).
+uint8_t *pack_params(const float *d_params, cudaStream_t st) {
+  uint8_t *packed = nullptr;
+  BZ_CUDA(cudaMallocAsync((void **)&packed, mlp::kPackedBytes, st));
+  mlp::pack(d_params, packed, st);
+  return packed;
+}
+
 // The device's engine if its shape matches and its blocks are large enough;
 // otherwise a new one (at least 900,000-byte blocks) replaces it.
 Compressor &engine_for(int64_t block_bytes) {
@@ -142,6 +174,8 @@ void compress_any(const uint8_t *in, size_t n, int level, int block_bytes, bool 
   }
   Compressor &c = engine_for(std::max<int64_t>(block_bytes, 1));
   const_cast<CompressorConfig &>(c.config()).time_stages = g_timing;
+  const_cast<CompressorConfig &>(c.config()).selector = current_selector();
+  const_cast<CompressorConfig &>(c.config()).plain_passes = current_passes();
   g_last_stats = StageTimes();
   if (on_device)
     c.compress_device(ptrs.data(), lens.data(), (int)nb, level, out, &g_last_stats);
@@ -256,6 +290,8 @@ int bz2g_compress_batch(int count, const uint8_t *const *inputs, const size_t *s
     std::vector<size_t> offs;
     g_last_stats = StageTimes();
     const_cast<CompressorConfig &>(c.config()).time_stages = g_timing;
+    const_cast<CompressorConfig &>(c.config()).selector = current_selector();
+  const_cast<CompressorConfig &>(c.config()).plain_passes = current_passes();
     c.compress_batch(items.data(), count, on_device != 0, sink, offs, &g_last_stats);
     for (int i = 0; i <= count; i++) offsets[i] = offs[i];
   });
@@ -273,7 +309,7 @@ int bz2g_last_stats(double *out, int n) {
                       (double)t.s,      (double)t.g,   (double)t.bits, t.rle1,
                       t.bwt,            t.mtf,         t.rle2,       t.huffman,
                       t.sizes,          t.place,       (double)t.scatter_launches,
-                      t.scatter_ms,     t.scatter_bytes};
+                      t.scatter_ms,     t.scatter_bytes, (double)t.learned_blocks};
   const int k = (int)(sizeof(v) / sizeof(v[0]));
   for (int i = 0; i < n && i < k; i++) out[i] = v[i];
   return k;
@@ -494,6 +530,268 @@ int bz2g_count_frequencies(const uint16_t *d_syms, int s, int32_t *d_freqs, void
     k_histogram<<<std::min((s + 255) / 256, 296), 256, 0, st>>>(d_syms, s, d_freqs);
     BZ_LAUNCH_CHECK();
     BZ_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+}  // extern "C"
+
+// ----------------------------------------------------- learned table selector
+namespace {
+// Error word of the training kernels, per device.
+int *train_err() {
+  static std::mutex mu;
+  static std::map<int, int *> words;
+  int dev = 0;
+  BZ_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  int *&w = words[dev];
+  if (!w) {
+    BZ_CUDA(cudaMalloc((void **)&w, 64));
+    BZ_CUDA(cudaMemset(w, 0, 64));
+  }
+  return w;
+}
+
+mlp::Batch batch_views(int B, const void *X, const float *inv, const uint8_t *labels, void *work,
+                       float *stats) {
+  mlp::Batch b{};
+  b.B = B;
+  b.X = static_cast<const __nv_bfloat16 *>(X);
+  b.inv = inv;
+  b.labels = labels;
+  uint8_t *p = static_cast<uint8_t *>(work);
+  const size_t hb = align_up((int64_t)B * mlp::kHid * 2, 256);
+  b.H1 = reinterpret_cast<__nv_bfloat16 *>(p);
+  b.H2 = reinterpret_cast<__nv_bfloat16 *>(p + hb);
+  b.dZ2 = reinterpret_cast<__nv_bfloat16 *>(p + 2 * hb);
+  b.dZ1 = reinterpret_cast<__nv_bfloat16 *>(p + 3 * hb);
+  b.Z3 = reinterpret_cast<float *>(p + 4 * hb);
+  b.dZ3 = reinterpret_cast<__nv_bfloat16 *>(p + 4 * hb + align_up((int64_t)B * 64, 256));
+  b.stats = stats;
+  return b;
+}
+}  // namespace
+
+extern "C" {
+
+int bz2g_selector_load(const float *params, size_t count) {
+  return guard([&] {
+    BZ_REQUIRE(params && count == (size_t)mlp::kParams, kErrArg,
+               "selector parameters: expected BZ2G_SELECTOR_PARAMS floats");
+    int dev = 0;
+    BZ_CUDA(cudaGetDevice(&dev));
+    float *d = nullptr;
+    uint8_t *packed = nullptr;
+    BZ_CUDA(cudaMalloc((void **)&d, sizeof(float) * mlp::kParams));
+    BZ_CUDA(cudaMemcpy(d, params, sizeof(float) * mlp::kParams, cudaMemcpyHostToDevice));
+    BZ_CUDA(cudaMalloc((void **)&packed, mlp::kPackedBytes));
+    mlp::pack(d, packed, 0);
+    BZ_CUDA(cudaDeviceSynchronize());
+    BZ_CUDA(cudaFree(d));
+    std::lock_guard<std::mutex> g(g_sel_mu);
+    uint8_t *&slot = g_sel_packed[dev];
+    if (slot) BZ_CUDA(cudaFree(slot));
+    slot = packed;
+  });
+}
+
+int bz2g_set_selector(int mode) {
+  return guard([&] {
+    BZ_REQUIRE(mode >= 0 && mode <= 2, kErrArg, "selector mode must be 0, 1 or 2");
+    std::lock_guard<std::mutex> g(g_sel_mu);
+    g_sel_mode = mode;
+  });
+}
+
+int bz2g_get_selector(void) {
+  std::lock_guard<std::mutex> g(g_sel_mu);
+  return g_sel_mode;
+}
+
+int bz2g_selector_logits(const uint16_t *d_syms, int s, const float *d_params, float *d_logits,
+                         uint8_t *d_sel, void *stream) {
+  return guard([&] {
+    BZ_REQUIRE(s > 0 && d_syms && d_params && d_logits && d_sel, kErrArg, "bad arguments");
+    cudaStream_t st = S(stream);
+    OneBlock ob(s, st);
+    const SlabDev &d = ob.d();
+    const int nsel = (s + kGroupSize - 1) / kGroupSize;
+    BZ_CUDA(cudaMemcpyAsync(d.rle2, d_syms, sizeof(uint16_t) * s, cudaMemcpyDeviceToDevice, st));
+    set_int(d.s, s, st);
+    set_int(d.n_sel, nsel, st);
+    set_int(d.n_groups, kMaxGroups, st);
+    set_int(d.learned, 1, st);
+    BZ_CUDA(cudaMemsetAsync(d.rfreq, 0, sizeof(int32_t) * kMaxGroups * kMaxAlpha, st));
+    float *raw = nullptr;
+    BZ_CUDA(cudaMallocAsync((void **)&raw, sizeof(float) * 8 * kGroupTile * d.n_group_tiles, st));
+    uint8_t *packed = pack_params(d_params, st);
+    mlp::launch_select(d, packed, raw, nullptr, st);
+    BZ_CUDA(cudaMemcpy2DAsync(d_logits, 6 * sizeof(float), raw, 8 * sizeof(float),
+                              6 * sizeof(float), nsel, cudaMemcpyDeviceToDevice, st));
+    BZ_CUDA(cudaMemcpyAsync(d_sel, d.sel, nsel, cudaMemcpyDeviceToDevice, st));
+    BZ_CUDA(cudaMemcpyAsync(d.h_flags, d.err, 4, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaFreeAsync(packed, st));
+    BZ_CUDA(cudaFreeAsync(raw, st));
+    BZ_CUDA(cudaStreamSynchronize(st));
+    BZ_REQUIRE(d.h_flags[0] == 0, kErrInternal, "selector kernel: a tensor-core wait timed out");
+  });
+}
+
+int bz2g_huffman_build_learned(const uint16_t *d_syms, int s, int n_in_use, const float *d_params,
+                               uint8_t *len, int32_t *code, uint8_t *selectors,
+                               uint8_t *mlp_selectors, int *n_selectors, int *n_groups,
+                               void *stream) {
+  return guard([&] {
+    BZ_REQUIRE(s > 0 && d_syms && d_params && len && code && selectors && n_groups, kErrArg,
+               "bad arguments");
+    BZ_REQUIRE(n_in_use >= 0 && n_in_use <= 256, kErrArg, "n_in_use outside [0, 256]");
+    cudaStream_t st = S(stream);
+    OneBlock ob(s, st);
+    const SlabDev &d = ob.d();
+    const int nsel = (s + kGroupSize - 1) / kGroupSize;
+    BZ_CUDA(cudaMemcpyAsync(d.rle2, d_syms, sizeof(uint16_t) * s, cudaMemcpyDeviceToDevice, st));
+    set_int(d.s, s, st);
+    set_int(d.n_in_use, n_in_use, st);
+    BZ_CUDA(cudaMemsetAsync(d.freq, 0, sizeof(int32_t) * kMaxAlpha, st));
+    k_histogram<<<std::min((s + 255) / 256, 296), 256, 0, st>>>(d.rle2, s, d.freq);
+    BZ_LAUNCH_CHECK();
+    uint8_t *packed = pack_params(d_params, st);
+    uint8_t *msel = nullptr;
+    BZ_CUDA(cudaMallocAsync((void **)&msel, nsel, st));
+    BZ_CUDA(cudaMemsetAsync(msel, 0, nsel, st));
+    stage_huffman(d, st, packed, kIters, msel, nsel);
+    std::vector<uint8_t> hl(kMaxGroups * kMaxAlpha);
+    std::vector<int32_t> hc(kMaxGroups * kMaxAlpha);
+    int ng = 0;
+    BZ_CUDA(cudaMemcpyAsync(hl.data(), d.len, hl.size(), cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaMemcpyAsync(hc.data(), d.code, hc.size() * 4, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaMemcpyAsync(selectors, d.sel, nsel, cudaMemcpyDeviceToHost, st));
+    if (mlp_selectors)
+      BZ_CUDA(cudaMemcpyAsync(mlp_selectors, msel, nsel, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaMemcpyAsync(&ng, d.n_groups, 4, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaMemcpyAsync(d.h_flags, d.err, 4, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaFreeAsync(packed, st));
+    BZ_CUDA(cudaFreeAsync(msel, st));
+    BZ_CUDA(cudaStreamSynchronize(st));
+    BZ_REQUIRE(d.h_flags[0] == 0, kErrInternal, "selector kernel: a tensor-core wait timed out");
+    const int alpha = n_in_use + 2;
+    for (int t = 0; t < kMaxGroups; t++)
+      for (int v = 0; v < alpha; v++) {
+        len[t * kMaxAlpha + v] = hl[t * kMaxAlpha + v];
+        if (t < ng) code[t * kMaxAlpha + v] = hc[t * kMaxAlpha + v];
+      }
+    *n_groups = ng;
+    if (n_selectors) *n_selectors = nsel;
+  });
+}
+
+int bz2g_selector_dataset(int count, const uint8_t *const *d_inputs, const size_t *sizes,
+                          const int *levels, uint16_t *d_group_syms, uint8_t *d_labels,
+                          int64_t cap, int64_t *n_groups) {
+  return guard([&] {
+    BZ_REQUIRE(count >= 0 && (count == 0 || (d_inputs && sizes && levels)) && n_groups &&
+                   cap >= 0 && (cap == 0 || (d_group_syms && d_labels)),
+               kErrArg, "bad arguments");
+    std::vector<Compressor::Item> items(count);
+    int64_t maxb = 1;
+    size_t bound = 64;
+    for (int i = 0; i < count; i++) {
+      const int lvl = std::min(std::max(levels[i], 1), 9);
+      items[i] = {d_inputs[i], (int64_t)sizes[i], lvl, 100000 * lvl};
+      maxb = std::max<int64_t>(maxb, 100000 * lvl);
+      bound += stream_bound((int64_t)sizes[i], ((int64_t)sizes[i] + 100000 * lvl - 1) / (100000 * lvl));
+    }
+    // one worker: slabs in a fixed order, so the groups come in a fixed order
+    CompressorConfig cfg;
+    cfg.slab_blocks = g_slab;
+    cfg.workers = 1;
+    cfg.max_block_bytes = std::max<int64_t>(maxb, 900000);
+    int64_t *ctl = nullptr;
+    BZ_CUDA(cudaMalloc((void **)&ctl, sizeof(int64_t) * (1 + cfg.slab_blocks)));
+    BZ_CUDA(cudaMemset(ctl, 0, sizeof(int64_t) * (1 + cfg.slab_blocks)));
+    mlp::SelectorTap tap{d_group_syms, d_labels, cap, ctl, ctl + 1};
+    cfg.tap = &tap;
+    try {
+      Compressor c(cfg);
+      ByteSink sink;
+      sink.reserve(bound);
+      std::vector<size_t> offs;
+      c.compress_batch(items.data(), count, true, sink, offs, nullptr);
+      BZ_CUDA(cudaMemcpy(n_groups, ctl, sizeof(int64_t), cudaMemcpyDeviceToHost));
+    } catch (...) {
+      cudaFree(ctl);
+      throw;
+    }
+    BZ_CUDA(cudaFree(ctl));
+  });
+}
+
+int bz2g_mlp_features(const uint16_t *d_group_syms, int64_t G, void *d_X, float *d_inv,
+                      void *stream) {
+  return guard([&] {
+    BZ_REQUIRE(G >= 0 && (G == 0 || (d_group_syms && d_X && d_inv)), kErrArg, "bad arguments");
+    mlp::features(d_group_syms, G, static_cast<__nv_bfloat16 *>(d_X), d_inv, S(stream));
+  });
+}
+
+size_t bz2g_mlp_work_bytes(int B) {
+  if (B <= 0) return 0;
+  return (size_t)(4 * align_up((int64_t)B * mlp::kHid * 2, 256) + align_up((int64_t)B * 64, 256) +
+                  align_up((int64_t)B * 32, 256));
+}
+
+int bz2g_mlp_grads(const void *d_p16, const float *d_params, int B, const void *d_X,
+                   const float *d_inv, const uint8_t *d_labels, void *d_work, float *d_grad,
+                   float *d_stats, void *stream) {
+  return guard([&] {
+    BZ_REQUIRE(B > 0 && B % 128 == 0, kErrArg, "batch must be a positive multiple of 128");
+    BZ_REQUIRE(d_p16 && d_params && d_X && d_inv && d_labels && d_work && d_grad && d_stats,
+               kErrArg, "null device pointer");
+    mlp::Batch b = batch_views(B, d_X, d_inv, d_labels, d_work, d_stats);
+    mlp::grads(static_cast<const __nv_bfloat16 *>(d_p16), d_params, b, d_grad, train_err(),
+               S(stream));
+  });
+}
+
+int bz2g_mlp_forward(const void *d_p16, const float *d_params, int B, const void *d_X,
+                     const float *d_inv, void *d_work, float *d_logits, void *stream) {
+  return guard([&] {
+    BZ_REQUIRE(B > 0 && B % 128 == 0, kErrArg, "batch must be a positive multiple of 128");
+    BZ_REQUIRE(d_p16 && d_params && d_X && d_inv && d_work && d_logits, kErrArg,
+               "null device pointer");
+    mlp::Batch b = batch_views(B, d_X, d_inv, nullptr, d_work, nullptr);
+    b.Z3 = d_logits;
+    mlp::forward(static_cast<const __nv_bfloat16 *>(d_p16), d_params, b, train_err(), S(stream));
+  });
+}
+
+int bz2g_mlp_adam(float *d_params, const float *d_grad, float *d_m, float *d_v, void *d_p16,
+                  float lr, float beta1, float beta2, float eps, int step, void *stream) {
+  return guard([&] {
+    BZ_REQUIRE(d_params && d_grad && d_m && d_v && d_p16 && step >= 1, kErrArg, "bad arguments");
+    mlp::adam(d_params, d_grad, d_m, d_v, static_cast<__nv_bfloat16 *>(d_p16), lr, beta1, beta2,
+              eps, step, S(stream));
+  });
+}
+
+int bz2g_mlp_to_bf16(const float *d_params, void *d_p16, void *stream) {
+  return guard([&] {
+    BZ_REQUIRE(d_params && d_p16, kErrArg, "null device pointer");
+    mlp::to_bf16(d_params, static_cast<__nv_bfloat16 *>(d_p16), S(stream));
+  });
+}
+
+int bz2g_mlp_status(void *stream) {
+  return guard([&] {
+    int *w = train_err();
+    int h = 0;
+    cudaStream_t st = S(stream);
+    BZ_CUDA(cudaMemcpyAsync(&h, w, 4, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaStreamSynchronize(st));
+    if (h) BZ_CUDA(cudaMemset(w, 0, 4));
+    BZ_REQUIRE(h == 0, kErrInternal,
+               "training kernels: a tensor-core wait timed out (error word " +
+                   std::to_string(h) + ")");
   });
 }
 

@@ -17,6 +17,7 @@
 #include <thread>
 
 #include "engine.h"
+#include "selector.h"
 
 namespace bz2g {
 
@@ -26,9 +27,10 @@ struct Compressor::Worker {
   uint8_t *h_out = nullptr;
   size_t h_out_cap = 0;
   int64_t *h_sizes = nullptr;  // [2 * max_blocks] hdr, pay
-  int32_t *h_cnt = nullptr;    // [3 * max_blocks] m, s, n_sel
+  int32_t *h_cnt = nullptr;    // [4 * max_blocks] m, s, n_sel, learned
   int64_t *h_act = nullptr;    // [max_blocks] A
   uint32_t *h_crc = nullptr;
+  int32_t *h_err = nullptr;    // the workspace's device error word
   cudaEvent_t ev[8] = {};
   cudaEvent_t kt_ev[2 * kMaxTimedLaunches] = {};
   int kt_n = 0;
@@ -47,6 +49,7 @@ struct Compressor::Worker {
     if (h_crc) cudaFreeHost(h_crc);
     if (h_cnt) cudaFreeHost(h_cnt);
     if (h_act) cudaFreeHost(h_act);
+    if (h_err) cudaFreeHost(h_err);
     if (st) cudaStreamDestroy(st);
   }
 };
@@ -63,8 +66,9 @@ Compressor::Compressor(const CompressorConfig &cfg) : cfg_(cfg) {
     BZ_CUDA(cudaMallocHost((void **)&w->h_out, w->h_out_cap));
     BZ_CUDA(cudaMallocHost((void **)&w->h_sizes, sizeof(int64_t) * 2 * cfg_.slab_blocks));
     BZ_CUDA(cudaMallocHost((void **)&w->h_crc, sizeof(uint32_t) * cfg_.slab_blocks));
-    BZ_CUDA(cudaMallocHost((void **)&w->h_cnt, sizeof(int32_t) * 3 * cfg_.slab_blocks));
+    BZ_CUDA(cudaMallocHost((void **)&w->h_cnt, sizeof(int32_t) * 4 * cfg_.slab_blocks));
     BZ_CUDA(cudaMallocHost((void **)&w->h_act, sizeof(int64_t) * cfg_.slab_blocks));
+    BZ_CUDA(cudaMallocHost((void **)&w->h_err, sizeof(int32_t)));
     for (auto &e : w->ev) BZ_CUDA(cudaEventCreate(&e));
     for (auto &e : w->kt_ev) BZ_CUDA(cudaEventCreate(&e));
     BZ_CUDA(cudaMallocHost((void **)&w->h_kt, 8 * kMaxTimedLaunches));
@@ -142,6 +146,14 @@ size_t stream_bound(int64_t n, int64_t nblocks) {
 }
 
 namespace {
+// The selector's tensor-core kernel bounds every wait; a wait that ran out
+// leaves a nonzero error word in the workspace (read back with the sizes).
+void check_err_word(const int32_t *h_err) {
+  BZ_REQUIRE(*h_err == 0, kErrInternal,
+             "learned selector: a tensor-core wait timed out (error word " +
+                 std::to_string(*h_err) + ")");
+}
+
 // 48-bit end-of-stream magic then the 32-bit combined CRC, MSB first, then
 // padding to a byte (src/compression/compress.cu:366-376).
 void put_eos(ByteSink &out, size_t base, int64_t bit, uint32_t crc) {
@@ -248,7 +260,8 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
       if (tm) BZ_CUDA(cudaEventRecord(w.ev[3], w.st));
       stage_rle2(d, w.st);
       if (tm) BZ_CUDA(cudaEventRecord(w.ev[4], w.st));
-      stage_huffman(d, w.st);
+      stage_huffman(d, w.st, cfg_.selector, cfg_.plain_passes);
+      if (cfg_.tap) mlp::tap_groups(d, *cfg_.tap, w.st);
       if (tm) BZ_CUDA(cudaEventRecord(w.ev[5], w.st));
       stage_sizes(d, w.st);
       if (tm) BZ_CUDA(cudaEventRecord(w.ev[6], w.st));
@@ -257,15 +270,18 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
       BZ_CUDA(cudaMemcpyAsync(w.h_sizes + B, d.pay_bits, sizeof(int64_t) * nb,
                               cudaMemcpyDeviceToHost, w.st));
       BZ_CUDA(cudaMemcpyAsync(w.h_crc, d.crc, sizeof(uint32_t) * nb, cudaMemcpyDeviceToHost, w.st));
+      BZ_CUDA(cudaMemcpyAsync(w.h_err, d.err, sizeof(int32_t), cudaMemcpyDeviceToHost, w.st));
       if (times) {
         BZ_CUDA(cudaMemcpyAsync(w.h_cnt, d.m, 4 * nb, cudaMemcpyDeviceToHost, w.st));
         BZ_CUDA(cudaMemcpyAsync(w.h_cnt + B, d.s, 4 * nb, cudaMemcpyDeviceToHost, w.st));
         BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 2 * B, d.n_sel, 4 * nb, cudaMemcpyDeviceToHost, w.st));
+        BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 3 * B, d.learned, 4 * nb, cudaMemcpyDeviceToHost, w.st));
         BZ_CUDA(cudaMemcpyAsync(w.h_act, d.active_sum, 8 * nb, cudaMemcpyDeviceToHost, w.st));
       }
       if (tm && w.kt_n > 0)
         BZ_CUDA(cudaMemcpyAsync(w.h_kt, d.kt_elems, 8 * w.kt_n, cudaMemcpyDeviceToHost, w.st));
       BZ_CUDA(cudaStreamSynchronize(w.st));
+      check_err_word(w.h_err);
       int64_t total = 0;
       for (int i = 0; i < nb; i++) total += w.h_sizes[i] + w.h_sizes[B + i];
       if (times) {
@@ -278,6 +294,7 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
           tsum.g += w.h_cnt[2 * B + i];
           tsum.A += w.h_act[i];
           tsum.bits += w.h_sizes[B + i];
+          tsum.learned_blocks += w.h_cnt[3 * B + i];
         }
       }
       int64_t start;
@@ -452,20 +469,24 @@ void Compressor::compress_batch(const Item *items, int count, bool on_device, By
       stage_bwt(d, plan.max_m_bound, w.st);
       stage_mtf(d, w.st);
       stage_rle2(d, w.st);
-      stage_huffman(d, w.st);
+      stage_huffman(d, w.st, cfg_.selector, cfg_.plain_passes);
+      if (cfg_.tap) mlp::tap_groups(d, *cfg_.tap, w.st);
       stage_sizes(d, w.st);
       BZ_CUDA(cudaMemcpyAsync(w.h_sizes, d.hdr_bits, sizeof(int64_t) * ns, cudaMemcpyDeviceToHost,
                               w.st));
       BZ_CUDA(cudaMemcpyAsync(w.h_sizes + B, d.pay_bits, sizeof(int64_t) * ns,
                               cudaMemcpyDeviceToHost, w.st));
       BZ_CUDA(cudaMemcpyAsync(w.h_crc, d.crc, sizeof(uint32_t) * ns, cudaMemcpyDeviceToHost, w.st));
+      BZ_CUDA(cudaMemcpyAsync(w.h_err, d.err, sizeof(int32_t), cudaMemcpyDeviceToHost, w.st));
       if (times) {
         BZ_CUDA(cudaMemcpyAsync(w.h_cnt, d.m, 4 * ns, cudaMemcpyDeviceToHost, w.st));
         BZ_CUDA(cudaMemcpyAsync(w.h_cnt + B, d.s, 4 * ns, cudaMemcpyDeviceToHost, w.st));
         BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 2 * B, d.n_sel, 4 * ns, cudaMemcpyDeviceToHost, w.st));
+        BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 3 * B, d.learned, 4 * ns, cudaMemcpyDeviceToHost, w.st));
         BZ_CUDA(cudaMemcpyAsync(w.h_act, d.active_sum, 8 * ns, cudaMemcpyDeviceToHost, w.st));
       }
       BZ_CUDA(cudaStreamSynchronize(w.st));
+      check_err_word(w.h_err);
       int64_t words = 0;
       int64_t base;
       uint32_t *arena;
@@ -492,6 +513,7 @@ void Compressor::compress_batch(const Item *items, int count, bool on_device, By
             tsum.g += w.h_cnt[2 * B + i];
             tsum.A += w.h_act[i];
             tsum.bits += w.h_sizes[B + i];
+            tsum.learned_blocks += w.h_cnt[3 * B + i];
           }
       }
       // block starts (bits) in the arena, staged through the sizes buffer

@@ -12,6 +12,9 @@
 namespace bz2g {
 
 class Workspace;
+namespace mlp {
+struct SelectorTap;
+}
 
 struct StageTimes {
   // milliseconds of device time summed over slabs (CUDA events on each
@@ -24,6 +27,8 @@ struct StageTimes {
   // ms, and algorithmic bytes (each element's item read and written once)
   int64_t scatter_launches = 0;
   double scatter_ms = 0, scatter_bytes = 0;
+  // blocks whose tables came from the learned selector
+  int64_t learned_blocks = 0;
 };
 
 struct CompressorConfig {
@@ -31,6 +36,15 @@ struct CompressorConfig {
   int workers = 3;
   int64_t max_block_bytes = 900000;
   bool time_stages = false;
+  // Learned table selector: packed weights on this engine's device
+  // (selector.h), or nullptr for the reference's plain selector.
+  const uint8_t *selector = nullptr;
+  // Selection passes of the plain selector (the reference's 4; 1 is the
+  // single-pass baseline the learned form is measured against).
+  int plain_passes = 4;
+  // Training-set tap: every block with six tables appends its groups and the
+  // plain selector's choices (deterministic order with one worker).
+  const mlp::SelectorTap *tap = nullptr;
 };
 
 // Destination of a stream: a malloc'd buffer that this library grows (and

@@ -67,6 +67,8 @@ struct SlabDev {
   uint8_t *len;                        // [nblocks * 6 * 258]
   int32_t *code;                       // [nblocks * 6 * 258]
   int32_t *rfreq;                      // [nblocks * 6 * 258]
+  int32_t *learned;                    // [nblocks]: table selection by the learned selector
+  int32_t *err;                        // device error word of the tensor-core kernels
   int32_t *sort_len, *done, *ngroups;  // BWT control (ngroups: groups among active rotations)
   int32_t *act_len;                    // BWT: active rotations entering the next round
   int32_t *tile_list;                  // BWT: tiles holding active rotations [ntiles]
@@ -126,7 +128,15 @@ void stage_rle1_crc(const SlabDev &d, cudaStream_t st);
 void stage_bwt(const SlabDev &d, int max_m, cudaStream_t st);
 void stage_mtf(const SlabDev &d, cudaStream_t st);
 void stage_rle2(const SlabDev &d, cudaStream_t st);
-void stage_huffman(const SlabDev &d, cudaStream_t st);
+// Table selection, code lengths and codes.  learned: packed selector weights
+// (selector.h) for the learned form, or nullptr for the reference's plain
+// selector.  plain_passes: selection passes of the plain selector (the
+// reference runs 4; 1 gives the single-pass baseline of the learned form's
+// measurements).  mlp_sel_out (optional): a copy of the selector array right
+// after the MLP's assignment (mlp_sel_bytes from d.sel), for tests.
+void stage_huffman(const SlabDev &d, cudaStream_t st, const uint8_t *learned = nullptr,
+                   int plain_passes = kIters, uint8_t *mlp_sel_out = nullptr,
+                   size_t mlp_sel_bytes = 0);
 // payload bit counts, header bit counts and selector MTF
 void stage_sizes(const SlabDev &d, cudaStream_t st);
 // payload bit counts only (tables, selectors and symbols already in place)

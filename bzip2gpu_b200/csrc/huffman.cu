@@ -7,12 +7,22 @@
 // length-limited (17) Huffman code lengths per table; canonical codes.
 // The histogram is defined as zeroed (the reference leaves it uninitialised).
 #include "engine.h"
+#include "selector.h"
 
 namespace bz2g {
 
 namespace {
 
-__global__ void k_huff_init(SlabDev d) {
+// Which blocks a pass serves: every block, the plain-selector blocks only, or
+// the learned-selector blocks only.
+enum Which { kAll = 0, kPlain = 1, kLearned = 2 };
+
+__device__ __forceinline__ bool serves(const SlabDev &d, int b, int which) {
+  return which == kAll || (which == kPlain) == (d.learned[b] == 0);
+}
+
+// learned_mode: blocks with six tables take the learned selector.
+__global__ void k_huff_init(SlabDev d, int learned_mode) {
   const int b = blockIdx.x;
   const int s = d.s[b];
   const int alpha = d.n_in_use[b] + 2;
@@ -23,6 +33,7 @@ __global__ void k_huff_init(SlabDev d) {
   const int ng = s < 200 ? 2 : s < 600 ? 3 : s < 1200 ? 4 : s < 2400 ? 5 : 6;
   d.n_groups[b] = ng;
   d.n_sel[b] = (s + 49) / 50;
+  d.learned[b] = (learned_mode && ng == kMaxGroups) ? 1 : 0;
   // initial partition, src/compression/huffman.cu:148-185
   const int32_t *freq = d.freq + (size_t)b * kMaxAlpha;
   int gs = 0, remaining = s;
@@ -47,7 +58,7 @@ __global__ void k_huff_init(SlabDev d) {
 // One thread per 50-symbol group.  Costs of all tables are packed in 10-bit
 // fields of one 64-bit word per symbol (50 * 17 < 1024), so a group's six
 // costs are one 64-bit sum.
-__global__ void __launch_bounds__(kGroupTile) k_huff_select(SlabDev d) {
+__global__ void __launch_bounds__(kGroupTile) k_huff_select(SlabDev d, int which) {
   __shared__ uint16_t sy[kGroupTile * kGroupSize];
   __shared__ uint64_t plen[kMaxAlpha];
   __shared__ int rf[kMaxGroups * kMaxAlpha];
@@ -55,7 +66,7 @@ __global__ void __launch_bounds__(kGroupTile) k_huff_select(SlabDev d) {
   const int b = d.gt_block[gt];
   const int g0 = d.gt_first[gt];
   const int nsel = d.n_sel[b];
-  if (g0 >= nsel) return;
+  if (g0 >= nsel || !serves(d, b, which)) return;
   const int ng_here = min(kGroupTile, nsel - g0);
   const int s = d.s[b];
   const int ngrp = d.n_groups[b];
@@ -108,7 +119,7 @@ constexpr int kNodeN = kMaxAlpha * 2;
 
 __device__ __forceinline__ uint32_t hw(uint64_t e) { return (uint32_t)(e >> 32); }
 
-__global__ void __launch_bounds__(kMaxGroups * 32) k_huff_lengths(SlabDev d) {
+__global__ void __launch_bounds__(kMaxGroups * 32) k_huff_lengths(SlabDev d, int which) {
   __shared__ __align__(16) uint64_t heap_s[kMaxGroups][kHeapN + 2];
   __shared__ int32_t leafw_s[kMaxGroups][kMaxAlpha + 1];
   __shared__ int16_t parent_s[kMaxGroups][kNodeN];
@@ -116,7 +127,7 @@ __global__ void __launch_bounds__(kMaxGroups * 32) k_huff_lengths(SlabDev d) {
   const int t = warp_id();
   const int ln = lane_id();
   const int ngrp = d.n_groups[b];
-  if (t >= ngrp) return;
+  if (t >= ngrp || !serves(d, b, which)) return;
   const int alpha = d.n_in_use[b] + 2;
   uint64_t *heap = heap_s[t];
   int32_t *leafw = leafw_s[t];
@@ -230,15 +241,45 @@ __global__ void k_huff_codes(SlabDev d) {
 
 }  // namespace
 
-void stage_huffman(const SlabDev &d, cudaStream_t st) {
-  k_huff_init<<<d.nblocks, 32, 0, st>>>(d);
+namespace {
+void select_pass(const SlabDev &d, int which, cudaStream_t st) {
+  BZ_CUDA(cudaMemsetAsync(d.rfreq, 0, sizeof(int32_t) * kMaxGroups * kMaxAlpha * d.nblocks, st));
+  k_huff_select<<<d.n_group_tiles, kGroupTile, 0, st>>>(d, which);
   BZ_LAUNCH_CHECK();
-  for (int it = 0; it < kIters; it++) {
-    BZ_CUDA(cudaMemsetAsync(d.rfreq, 0, sizeof(int32_t) * kMaxGroups * kMaxAlpha * d.nblocks, st));
-    k_huff_select<<<d.n_group_tiles, kGroupTile, 0, st>>>(d);
-    BZ_LAUNCH_CHECK();
-    k_huff_lengths<<<d.nblocks, kMaxGroups * 32, 0, st>>>(d);
-    BZ_LAUNCH_CHECK();
+}
+void lengths_pass(const SlabDev &d, int which, cudaStream_t st) {
+  k_huff_lengths<<<d.nblocks, kMaxGroups * 32, 0, st>>>(d, which);
+  BZ_LAUNCH_CHECK();
+}
+}  // namespace
+
+// Plain form (the reference's): initial tables, then 4 passes of selection
+// and code lengths.  Learned form: blocks with six tables start from the
+// MLP's selection (code lengths from its choice) and take one exact
+// selection pass and code lengths; the other blocks run the plain passes in
+// the same launches (the later plain-only launches return at once for
+// learned blocks).
+void stage_huffman(const SlabDev &d, cudaStream_t st, const uint8_t *learned, int plain_passes,
+                   uint8_t *mlp_sel_out, size_t mlp_sel_bytes) {
+  k_huff_init<<<d.nblocks, 32, 0, st>>>(d, learned ? 1 : 0);
+  BZ_LAUNCH_CHECK();
+  if (!learned) {
+    for (int it = 0; it < plain_passes; it++) {
+      select_pass(d, kAll, st);
+      lengths_pass(d, kAll, st);
+    }
+  } else {
+    select_pass(d, kPlain, st);
+    mlp::launch_select(d, learned, nullptr, nullptr, st);
+    if (mlp_sel_out)
+      BZ_CUDA(cudaMemcpyAsync(mlp_sel_out, d.sel, mlp_sel_bytes, cudaMemcpyDeviceToDevice, st));
+    lengths_pass(d, kAll, st);
+    select_pass(d, kAll, st);
+    lengths_pass(d, kAll, st);
+    for (int it = 2; it < kIters; it++) {
+      select_pass(d, kPlain, st);
+      lengths_pass(d, kPlain, st);
+    }
   }
   k_huff_codes<<<d.nblocks, 32, 0, st>>>(d);
   BZ_LAUNCH_CHECK();

@@ -1,0 +1,288 @@
+"""Learned table selector: parameter files, training and held-out evaluation.
+
+The selector is an MLP 258 -> 256 -> 256 -> 6 (ReLU) over the symbol
+histogram of each 50-symbol group; it predicts the table that the reference's
+iterative selector (src/compression/huffman.cu:188-243,304-323 of
+SebastianBoteroLeonik/bzip2gpu) assigns.  Inference and training both run in
+the native library on the tensor cores (bzip2gpu_b200/csrc/mlp.cu); torch
+only provides device memory here.
+
+    python -m bzip2gpu_b200.selector train [--out PATH] [--blocks N] [--epochs E]
+    python -m bzip2gpu_b200.selector eval  [--weights PATH] [--blocks N]
+
+Parameter file (little-endian): b"BZ2GSEL1", then bf16 W1 [256 x 258],
+fp32 b1 [256], bf16 W2 [256 x 256], fp32 b2 [256], bf16 W3 [6 x 256],
+fp32 b3 [6].  In memory the parameters are the flat fp32 array of
+include/bz2g.h (BZ2G_SELECTOR_PARAMS values, zero padding).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+from . import SELECTOR_PARAMS, _check, _ptr, lib
+
+WEIGHTS = Path(__file__).resolve().parent / "selector_weights.bin"
+MAGIC = b"BZ2GSEL1"
+IN, IN_PAD, HID, OUT, OUT_PAD = 258, 272, 256, 6, 16
+OFF_W1 = 0
+OFF_B1 = OFF_W1 + HID * IN_PAD
+OFF_W2 = OFF_B1 + HID
+OFF_B2 = OFF_W2 + HID * HID
+OFF_W3 = OFF_B2 + HID
+OFF_B3 = OFF_W3 + OUT_PAD * HID
+assert OFF_B3 + OUT_PAD == SELECTOR_PARAMS
+
+
+# ------------------------------------------------------------ parameters
+def unflatten(P: np.ndarray):
+    """Flat fp32 parameters -> (W1 [256,258], b1, W2 [256,256], b2, W3 [6,256], b3)."""
+    P = np.asarray(P, np.float32)
+    W1 = P[OFF_W1:OFF_B1].reshape(HID, IN_PAD)[:, :IN]
+    W2 = P[OFF_W2:OFF_B2].reshape(HID, HID)
+    W3 = P[OFF_W3:OFF_B3].reshape(OUT_PAD, HID)[:OUT]
+    return W1, P[OFF_B1:OFF_W2], W2, P[OFF_B2:OFF_W3], W3, P[OFF_B3:OFF_B3 + OUT]
+
+
+def flatten(W1, b1, W2, b2, W3, b3) -> np.ndarray:
+    P = np.zeros(SELECTOR_PARAMS, np.float32)
+    P[OFF_W1:OFF_B1].reshape(HID, IN_PAD)[:, :IN] = W1
+    P[OFF_B1:OFF_W2] = b1
+    P[OFF_W2:OFF_B2] = np.asarray(W2, np.float32).reshape(-1)
+    P[OFF_B2:OFF_W3] = b2
+    P[OFF_W3:OFF_B3].reshape(OUT_PAD, HID)[:OUT] = W3
+    P[OFF_B3:OFF_B3 + OUT] = b3
+    return P
+
+
+def _to_bf16_bits(a) -> np.ndarray:
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32)
+    return ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
+
+
+def _from_bf16_bits(b) -> np.ndarray:
+    return (np.asarray(b, np.uint16).astype(np.uint32) << 16).view(np.float32)
+
+
+def save(P, path) -> None:
+    W1, b1, W2, b2, W3, b3 = unflatten(P)
+    with open(path, "wb") as f:
+        f.write(MAGIC)
+        for w, b in ((W1, b1), (W2, b2), (W3, b3)):
+            f.write(_to_bf16_bits(w).tobytes())
+            f.write(np.ascontiguousarray(b, np.float32).tobytes())
+
+
+def load(path=WEIGHTS) -> np.ndarray:
+    """Flat fp32 parameters from a parameter file (weights as stored, bf16)."""
+    raw = Path(path).read_bytes()
+    if raw[:8] != MAGIC:
+        raise ValueError(f"{path}: not a selector parameter file")
+    pos = 8
+    parts = []
+    for shape in ((HID, IN), (HID, HID), (OUT, HID)):
+        n = shape[0] * shape[1]
+        w = _from_bf16_bits(np.frombuffer(raw, np.uint16, n, pos)).reshape(shape)
+        pos += 2 * n
+        b = np.frombuffer(raw, np.float32, shape[0], pos).copy()
+        pos += 4 * shape[0]
+        parts += [w, b]
+    if pos != len(raw):
+        raise ValueError(f"{path}: unexpected size")
+    return flatten(*parts)
+
+
+def load_default(path=WEIGHTS) -> None:
+    """Load the shipped parameters into the native library (current device)."""
+    from . import selector_load
+    selector_load(load(path))
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    """He-uniform weights, zero biases."""
+    rng = np.random.default_rng(seed)
+
+    def he(o, i):
+        lim = math.sqrt(6.0 / i)
+        return rng.uniform(-lim, lim, (o, i)).astype(np.float32)
+
+    return flatten(he(HID, IN), np.zeros(HID), he(HID, HID), np.zeros(HID), he(OUT, HID),
+                   np.zeros(OUT))
+
+
+# --------------------------------------------------------------- training
+class Trainer:
+    """Adam on the tensor-core gradient kernels (bz2g_mlp_grads / _adam)."""
+
+    def __init__(self, P: np.ndarray, batch: int = 8192, lr: float = 1e-3):
+        import torch
+        self.torch = torch
+        self.B = batch
+        self.lr = lr
+        self.P = torch.from_numpy(np.ascontiguousarray(P, np.float32)).cuda()
+        self.P16 = torch.empty(SELECTOR_PARAMS, dtype=torch.int16, device="cuda")
+        self.G = torch.zeros(SELECTOR_PARAMS, dtype=torch.float32, device="cuda")
+        self.m = torch.zeros_like(self.G)
+        self.v = torch.zeros_like(self.G)
+        self.work = torch.empty(lib().bz2g_mlp_work_bytes(batch), dtype=torch.uint8,
+                                device="cuda")
+        self.X = torch.empty((batch, IN_PAD), dtype=torch.int16, device="cuda")
+        self.inv = torch.empty(batch, dtype=torch.float32, device="cuda")
+        self.stats = torch.zeros(2, dtype=torch.float32, device="cuda")
+        self.step_no = 0
+        self.st = torch.cuda.current_stream().cuda_stream
+        _check(lib().bz2g_mlp_to_bf16(_ptr(self.P), _ptr(self.P16), self.st))
+
+    def features(self, gsyms) -> None:
+        _check(lib().bz2g_mlp_features(_ptr(gsyms), gsyms.shape[0], _ptr(self.X), _ptr(self.inv),
+                                       self.st))
+
+    def grads(self, gsyms, labels):
+        """Loss sum and correct count of one batch; gradients left in self.G."""
+        self.features(gsyms)
+        _check(lib().bz2g_mlp_grads(_ptr(self.P16), _ptr(self.P), self.B, _ptr(self.X),
+                                    _ptr(self.inv), _ptr(labels), _ptr(self.work), _ptr(self.G),
+                                    _ptr(self.stats), self.st))
+        return self.stats
+
+    def step(self, gsyms, labels, lr=None):
+        st = self.grads(gsyms, labels)
+        self.step_no += 1
+        _check(lib().bz2g_mlp_adam(_ptr(self.P), _ptr(self.G), _ptr(self.m), _ptr(self.v),
+                                   _ptr(self.P16), self.lr if lr is None else lr, 0.9, 0.999,
+                                   1e-8, self.step_no, self.st))
+        return st
+
+    def logits(self, gsyms):
+        torch = self.torch
+        self.features(gsyms)
+        out = torch.empty((self.B, OUT_PAD), dtype=torch.float32, device="cuda")
+        _check(lib().bz2g_mlp_forward(_ptr(self.P16), _ptr(self.P), self.B, _ptr(self.X),
+                                      _ptr(self.inv), _ptr(self.work), _ptr(out), self.st))
+        return out
+
+    def check(self) -> None:
+        _check(lib().bz2g_mlp_status(self.st))
+
+    def params(self) -> np.ndarray:
+        return self.P.cpu().numpy()
+
+
+def dataset(specs, log=print):
+    """Training groups (device) of config-2-style inputs: (symbols [G, 50]
+    int16 tensor, labels [G] uint8 tensor, inputs generated)."""
+    from . import selector_dataset
+    t0 = time.time()
+    inputs = [sp.make(device=True) for sp in specs]
+    levels = [sp.level for sp in specs]
+    _, _, n = selector_dataset(inputs, levels, 0)
+    syms, labels, n2 = selector_dataset(inputs, levels, n)
+    assert n2 == n
+    log(f"dataset: {len(specs)} inputs, {sum(sp.size for sp in specs)} bytes, {n} groups "
+        f"({time.time() - t0:.1f} s)")
+    del inputs
+    return syms, labels
+
+
+def train(blocks: int = 20000, epochs: int = 3, batch: int = 8192, lr: float = 2e-3,
+          seed: int = 0xB2C3, log=print) -> np.ndarray:
+    import torch
+    from . import workloads as W
+    syms, labels = dataset(W.selector_specs(blocks, seed), log)
+    G = syms.shape[0]
+    tr = Trainer(init_params(seed), batch=batch, lr=lr)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    steps = epochs * (G // batch)
+    t0 = time.time()
+    k = 0
+    for ep in range(epochs):
+        perm = torch.randperm(G, device="cuda", generator=gen)
+        tot = torch.zeros(2, dtype=torch.float64, device="cuda")
+        for i in range(G // batch):
+            idx = perm[i * batch:(i + 1) * batch]
+            # cosine decay over all steps
+            cur = lr * 0.5 * (1 + math.cos(math.pi * k / max(steps, 1)))
+            st = tr.step(syms[idx], labels[idx], cur)
+            tot += st.double()
+            k += 1
+        tr.check()
+        loss, acc = (tot / ((G // batch) * batch)).tolist()
+        log(f"epoch {ep}: loss {loss:.4f} acc {acc:.4f} ({time.time() - t0:.1f} s)")
+    return tr.params()
+
+
+# -------------------------------------------------------------- evaluation
+def evaluate(P: np.ndarray, blocks: int = 20000, seed: int = 0xB2C3F, log=print) -> dict:
+    """Held-out sizes of the three selectors over config-3 inputs (batched
+    form), the learned form's fallback share and round trips of its streams."""
+    import bz2
+
+    import torch
+    from . import compress_batch, last_stats, selector_load, set_selector, set_timing
+    from . import workloads as W
+    specs = W.selector_specs(blocks, seed)
+    inputs = [sp.make(device=True) for sp in specs]
+    levels = [sp.level for sp in specs]
+    selector_load(P)
+    res = {"inputs": len(specs), "input_bytes": int(sum(sp.size for sp in specs))}
+    streams = {}
+    set_timing(True)
+    try:
+        for mode in ("plain", "one_pass", "learned"):
+            set_selector(mode)
+            torch.cuda.synchronize()
+            t0 = time.time()
+            out = compress_batch(inputs, levels, on_device=True)
+            dt = time.time() - t0
+            st = last_stats()
+            streams[mode] = out
+            res[mode] = {"bytes": int(sum(len(o) for o in out)), "wall_s": round(dt, 3),
+                         "ms_huffman": round(st["ms_huffman"], 2)}
+            res["blocks"] = int(st["blocks"])
+            if mode == "learned":
+                res["learned_blocks"] = int(st["learned_blocks"])
+    finally:
+        set_selector("plain")
+        set_timing(False)
+    res["fallback_rate"] = 1.0 - res["learned_blocks"] / max(res["blocks"], 1)
+    pick = list(range(0, len(specs), max(1, len(specs) // 64)))
+    ok = sum(bz2.decompress(bytes(streams["learned"][i])) == inputs[i].cpu().numpy().tobytes()
+             for i in pick)
+    res["round_trip_checked"] = len(pick)
+    res["round_trip_ok"] = int(ok)
+    res["learned_vs_plain"] = res["learned"]["bytes"] / res["plain"]["bytes"]
+    res["learned_vs_one_pass"] = res["learned"]["bytes"] / res["one_pass"]["bytes"]
+    res["one_pass_vs_plain"] = res["one_pass"]["bytes"] / res["plain"]["bytes"]
+    log(json.dumps(res))
+    return res
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(prog="python -m bzip2gpu_b200.selector")
+    ap.add_argument("cmd", choices=["train", "eval"])
+    ap.add_argument("--out", default=str(WEIGHTS))
+    ap.add_argument("--weights", default=str(WEIGHTS))
+    ap.add_argument("--blocks", type=int, default=20000)
+    ap.add_argument("--epochs", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=8192)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    a = ap.parse_args(argv)
+    if a.cmd == "train":
+        P = train(a.blocks, a.epochs, a.batch, a.lr)
+        save(P, a.out)
+        print(f"saved {a.out}")
+        evaluate(load(a.out), a.blocks)
+    else:
+        evaluate(load(a.weights), a.blocks)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -13,6 +13,8 @@ with the seeds below.
                 alphabet size 2..256 (random subset), alpha log-uniform
                 0.05 .. 5, level 1..9 (block = level * 100,000), run starts 1 %,
                 run length 4..255
+  selector_specs config 3: config-2 inputs until 20,000 blocks (seed
+                0xB2C3 training, 0xB2C3F held out), for the learned selector
   large_stream  config 4: 10 GiB; every 64 MiB a new alphabet (size 2..256)
                 and alpha (log-uniform 0.05 .. 5); run starts 2 %, run length
                 4..300, seed 0xB2C4
@@ -94,14 +96,44 @@ class BatchInput:
     level: int
 
 
-def batch_inputs(count: int = 2048, seed: int = 0xB2C2, max_size: int = 8 << 20):
-    """Config 2 inputs (host arrays) with their levels."""
+@dataclass
+class BatchSpec:
+    size: int
+    segment: Segment
+    level: int
+
+    def make(self, device: bool = False):
+        sg = self.segment
+        return gen_markov(self.size, sg.seed, sg.alphabet, sg.alpha, 0.01, 4, 255, device=device)
+
+
+def batch_specs(count: int = 2048, seed: int = 0xB2C2, max_size: int = 8 << 20):
+    """Parameters of the config-2 inputs (sizes, sources, levels), no bytes."""
     rng = np.random.default_rng(seed)
     res = []
     for i in range(count):
         size = int(math.floor(math.exp(rng.uniform(math.log(1024), math.log(max_size)))))
         sg = _draw_segment(rng, seed * 1000003 + i)
         level = int(rng.integers(1, 10))
-        d = gen_markov(size, sg.seed, sg.alphabet, sg.alpha, 0.01, 4, 255)
-        res.append(BatchInput(d, level))
+        res.append(BatchSpec(size, sg, level))
+    return res
+
+
+def batch_inputs(count: int = 2048, seed: int = 0xB2C2, max_size: int = 8 << 20):
+    """Config 2 inputs (host arrays) with their levels."""
+    return [BatchInput(sp.make(), sp.level) for sp in batch_specs(count, seed, max_size)]
+
+
+def selector_specs(blocks: int = 20000, seed: int = 0xB2C3):
+    """Config 3: config-2 inputs (seed 0xB2C3 training, 0xB2C3F held out) until
+    their blocks (level * 100,000 bytes each) number at least `blocks`."""
+    rng = np.random.default_rng(seed)
+    res, nb, i = [], 0, 0
+    while nb < blocks:
+        size = int(math.floor(math.exp(rng.uniform(math.log(1024), math.log(8 << 20)))))
+        sg = _draw_segment(rng, seed * 1000003 + i)
+        level = int(rng.integers(1, 10))
+        res.append(BatchSpec(size, sg, level))
+        nb += -(-size // (level * 100000))
+        i += 1
     return res

@@ -87,8 +87,9 @@ int bz2g_set_engine(int slab_blocks, int workers);
  * this thread: blocks, sum n, sum m, sum A, sum s, sum groups, payload bits,
  * then device ms of RLE1+CRC, BWT, MTF, RLE2, Huffman, sizes, placement,
  * then the radix-scatter kernel's timed launches, their summed device ms and
- * their algorithmic bytes (items read + written); returns the field count.  bz2g_launch_count: kernels launched by this
- * library since it was loaded. */
+ * their algorithmic bytes (items read + written), then the blocks whose
+ * tables came from the learned selector; returns the field count.
+ * bz2g_launch_count: kernels launched by this library since it was loaded. */
 int bz2g_set_timing(int on);
 int bz2g_last_stats(double *out, int n);
 int64_t bz2g_launch_count(void);
@@ -174,6 +175,76 @@ int bz2g_huffman_encode(const uint16_t *d_syms, int s, const uint8_t *len, const
  * Replaces: __global__ count_frequencies(uint16_t*, int, int*)
  *           src/compression/huffman.cu:126-133 */
 int bz2g_count_frequencies(const uint16_t *d_syms, int s, int32_t *d_freqs, void *stream);
+
+/* ------------------------------------------------- learned table selector */
+/* No counterpart in the reference.  An MLP 258 -> 256 -> 256 -> 6 (ReLU, bf16
+ * weights, fp32 accumulation on the tensor cores) over each 50-symbol
+ * group's symbol histogram predicts the table the reference's iterative
+ * selector (src/compression/huffman.cu:188-243,304-323) would choose.  With
+ * the learned selector on, a block with six tables takes: MLP assignment ->
+ * code lengths -> one exact selection pass -> code lengths -> codes; blocks
+ * with fewer tables keep the plain selector.  Streams stay valid bzip2; they
+ * are no longer byte-identical to the reference's.
+ *
+ * Parameters: BZ2G_SELECTOR_PARAMS floats, one flat array, row-major with
+ * zero padding: W1[256][272] b1[256] W2[256][256] b2[256] W3[16][256] b3[16]
+ * (W1 columns 258..271 and W3 rows 6..15 are padding).  Layer 1's
+ * pre-activation is (counts . W1) / (symbols in the group) + b1. */
+#define BZ2G_SELECTOR_PARAMS 139792
+
+/* Loads parameters (host fp32) for the current device. */
+int bz2g_selector_load(const float *params, size_t count);
+/* Selector of the whole-stream calls: 0 = plain (default, the reference's),
+ * 1 = learned, 2 = plain with a single selection pass (the baseline the
+ * learned form is measured against). */
+int bz2g_set_selector(int mode);
+int bz2g_get_selector(void);
+
+/* The fused tensor-core selector over s symbols treated as one six-table
+ * block: logits (device, ceil(s/50) x 6 floats) and choices (device,
+ * ceil(s/50) bytes); d_params: device fp32 parameters. */
+int bz2g_selector_logits(const uint16_t *d_syms, int s, const float *d_params, float *d_logits,
+                         uint8_t *d_sel, void *stream);
+
+/* bz2g_huffman_build with the learned selector (d_params: device fp32
+ * parameters).  mlp_selectors (host, ceil(s/50) bytes, may be NULL) gets the
+ * MLP's own choices before the exact pass. */
+int bz2g_huffman_build_learned(const uint16_t *d_syms, int s, int n_in_use, const float *d_params,
+                               uint8_t *len, int32_t *code, uint8_t *selectors,
+                               uint8_t *mlp_selectors, int *n_selectors, int *n_groups,
+                               void *stream);
+
+/* Training set: the inputs (device memory) compressed as the batched form
+ * does (block = 100000 * level), and for every block with six tables each
+ * group's 50 symbols (0xFFFF past the group's end) and the plain selector's
+ * choice, in a deterministic order.  At most cap groups are written;
+ * *n_groups gets the number available. */
+int bz2g_selector_dataset(int count, const uint8_t *const *d_inputs, const size_t *sizes,
+                          const int *levels, uint16_t *d_group_syms, uint8_t *d_labels,
+                          int64_t cap, int64_t *n_groups);
+
+/* Training on the tensor cores.  d_X: bf16 [G][272] symbol counts, d_inv:
+ * 1 / (symbols in the group); d_p16: bf16 copy of the parameters (same flat
+ * layout).  Batches B are multiples of 128; d_work holds
+ * bz2g_mlp_work_bytes(B) bytes. */
+int bz2g_mlp_features(const uint16_t *d_group_syms, int64_t G, void *d_X, float *d_inv,
+                      void *stream);
+size_t bz2g_mlp_work_bytes(int B);
+/* Mean cross-entropy gradients into d_grad (BZ2G_SELECTOR_PARAMS floats);
+ * d_stats[0] += summed loss, d_stats[1] += correct predictions (zeroed
+ * first). */
+int bz2g_mlp_grads(const void *d_p16, const float *d_params, int B, const void *d_X,
+                   const float *d_inv, const uint8_t *d_labels, void *d_work, float *d_grad,
+                   float *d_stats, void *stream);
+/* Logits (device, B x 16 floats; columns 6..15 are padding). */
+int bz2g_mlp_forward(const void *d_p16, const float *d_params, int B, const void *d_X,
+                     const float *d_inv, void *d_work, float *d_logits, void *stream);
+int bz2g_mlp_adam(float *d_params, const float *d_grad, float *d_m, float *d_v, void *d_p16,
+                  float lr, float beta1, float beta2, float eps, int step, void *stream);
+int bz2g_mlp_to_bf16(const float *d_params, void *d_p16, void *stream);
+/* Waits for the stream; reports a timed-out tensor-core wait of the training
+ * kernels since the last call. */
+int bz2g_mlp_status(void *stream);
 
 /* ------------------------------------------------------ synthetic inputs */
 /* Seeded workload generators (no counterpart in the reference, which has no

@@ -59,6 +59,9 @@ def lib():
         L.orc_encode.restype = ctypes.c_int64
         L.orc_encode.argtypes = [_vp, _i, _vp, _vp, _vp, _vp]
         L.orc_selector_mtf.argtypes = [_vp, _i, _i, _vp]
+        L.orc_huffman_refine.argtypes = [_vp, _i, _i, _vp, _i, _vp, _vp, _vp]
+        L.orc_coded_bits.restype = ctypes.c_int64
+        L.orc_coded_bits.argtypes = [_vp, _i, _vp, _i, _i, _vp]
         L.orc_compress_block.argtypes = [_vp, _i, ctypes.POINTER(BlockInfo), _vp, _vp, _vp, _vp,
                                          _vp]
         L.orc_compress.restype = ctypes.c_int64
@@ -170,6 +173,28 @@ def encode(syms, selectors, len_tab, code_tab):
     bits = lib().orc_encode(s.ctypes.data, s.size, sel.ctypes.data, lt.ctypes.data,
                             ct.ctypes.data, words.ctypes.data)
     return words[: (bits + 31) // 32].copy(), bits
+
+
+def huffman_refine(syms, n_in_use: int, sel_in, n_refine: int = 1):
+    """The learned form after its first assignment sel_in (six tables):
+    (len[6,258], code[6,258], selectors)."""
+    s = np.ascontiguousarray(syms, dtype=np.uint16)
+    si = np.ascontiguousarray(sel_in, dtype=np.uint8)
+    ln = np.zeros((G, A), np.uint8)
+    code = np.zeros((G, A), np.int32)
+    sel = np.zeros(s.size // 50 + 2, np.uint8)
+    nsel = lib().orc_huffman_refine(s.ctypes.data, s.size, n_in_use, si.ctypes.data, n_refine,
+                                    ln.ctypes.data, code.ctypes.data, sel.ctypes.data)
+    return ln, code, sel[:nsel].copy()
+
+
+def coded_bits(syms, selectors, n_groups: int, n_in_use: int, len_tab) -> int:
+    """Selection-dependent bits of a block (payload, selector MTF, tables)."""
+    s = np.ascontiguousarray(syms, dtype=np.uint16)
+    sel = np.ascontiguousarray(selectors, dtype=np.uint8)
+    lt = np.ascontiguousarray(len_tab, dtype=np.uint8)
+    return lib().orc_coded_bits(s.ctypes.data, s.size, sel.ctypes.data, n_groups, n_in_use,
+                                lt.ctypes.data)
 
 
 def selector_mtf(sel, n_groups: int) -> np.ndarray:

@@ -303,6 +303,47 @@ void orc_initial_assignment(int n_groups, int s, int alpha_size,
   }
 }
 
+/* One selection pass (src/compression/huffman.cu:188-243): per 50-symbol
+ * group the cost of every table, the first minimum wins, and the chosen
+ * table's symbol counts. */
+static void select_pass(const uint16_t *syms, int s, int ng,
+                        uint8_t len[ORC_MAX_GROUPS][ORC_MAX_ALPHA], uint8_t *selectors,
+                        int32_t rfreq[ORC_MAX_GROUPS][ORC_MAX_ALPHA]) {
+  int nsel = (s + 49) / 50;
+  memset(rfreq, 0, sizeof(int32_t) * ORC_MAX_GROUPS * ORC_MAX_ALPHA);
+  for (int g = 0; g < nsel; g++) {
+    int gs = g * 50, ge = gs + 49;
+    if (ge >= s) ge = s - 1;
+    uint32_t cost[ORC_MAX_GROUPS] = {0};
+    for (int i = gs; i <= ge; i++)
+      for (int t = 0; t < ng; t++) cost[t] += len[t][syms[i]];
+    uint32_t bc = 0xFFFFFFFFu;
+    int bt = -1;
+    for (int t = 0; t < ng; t++)
+      if (cost[t] < bc) { bc = cost[t]; bt = t; }
+    selectors[g] = (uint8_t)bt;
+    for (int i = gs; i <= ge; i++) rfreq[bt][syms[i]]++;
+  }
+}
+
+/* canonical codes, src/compression/huffman.cu:135-146,352-362 */
+static void canonical_codes(int ng, int alpha, uint8_t len[ORC_MAX_GROUPS][ORC_MAX_ALPHA],
+                            int32_t code[ORC_MAX_GROUPS][ORC_MAX_ALPHA]) {
+  for (int t = 0; t < ng; t++) {
+    int mn = 32, mx = 0;
+    for (int v = 0; v < alpha; v++) {
+      if (len[t][v] > mx) mx = len[t][v];
+      if (len[t][v] < mn) mn = len[t][v];
+    }
+    int vec = 0;
+    for (int l = mn; l <= mx; l++) {
+      for (int v = 0; v < alpha; v++)
+        if (len[t][v] == l) code[t][v] = vec++;
+      vec <<= 1;
+    }
+  }
+}
+
 /* src/compression/huffman.cu:256-364 with a zeroed histogram. */
 int orc_huffman_build(const uint16_t *syms, int s, int alphabet_size,
                       uint8_t len[ORC_MAX_GROUPS][ORC_MAX_ALPHA],
@@ -318,38 +359,65 @@ int orc_huffman_build(const uint16_t *syms, int s, int alphabet_size,
   int nsel = (s + 49) / 50;
   int32_t rfreq[ORC_MAX_GROUPS][ORC_MAX_ALPHA];
   for (int iter = 0; iter < 4; iter++) {
-    memset(rfreq, 0, sizeof(rfreq));
-    for (int g = 0; g < nsel; g++) {
-      int gs = g * 50, ge = gs + 49;
-      if (ge >= s) ge = s - 1;
-      uint32_t cost[ORC_MAX_GROUPS] = {0};
-      for (int i = gs; i <= ge; i++)
-        for (int t = 0; t < ng; t++) cost[t] += len[t][syms[i]];
-      uint32_t bc = 0xFFFFFFFFu;
-      int bt = -1;
-      for (int t = 0; t < ng; t++)
-        if (cost[t] < bc) { bc = cost[t]; bt = t; }
-      selectors[g] = (uint8_t)bt;
-      for (int i = gs; i <= ge; i++) rfreq[bt][syms[i]]++;
-    }
+    select_pass(syms, s, ng, len, selectors, rfreq);
     for (int t = 0; t < ng; t++) orc_code_lengths(rfreq[t], len[t], alpha, 17);
   }
-  /* canonical codes, huffman.cu:135-146,352-362 */
-  for (int t = 0; t < ng; t++) {
-    int mn = 32, mx = 0;
-    for (int v = 0; v < alpha; v++) {
-      if (len[t][v] > mx) mx = len[t][v];
-      if (len[t][v] < mn) mn = len[t][v];
-    }
-    int vec = 0;
-    for (int l = mn; l <= mx; l++) {
-      for (int v = 0; v < alpha; v++)
-        if (len[t][v] == l) code[t][v] = vec++;
-      vec <<= 1;
-    }
-  }
+  canonical_codes(ng, alpha, len, code);
   *n_groups_out = ng;
   return nsel;
+}
+
+/* The learned form's passes after its first assignment sel_in (six tables):
+ * code lengths from the chosen tables' symbol counts, then n_refine passes
+ * of exact selection and code lengths, then canonical codes.  Written from
+ * bzip2gpu_b200/csrc/huffman.cu's learned schedule; the pass itself is the
+ * reference's (src/compression/huffman.cu:188-243). */
+int orc_huffman_refine(const uint16_t *syms, int s, int alphabet_size, const uint8_t *sel_in,
+                       int n_refine, uint8_t len[ORC_MAX_GROUPS][ORC_MAX_ALPHA],
+                       int32_t code[ORC_MAX_GROUPS][ORC_MAX_ALPHA], uint8_t *selectors) {
+  const int alpha = alphabet_size + 2, ng = ORC_MAX_GROUPS;
+  const int nsel = (s + 49) / 50;
+  for (int g = 0; g < ORC_MAX_GROUPS; g++)
+    for (int v = 0; v < alpha; v++) len[g][v] = 15;
+  int32_t rfreq[ORC_MAX_GROUPS][ORC_MAX_ALPHA];
+  memset(rfreq, 0, sizeof(rfreq));
+  for (int g = 0; g < nsel; g++) {
+    int gs = g * 50, ge = gs + 49;
+    if (ge >= s) ge = s - 1;
+    selectors[g] = sel_in[g];
+    for (int i = gs; i <= ge; i++) rfreq[sel_in[g]][syms[i]]++;
+  }
+  for (int t = 0; t < ng; t++) orc_code_lengths(rfreq[t], len[t], alpha, 17);
+  for (int r = 0; r < n_refine; r++) {
+    select_pass(syms, s, ng, len, selectors, rfreq);
+    for (int t = 0; t < ng; t++) orc_code_lengths(rfreq[t], len[t], alpha, 17);
+  }
+  canonical_codes(ng, alpha, len, code);
+  return nsel;
+}
+
+/* Bits of one block's coded part that depend on the table selection:
+ * payload, the unary selector MTF codes, and the table deltas
+ * (src/compression/compress.cu:300-345). */
+int64_t orc_coded_bits(const uint16_t *syms, int s, const uint8_t *selectors, int ng,
+                       int alphabet_size, const uint8_t len[ORC_MAX_GROUPS][ORC_MAX_ALPHA]) {
+  const int alpha = alphabet_size + 2, nsel = (s + 49) / 50;
+  int64_t bits = 0;
+  for (int i = 0; i < s; i++) bits += len[selectors[i / 50]][syms[i]];
+  uint8_t *mtf = (uint8_t *)malloc(nsel > 0 ? nsel : 1);
+  orc_selector_mtf(selectors, nsel, ng, mtf);
+  for (int g = 0; g < nsel; g++) bits += mtf[g] + 1;
+  free(mtf);
+  for (int t = 0; t < ng; t++) {
+    int cur = len[t][0];
+    bits += 5;
+    for (int v = 0; v < alpha; v++) {
+      int d = (int)len[t][v] - cur;
+      bits += 2 * (d < 0 ? -d : d) + 1;
+      cur = len[t][v];
+    }
+  }
+  return bits;
 }
 
 /* src/compression/huffman_encode.cu:30-71: code of symbol i from table

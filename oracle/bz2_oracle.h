@@ -79,6 +79,18 @@ int orc_huffman_build(const uint16_t *syms, int s, int alphabet_size,
                       int32_t code[ORC_MAX_GROUPS][ORC_MAX_ALPHA],
                       uint8_t *selectors, int *n_groups);
 
+/* The learned form's passes after its first assignment sel_in (six tables):
+ * code lengths from the chosen tables' counts, n_refine passes of exact
+ * selection + code lengths, canonical codes.  Returns the selector count. */
+int orc_huffman_refine(const uint16_t *syms, int s, int alphabet_size, const uint8_t *sel_in,
+                       int n_refine, uint8_t len[ORC_MAX_GROUPS][ORC_MAX_ALPHA],
+                       int32_t code[ORC_MAX_GROUPS][ORC_MAX_ALPHA], uint8_t *selectors);
+
+/* Selection-dependent bits of a block: payload + unary selector MTF +
+ * table deltas (src/compression/compress.cu:300-345). */
+int64_t orc_coded_bits(const uint16_t *syms, int s, const uint8_t *selectors, int ng,
+                       int alphabet_size, const uint8_t len[ORC_MAX_GROUPS][ORC_MAX_ALPHA]);
+
 /* Initial table assignment only (before refinement).
  * src/compression/huffman.cu:148-185 */
 void orc_initial_assignment(int n_groups, int s, int alpha_size,

@@ -1,0 +1,236 @@
+"""Learned table selector on the GPU: the tensor-core kernels against the fp64
+oracle (oracle/mlp.py), the learned form's passes against the C oracle
+(bit-exact given the MLP's choices), and whole learned streams (valid bzip2,
+deterministic).
+
+Tolerances.  The kernels hold weights, hidden activations and the
+back-propagated deltas in bf16 and accumulate in fp32.  Against the oracle
+with the same bf16 rounding points (emulate=True) the remaining differences
+are fp32 summation order and rare bf16 rounding flips: logits within
+2e-3 * max(1, max |logit|), gradients within a relative Frobenius error of
+5e-3 per tensor.  Against exact fp64 over the fp32 parameters (emulate=False)
+the bf16 rounding itself shows: 5e-2 for both.
+"""
+import bz2
+
+import numpy as np
+import pytest
+
+import oracle
+import oracle.mlp as M
+import bzip2gpu_b200 as B
+import bzip2gpu_b200.selector as S
+import bzip2gpu_b200.workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _params(seed=7):
+    rng = np.random.default_rng(seed)
+    P = S.init_params(seed)
+    P[S.OFF_B1:S.OFF_W2] = rng.normal(0, 0.1, S.HID)
+    P[S.OFF_B2:S.OFF_W3] = rng.normal(0, 0.1, S.HID)
+    P[S.OFF_B3:S.OFF_B3 + S.OUT] = rng.normal(0, 0.3, S.OUT)
+    return P
+
+
+def _block_groups(seed=3, n=900000):
+    st, info = oracle.compress_block(W.small_markov(n, seed=seed))
+    return st, info
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.fixture(scope="module")
+def groups(torch_cuda):
+    st, info = _block_groups()
+    gs = M.groups_of_stream(st["rle2"])[:1024]
+    labels = st["sel"][:1024].astype(np.uint8)
+    return gs, labels
+
+
+def test_training_forward_matches_oracle(torch_cuda, groups):
+    gs, _ = groups
+    P = _params()
+    tr = S.Trainer(P, batch=gs.shape[0])
+    d = torch_cuda.from_numpy(gs.astype(np.int16)).cuda()
+    z = tr.logits(d).cpu().numpy()[:, :6].astype(np.float64)
+    c, n = M.features(gs)
+    ze = M.logits(P, c, n, emulate=True)
+    zx = M.logits(P, c, n, emulate=False)
+    scale = max(1.0, float(np.abs(ze).max()))
+    assert np.abs(z - ze).max() <= 2e-3 * scale
+    assert np.abs(z - zx).max() <= 5e-2 * scale
+
+
+def test_fused_selector_matches_oracle(torch_cuda):
+    st, info = _block_groups(5)
+    syms = st["rle2"]
+    P = _params(9)
+    d_syms = torch_cuda.from_numpy(syms.astype(np.int16)).cuda()
+    d_P = torch_cuda.from_numpy(P).cuda()
+    lg, sel = B.selector_logits(d_syms, d_P)
+    lg = lg.cpu().numpy().astype(np.float64)
+    sel = sel.cpu().numpy()
+    c, n = M.features(M.groups_of_stream(syms))
+    ze = M.logits(P, c, n, emulate=True)
+    scale = max(1.0, float(np.abs(ze).max()))
+    assert lg.shape == ze.shape
+    assert np.abs(lg - ze).max() <= 2e-3 * scale
+    assert np.abs(lg - M.logits(P, c, n, emulate=False)).max() <= 5e-2 * scale
+    # the choice is the first maximum of the kernel's own logits, and agrees
+    # with the oracle's wherever the oracle's top two are apart
+    assert np.array_equal(sel, lg.argmax(1))
+    top2 = np.sort(ze, 1)[:, -2:]
+    clear = top2[:, 1] - top2[:, 0] > 4e-3 * scale
+    assert np.array_equal(sel[clear], ze.argmax(1)[clear])
+
+
+def test_fused_selector_ragged_tail(torch_cuda):
+    # a symbol count that leaves a short last group and a partial group tile
+    st, _ = _block_groups(6, 100000)
+    syms = st["rle2"][: 128 * 50 * 2 + 50 * 3 + 17]
+    P = _params(4)
+    lg, sel = B.selector_logits(torch_cuda.from_numpy(syms.astype(np.int16)).cuda(),
+                                torch_cuda.from_numpy(P).cuda())
+    c, n = M.features(M.groups_of_stream(syms))
+    assert n[-1] == 17
+    ze = M.logits(P, c, n, emulate=True)
+    assert np.abs(lg.cpu().numpy() - ze).max() <= 2e-3 * max(1.0, float(np.abs(ze).max()))
+
+
+def test_gradients_match_oracle(torch_cuda, groups):
+    gs, labels = groups
+    P = _params(13)
+    tr = S.Trainer(P, batch=gs.shape[0])
+    d = torch_cuda.from_numpy(gs.astype(np.int16)).cuda()
+    y = torch_cuda.from_numpy(labels).cuda()
+    stats = tr.grads(d, y).cpu().numpy()
+    tr.check()
+    g = tr.G.cpu().numpy().astype(np.float64)
+    c, n = M.features(gs)
+    loss_e, corr_e, ge = M.loss_grads(P, c, n, labels, emulate=True)
+    _, _, gx = M.loss_grads(P, c, n, labels, emulate=False)
+    assert abs(stats[0] - loss_e) <= 1e-3 * abs(loss_e)
+    assert abs(stats[1] - corr_e) <= 0.01 * gs.shape[0]
+    parts = {"W1": (S.OFF_W1, S.OFF_B1), "b1": (S.OFF_B1, S.OFF_W2), "W2": (S.OFF_W2, S.OFF_B2),
+             "b2": (S.OFF_B2, S.OFF_W3), "W3": (S.OFF_W3, S.OFF_B3),
+             "b3": (S.OFF_B3, S.OFF_B3 + 16)}
+    for name, (a, b) in parts.items():
+        assert _rel(g[a:b], ge[a:b]) <= 5e-3, (name, _rel(g[a:b], ge[a:b]))
+        assert _rel(g[a:b], gx[a:b]) <= 5e-2, (name, _rel(g[a:b], gx[a:b]))
+    assert np.all(g[S.OFF_W1:S.OFF_B1].reshape(S.HID, S.IN_PAD)[:, S.IN:] == 0)
+
+
+def test_training_steps_reduce_loss(torch_cuda, groups):
+    gs, labels = groups
+    tr = S.Trainer(S.init_params(1), batch=gs.shape[0], lr=2e-3)
+    d = torch_cuda.from_numpy(gs.astype(np.int16)).cuda()
+    y = torch_cuda.from_numpy(labels).cuda()
+    first = float(tr.step(d, y)[0].item())
+    for _ in range(40):
+        last = float(tr.step(d, y)[0].item())
+    tr.check()
+    assert last < 0.8 * first
+
+
+@pytest.mark.parametrize("seed,n", [(3, 900000), (12, 400000), (2, 30000)])
+def test_learned_build_matches_oracle_given_mlp_choices(torch_cuda, seed, n):
+    st, info = _block_groups(seed, n)
+    syms = st["rle2"]
+    P = _params(seed)
+    d_syms = torch_cuda.from_numpy(syms.astype(np.int16)).cuda()
+    d_P = torch_cuda.from_numpy(P).cuda()
+    ln, code, sel, ng, msel = B.huffman_build_learned(d_syms, info.n_in_use, d_P)
+    a = info.n_in_use + 2
+    if info.n_groups == 6:
+        ref_ln, ref_code, ref_sel = oracle.huffman_refine(syms, info.n_in_use, msel, 1)
+        # the MLP's choices are those of the fused kernel
+        lg, fsel = B.selector_logits(d_syms, d_P)
+        assert np.array_equal(msel, fsel.cpu().numpy())
+    else:
+        ref_ln, ref_code, ref_sel, _ = oracle.huffman_build(syms, info.n_in_use)
+    assert ng == info.n_groups
+    assert np.array_equal(sel, ref_sel)
+    assert np.array_equal(ln[:ng, :a], ref_ln[:ng, :a])
+    assert np.array_equal(code[:ng, :a], ref_code[:ng, :a])
+
+
+def test_dataset_tap_groups_and_labels(torch_cuda):
+    # three inputs: the groups of every six-table block, in slab order
+    # (length-sorted, stable), with the plain selector's choices
+    specs = W.batch_specs(3, 0xB2C3)
+    inputs = [sp.make(device=True) for sp in specs]
+    levels = [sp.level for sp in specs]
+    syms, labels, n = B.selector_dataset(inputs, levels, 1 << 20)
+    assert syms.shape[0] == n > 0
+    blocks = []
+    for sp, x in zip(specs, inputs):
+        h = x.cpu().numpy()
+        bb = sp.level * 100000
+        blocks += [h[o:o + bb] for o in range(0, h.size, bb)]
+    order = sorted(range(len(blocks)), key=lambda i: -blocks[i].size)
+    exp_s, exp_l = [], []
+    for i in order:
+        st, info = oracle.compress_block(blocks[i])
+        if info.n_groups == 6:
+            exp_s.append(M.groups_of_stream(st["rle2"]))
+            exp_l.append(st["sel"])
+    exp_s = np.concatenate(exp_s).astype(np.uint16)
+    exp_l = np.concatenate(exp_l)
+    assert np.array_equal(syms.cpu().numpy().view(np.uint16), exp_s)
+    assert np.array_equal(labels.cpu().numpy(), exp_l)
+
+
+@pytest.fixture
+def learned_mode(torch_cuda):
+    P = S.load() if S.WEIGHTS.exists() else _params(21)
+    B.selector_load(P)
+    B.set_selector("learned")
+    yield P
+    B.set_selector("plain")
+
+
+def test_learned_streams_decode_and_repeat(learned_mode):
+    for a in (W.small_markov(3000000, seed=41), np.zeros(1000000, np.uint8),
+              B.gen_uniform(700000, 42), W.small_markov(2000, seed=43)):
+        s1 = B.compress(a, 9)
+        assert bz2.decompress(s1) == a.tobytes()
+        assert B.compress(a, 9) == s1
+
+
+def test_learned_batched_equals_learned_plain_calls(learned_mode):
+    specs = W.batch_specs(6, 0xB2C3F)
+    inputs = [sp.make() for sp in specs]
+    levels = [sp.level for sp in specs]
+    outs = B.compress_batch(inputs, levels)
+    for x, lv, o in zip(inputs, levels, outs):
+        assert bytes(o) == B.compress(x, lv, lv * 100000)
+
+
+def test_one_pass_mode_decodes(torch_cuda):
+    a = W.small_markov(1500000, seed=44)
+    B.set_selector("one_pass")
+    try:
+        s = B.compress(a, 9)
+    finally:
+        B.set_selector("plain")
+    assert bz2.decompress(s) == a.tobytes()
+    assert B.compress(a, 9) == oracle.compress(a, 9, threads=8)
+
+
+@pytest.mark.skipif(not S.WEIGHTS.exists(), reason="no shipped selector parameters")
+def test_shipped_selector_size_within_half_percent(learned_mode):
+    specs = W.selector_specs(300, 0xB2C3F)
+    inputs = [sp.make() for sp in specs]
+    levels = [sp.level for sp in specs]
+    learned = sum(len(o) for o in B.compress_batch(inputs, levels))
+    B.set_selector("plain")
+    plain = sum(len(o) for o in B.compress_batch(inputs, levels))
+    B.set_selector("one_pass")
+    one = sum(len(o) for o in B.compress_batch(inputs, levels))
+    B.set_selector("learned")
+    assert learned <= 1.005 * plain
+    assert learned < one
