@@ -300,6 +300,29 @@ def main():
     assert bytes(bout[0]) == out
     bt = max_over_ranks(bt, world)
     batched_value = n * world * args.steps / bt / 1e6
+    # batched + learned selector (shipped parameters); the streams differ
+    # from the reference's, so they are checked by decoding, and their size
+    # is reported against the plain stream's
+    learned = None
+    import bzip2gpu_b200.selector as SEL
+    if SEL.WEIGHTS.exists():
+        SEL.load_default()
+        B.set_selector("learned")
+        try:
+            B.compress_batch([d_in], [9], [900000], out=h_out, on_device=True)  # warm
+            lt, lout = timed(lambda: B.compress_batch([d_in], [9], [900000], out=h_out,
+                                                      on_device=True))
+            lbytes = bytes(lout[0])
+        finally:
+            B.set_selector("plain")
+        lt = max_over_ranks(lt, world)
+        import bz2
+        dec = bz2.BZ2Decompressor().decompress(lbytes[: 4 << 20], max_length=8 << 20)
+        head = d_in[: len(dec)].cpu().numpy().tobytes()
+        learned = {"MB/s": round(n * world * args.steps / lt / 1e6, 2),
+                   "ratio": round(len(lbytes) / n, 5),
+                   "size_vs_plain": round(len(lbytes) / len(out), 6),
+                   "decoded_prefix_bytes": len(dec), "decoded_prefix_ok": dec == head}
     dt = max_over_ranks(dt, world)
     value = n * world * args.steps / dt / 1e6
 
@@ -365,7 +388,7 @@ def main():
                        "blocks": int(stats["blocks"]), "ratio": round(ratio, 4)},
             "e2e": e2e, "roofline": roof, "pipeline_roofline": pipeline, "cpu_baseline": cpu,
             "forms": {"plain": round(value, 2), "batched": round(batched_value, 2),
-                      "learned": None},
+                      "learned": learned},
             "clocks": clk.summary(), "gpu_launches": int(launches),
             "stats": {k: stats[k] for k in ("n", "m", "A", "s", "g", "bits")},
             "stage_ms_sum_over_slabs_last_step": stage_ms,

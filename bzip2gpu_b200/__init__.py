@@ -238,7 +238,8 @@ def set_timing(on: bool) -> None:
 
 STAT_FIELDS = ("blocks", "n", "m", "A", "s", "g", "bits", "ms_rle1", "ms_bwt", "ms_mtf",
                "ms_rle2", "ms_huffman", "ms_sizes", "ms_place", "scatter_launches",
-               "scatter_ms", "scatter_bytes", "learned_blocks")
+               "scatter_ms", "scatter_bytes", "learned_blocks",
+               "six_table_blocks")
 
 
 def last_stats() -> dict:

@@ -309,7 +309,8 @@ int bz2g_last_stats(double *out, int n) {
                       (double)t.s,      (double)t.g,   (double)t.bits, t.rle1,
                       t.bwt,            t.mtf,         t.rle2,       t.huffman,
                       t.sizes,          t.place,       (double)t.scatter_launches,
-                      t.scatter_ms,     t.scatter_bytes, (double)t.learned_blocks};
+                      t.scatter_ms,     t.scatter_bytes, (double)t.learned_blocks,
+                      (double)t.six_table_blocks};
   const int k = (int)(sizeof(v) / sizeof(v[0]));
   for (int i = 0; i < n && i < k; i++) out[i] = v[i];
   return k;
@@ -625,7 +626,7 @@ int bz2g_selector_logits(const uint16_t *d_syms, int s, const float *d_params, f
     float *raw = nullptr;
     BZ_CUDA(cudaMallocAsync((void **)&raw, sizeof(float) * 8 * kGroupTile * d.n_group_tiles, st));
     uint8_t *packed = pack_params(d_params, st);
-    mlp::launch_select(d, packed, raw, nullptr, st);
+    mlp::launch_select(d, packed, raw, nullptr, nullptr, st);
     BZ_CUDA(cudaMemcpy2DAsync(d_logits, 6 * sizeof(float), raw, 8 * sizeof(float),
                               6 * sizeof(float), nsel, cudaMemcpyDeviceToDevice, st));
     BZ_CUDA(cudaMemcpyAsync(d_sel, d.sel, nsel, cudaMemcpyDeviceToDevice, st));

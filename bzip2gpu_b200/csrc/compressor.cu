@@ -27,7 +27,7 @@ struct Compressor::Worker {
   uint8_t *h_out = nullptr;
   size_t h_out_cap = 0;
   int64_t *h_sizes = nullptr;  // [2 * max_blocks] hdr, pay
-  int32_t *h_cnt = nullptr;    // [4 * max_blocks] m, s, n_sel, learned
+  int32_t *h_cnt = nullptr;    // [5 * max_blocks] m, s, n_sel, learned, n_groups
   int64_t *h_act = nullptr;    // [max_blocks] A
   uint32_t *h_crc = nullptr;
   int32_t *h_err = nullptr;    // the workspace's device error word
@@ -66,7 +66,7 @@ Compressor::Compressor(const CompressorConfig &cfg) : cfg_(cfg) {
     BZ_CUDA(cudaMallocHost((void **)&w->h_out, w->h_out_cap));
     BZ_CUDA(cudaMallocHost((void **)&w->h_sizes, sizeof(int64_t) * 2 * cfg_.slab_blocks));
     BZ_CUDA(cudaMallocHost((void **)&w->h_crc, sizeof(uint32_t) * cfg_.slab_blocks));
-    BZ_CUDA(cudaMallocHost((void **)&w->h_cnt, sizeof(int32_t) * 4 * cfg_.slab_blocks));
+    BZ_CUDA(cudaMallocHost((void **)&w->h_cnt, sizeof(int32_t) * 5 * cfg_.slab_blocks));
     BZ_CUDA(cudaMallocHost((void **)&w->h_act, sizeof(int64_t) * cfg_.slab_blocks));
     BZ_CUDA(cudaMallocHost((void **)&w->h_err, sizeof(int32_t)));
     for (auto &e : w->ev) BZ_CUDA(cudaEventCreate(&e));
@@ -276,6 +276,7 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
         BZ_CUDA(cudaMemcpyAsync(w.h_cnt + B, d.s, 4 * nb, cudaMemcpyDeviceToHost, w.st));
         BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 2 * B, d.n_sel, 4 * nb, cudaMemcpyDeviceToHost, w.st));
         BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 3 * B, d.learned, 4 * nb, cudaMemcpyDeviceToHost, w.st));
+        BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 4 * B, d.n_groups, 4 * nb, cudaMemcpyDeviceToHost, w.st));
         BZ_CUDA(cudaMemcpyAsync(w.h_act, d.active_sum, 8 * nb, cudaMemcpyDeviceToHost, w.st));
       }
       if (tm && w.kt_n > 0)
@@ -295,6 +296,7 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
           tsum.A += w.h_act[i];
           tsum.bits += w.h_sizes[B + i];
           tsum.learned_blocks += w.h_cnt[3 * B + i];
+          tsum.six_table_blocks += w.h_cnt[4 * B + i] == kMaxGroups;
         }
       }
       int64_t start;
@@ -483,6 +485,7 @@ void Compressor::compress_batch(const Item *items, int count, bool on_device, By
         BZ_CUDA(cudaMemcpyAsync(w.h_cnt + B, d.s, 4 * ns, cudaMemcpyDeviceToHost, w.st));
         BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 2 * B, d.n_sel, 4 * ns, cudaMemcpyDeviceToHost, w.st));
         BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 3 * B, d.learned, 4 * ns, cudaMemcpyDeviceToHost, w.st));
+        BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 4 * B, d.n_groups, 4 * ns, cudaMemcpyDeviceToHost, w.st));
         BZ_CUDA(cudaMemcpyAsync(w.h_act, d.active_sum, 8 * ns, cudaMemcpyDeviceToHost, w.st));
       }
       BZ_CUDA(cudaStreamSynchronize(w.st));
@@ -514,6 +517,7 @@ void Compressor::compress_batch(const Item *items, int count, bool on_device, By
             tsum.A += w.h_act[i];
             tsum.bits += w.h_sizes[B + i];
             tsum.learned_blocks += w.h_cnt[3 * B + i];
+            tsum.six_table_blocks += w.h_cnt[4 * B + i] == kMaxGroups;
           }
       }
       // block starts (bits) in the arena, staged through the sizes buffer

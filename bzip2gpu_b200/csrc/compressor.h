@@ -27,8 +27,9 @@ struct StageTimes {
   // ms, and algorithmic bytes (each element's item read and written once)
   int64_t scatter_launches = 0;
   double scatter_ms = 0, scatter_bytes = 0;
-  // blocks whose tables came from the learned selector
-  int64_t learned_blocks = 0;
+  // blocks whose tables came from the learned selector, and blocks with six
+  // tables (the learned selector's domain; the rest fell back to plain)
+  int64_t learned_blocks = 0, six_table_blocks = 0;
 };
 
 struct CompressorConfig {

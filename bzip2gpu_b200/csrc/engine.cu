@@ -122,6 +122,10 @@ Workspace::Workspace(int mb, int64_t mr, int64_t me, int mt, int mrt, int mgt)
     dev.code = (int32_t *)alloc(B * kMaxGroups * kMaxAlpha * 4);
     dev.rfreq = (int32_t *)alloc(B * kMaxGroups * kMaxAlpha * 4);
     dev.learned = (int32_t *)alloc(B * 4);
+    dev.rfreq_m = (int32_t *)alloc(B * kMaxGroups * kMaxAlpha * 4);
+    dev.len2 = (uint8_t *)alloc(B * kMaxGroups * kMaxAlpha);
+    dev.est_sp = (int64_t *)alloc(B * 8);
+    dev.plain_left = (int32_t *)alloc(B * 4);
     dev.err = (int32_t *)alloc(64);
     BZ_CUDA(cudaMemset(dev.err, 0, 64));
     dev.sort_len = (int32_t *)alloc(B * 4);

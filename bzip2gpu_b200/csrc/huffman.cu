@@ -13,52 +13,77 @@ namespace bz2g {
 
 namespace {
 
-// Which blocks a pass serves: every block, the plain-selector blocks only, or
-// the learned-selector blocks only.
-enum Which { kAll = 0, kPlain = 1, kLearned = 2 };
+// Which blocks a launch serves: every block, the plain-selector blocks, the
+// learned-selector blocks, or (learned form, after the judge) the plain
+// blocks that still have passes to run in this round.
+enum Which { kAll = 0, kPlain = 1, kLearned = 2, kPlainRound = 3 };
 
-__device__ __forceinline__ bool serves(const SlabDev &d, int b, int which) {
-  return which == kAll || (which == kPlain) == (d.learned[b] == 0);
+__device__ __forceinline__ bool serves(const SlabDev &d, int b, int which, int round) {
+  switch (which) {
+    case kAll:
+      return true;
+    case kPlain:
+      return d.learned[b] == 0;
+    case kLearned:
+      return d.learned[b] != 0;
+    default:
+      return d.learned[b] == 0 && round < d.plain_left[b];
+  }
 }
 
-// learned_mode: blocks with six tables take the learned selector.
+// bzip2's initial tables (src/compression/huffman.cu:148-185): every length
+// 15, then table n_part - 1 gets length 0 over the next range of symbols
+// holding about remaining / n_part of the symbol count.  One warp.
+__device__ void init_tables(const SlabDev &d, int b) {
+  const int s = d.s[b];
+  const int ng = d.n_groups[b];
+  const int alpha = d.n_in_use[b] + 2;
+  uint8_t *len = d.len + (size_t)b * kMaxGroups * kMaxAlpha;
+  for (int i = lane_id(); i < kMaxGroups * kMaxAlpha; i += 32) len[i] = 15;
+  __syncwarp();
+  if (lane_id() == 0) {
+    const int32_t *freq = d.freq + (size_t)b * kMaxAlpha;
+    int gs = 0, remaining = s;
+    for (int n_part = ng; n_part > 0; n_part--) {
+      int t_freq = remaining / n_part;
+      int ge = gs - 1, a_freq = 0;
+      while (a_freq < t_freq && ge < alpha) {
+        ge++;
+        a_freq += ge < kMaxAlpha ? freq[ge] : 0;
+      }
+      if (ge > gs && n_part != ng && n_part != 1 && ((ng - n_part) % 2 == 1)) {
+        a_freq -= ge < kMaxAlpha ? freq[ge] : 0;
+        ge--;
+      }
+      uint8_t *row = len + (n_part - 1) * kMaxAlpha;
+      for (int v = 0; v < alpha; v++) row[v] = (v >= gs && v <= ge) ? 0 : 15;
+      gs = ge + 1;
+      remaining -= a_freq;
+    }
+  }
+  __syncwarp();
+}
+
+// learned_mode: blocks with six tables take the learned selector; the plain
+// blocks of the learned form have 2 passes left after the two shared ones.
 __global__ void k_huff_init(SlabDev d, int learned_mode) {
   const int b = blockIdx.x;
   const int s = d.s[b];
-  const int alpha = d.n_in_use[b] + 2;
-  uint8_t *len = d.len + (size_t)b * kMaxGroups * kMaxAlpha;
-  for (int i = threadIdx.x; i < kMaxGroups * kMaxAlpha; i += blockDim.x) len[i] = 15;
-  __syncwarp();
-  if (threadIdx.x != 0) return;
   const int ng = s < 200 ? 2 : s < 600 ? 3 : s < 1200 ? 4 : s < 2400 ? 5 : 6;
-  d.n_groups[b] = ng;
-  d.n_sel[b] = (s + 49) / 50;
-  d.learned[b] = (learned_mode && ng == kMaxGroups) ? 1 : 0;
-  // initial partition, src/compression/huffman.cu:148-185
-  const int32_t *freq = d.freq + (size_t)b * kMaxAlpha;
-  int gs = 0, remaining = s;
-  for (int n_part = ng; n_part > 0; n_part--) {
-    int t_freq = remaining / n_part;
-    int ge = gs - 1, a_freq = 0;
-    while (a_freq < t_freq && ge < alpha) {
-      ge++;
-      a_freq += ge < kMaxAlpha ? freq[ge] : 0;
-    }
-    if (ge > gs && n_part != ng && n_part != 1 && ((ng - n_part) % 2 == 1)) {
-      a_freq -= ge < kMaxAlpha ? freq[ge] : 0;
-      ge--;
-    }
-    uint8_t *row = len + (n_part - 1) * kMaxAlpha;
-    for (int v = 0; v < alpha; v++) row[v] = (v >= gs && v <= ge) ? 0 : 15;
-    gs = ge + 1;
-    remaining -= a_freq;
+  if (threadIdx.x == 0) {
+    d.n_groups[b] = ng;
+    d.n_sel[b] = (s + 49) / 50;
+    d.learned[b] = (learned_mode && ng == kMaxGroups) ? 1 : 0;
+    d.plain_left[b] = kIters - 2;
   }
+  __syncwarp();
+  init_tables(d, b);
 }
 
 // One thread per 50-symbol group.  Costs of all tables are packed in 10-bit
 // fields of one 64-bit word per symbol (50 * 17 < 1024), so a group's six
 // costs are one 64-bit sum.
-__global__ void __launch_bounds__(kGroupTile) k_huff_select(SlabDev d, int which) {
+__global__ void __launch_bounds__(kGroupTile) k_huff_select(SlabDev d, int which, int round) {
   __shared__ uint16_t sy[kGroupTile * kGroupSize];
   __shared__ uint64_t plen[kMaxAlpha];
   __shared__ int rf[kMaxGroups * kMaxAlpha];
@@ -66,7 +91,7 @@ __global__ void __launch_bounds__(kGroupTile) k_huff_select(SlabDev d, int which
   const int b = d.gt_block[gt];
   const int g0 = d.gt_first[gt];
   const int nsel = d.n_sel[b];
-  if (g0 >= nsel || !serves(d, b, which)) return;
+  if (g0 >= nsel || !serves(d, b, which, round)) return;
   const int ng_here = min(kGroupTile, nsel - g0);
   const int s = d.s[b];
   const int ngrp = d.n_groups[b];
@@ -119,7 +144,11 @@ constexpr int kNodeN = kMaxAlpha * 2;
 
 __device__ __forceinline__ uint32_t hw(uint64_t e) { return (uint32_t)(e >> 32); }
 
-__global__ void __launch_bounds__(kMaxGroups * 32) k_huff_lengths(SlabDev d, int which) {
+// split != 0 (the learned form's first table build, grid.y = 2): y = 0 builds
+// every block's tables from its counts (the MLP's counts for learned blocks),
+// y = 1 builds the single-pass estimate's tables of learned blocks into len2.
+__global__ void __launch_bounds__(kMaxGroups * 32) k_huff_lengths(SlabDev d, int which, int round,
+                                                                  int split) {
   __shared__ __align__(16) uint64_t heap_s[kMaxGroups][kHeapN + 2];
   __shared__ int32_t leafw_s[kMaxGroups][kMaxAlpha + 1];
   __shared__ int16_t parent_s[kMaxGroups][kNodeN];
@@ -127,13 +156,25 @@ __global__ void __launch_bounds__(kMaxGroups * 32) k_huff_lengths(SlabDev d, int
   const int t = warp_id();
   const int ln = lane_id();
   const int ngrp = d.n_groups[b];
-  if (t >= ngrp || !serves(d, b, which)) return;
+  if (t >= ngrp) return;
+  const int32_t *rf_base = d.rfreq;
+  uint8_t *len_base = d.len;
+  if (split) {
+    if (blockIdx.y == 0) {
+      if (d.learned[b]) rf_base = d.rfreq_m;
+    } else {
+      if (!d.learned[b]) return;
+      len_base = d.len2;
+    }
+  } else if (!serves(d, b, which, round)) {
+    return;
+  }
   const int alpha = d.n_in_use[b] + 2;
   uint64_t *heap = heap_s[t];
   int32_t *leafw = leafw_s[t];
   int16_t *parent = parent_s[t];
-  const int32_t *freq = d.rfreq + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
-  uint8_t *len = d.len + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
+  const int32_t *freq = rf_base + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
+  uint8_t *len = len_base + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
   for (int i = ln; i < alpha; i += 32) {
     int f = freq[i];
     leafw[i + 1] = (f == 0 ? 1 : f) << 8;
@@ -218,6 +259,50 @@ __global__ void __launch_bounds__(kMaxGroups * 32) k_huff_lengths(SlabDev d, int
   }
 }
 
+// Predicted coded size of a block's selection (bits): payload from the
+// per-table counts and lengths, plus the table headers (5-bit start, 2 bits
+// per unit of length change, 1 terminator bit per symbol).  One warp.
+__device__ int64_t predicted_bits(const SlabDev &d, int b, const uint8_t *len_base) {
+  const int ng = d.n_groups[b];
+  const int alpha = d.n_in_use[b] + 2;
+  const int32_t *rf = d.rfreq + (size_t)b * kMaxGroups * kMaxAlpha;
+  const uint8_t *len = len_base + (size_t)b * kMaxGroups * kMaxAlpha;
+  int64_t e = 0;
+  for (int t = 0; t < ng; t++)
+    for (int v = lane_id(); v < alpha; v += 32) {
+      const int l = len[t * kMaxAlpha + v];
+      const int p = v ? len[t * kMaxAlpha + v - 1] : l;
+      e += (int64_t)rf[t * kMaxAlpha + v] * l + 2 * abs(l - p) + 1;
+    }
+  for (int o = 16; o; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+  return e + 5 * ng;
+}
+
+// Learned form: the single-pass estimate (first plain pass over the initial
+// tables, its tables in len2).
+__global__ void k_huff_estimate(SlabDev d) {
+  const int b = blockIdx.x;
+  if (!d.learned[b]) return;
+  const int64_t e = predicted_bits(d, b, d.len2);
+  if (lane_id() == 0) d.est_sp[b] = e;
+}
+
+// Learned form, after the exact selection pass and its tables: a block whose
+// predicted size exceeds the single-pass estimate falls back to the plain
+// selector (initial tables, then 4 passes in the plain rounds).
+__global__ void k_huff_judge(SlabDev d) {
+  const int b = blockIdx.x;
+  if (!d.learned[b]) return;
+  const int64_t e = predicted_bits(d, b, d.len);
+  if (e <= d.est_sp[b]) return;
+  __syncwarp();
+  if (lane_id() == 0) {
+    d.learned[b] = 0;
+    d.plain_left[b] = kIters;
+  }
+  init_tables(d, b);
+}
+
 // Canonical codes (src/compression/huffman.cu:135-146,352-362).
 __global__ void k_huff_codes(SlabDev d) {
   const int b = blockIdx.x;
@@ -242,43 +327,52 @@ __global__ void k_huff_codes(SlabDev d) {
 }  // namespace
 
 namespace {
-void select_pass(const SlabDev &d, int which, cudaStream_t st) {
+void select_pass(const SlabDev &d, int which, int round, cudaStream_t st) {
   BZ_CUDA(cudaMemsetAsync(d.rfreq, 0, sizeof(int32_t) * kMaxGroups * kMaxAlpha * d.nblocks, st));
-  k_huff_select<<<d.n_group_tiles, kGroupTile, 0, st>>>(d, which);
+  k_huff_select<<<d.n_group_tiles, kGroupTile, 0, st>>>(d, which, round);
   BZ_LAUNCH_CHECK();
 }
-void lengths_pass(const SlabDev &d, int which, cudaStream_t st) {
-  k_huff_lengths<<<d.nblocks, kMaxGroups * 32, 0, st>>>(d, which);
+void lengths_pass(const SlabDev &d, int which, int round, cudaStream_t st) {
+  k_huff_lengths<<<d.nblocks, kMaxGroups * 32, 0, st>>>(d, which, round, 0);
   BZ_LAUNCH_CHECK();
 }
 }  // namespace
 
 // Plain form (the reference's): initial tables, then 4 passes of selection
-// and code lengths.  Learned form: blocks with six tables start from the
-// MLP's selection (code lengths from its choice) and take one exact
-// selection pass and code lengths; the other blocks run the plain passes in
-// the same launches (the later plain-only launches return at once for
-// learned blocks).
+// and code lengths.
+// Learned form, blocks with six tables: pass 1 over the initial tables gives
+// the plain single-pass estimate; the MLP's choice gives the first tables;
+// one exact selection pass and code lengths follow; if the predicted size is
+// above the single-pass estimate the block falls back to the plain selector.
+// Blocks with fewer tables run the plain passes in the same launches
+// (launches that serve none of a slab's blocks return at once).
 void stage_huffman(const SlabDev &d, cudaStream_t st, const uint8_t *learned, int plain_passes,
                    uint8_t *mlp_sel_out, size_t mlp_sel_bytes) {
   k_huff_init<<<d.nblocks, 32, 0, st>>>(d, learned ? 1 : 0);
   BZ_LAUNCH_CHECK();
   if (!learned) {
     for (int it = 0; it < plain_passes; it++) {
-      select_pass(d, kAll, st);
-      lengths_pass(d, kAll, st);
+      select_pass(d, kAll, 0, st);
+      lengths_pass(d, kAll, 0, st);
     }
   } else {
-    select_pass(d, kPlain, st);
-    mlp::launch_select(d, learned, nullptr, nullptr, st);
+    const size_t rf_bytes = sizeof(int32_t) * kMaxGroups * kMaxAlpha * d.nblocks;
+    BZ_CUDA(cudaMemsetAsync(d.rfreq_m, 0, rf_bytes, st));
+    select_pass(d, kAll, 0, st);
+    mlp::launch_select(d, learned, nullptr, nullptr, d.rfreq_m, st);
     if (mlp_sel_out)
       BZ_CUDA(cudaMemcpyAsync(mlp_sel_out, d.sel, mlp_sel_bytes, cudaMemcpyDeviceToDevice, st));
-    lengths_pass(d, kAll, st);
-    select_pass(d, kAll, st);
-    lengths_pass(d, kAll, st);
-    for (int it = 2; it < kIters; it++) {
-      select_pass(d, kPlain, st);
-      lengths_pass(d, kPlain, st);
+    k_huff_lengths<<<dim3(d.nblocks, 2), kMaxGroups * 32, 0, st>>>(d, kAll, 0, 1);
+    BZ_LAUNCH_CHECK();
+    k_huff_estimate<<<d.nblocks, 32, 0, st>>>(d);
+    BZ_LAUNCH_CHECK();
+    select_pass(d, kAll, 0, st);
+    lengths_pass(d, kAll, 0, st);
+    k_huff_judge<<<d.nblocks, 32, 0, st>>>(d);
+    BZ_LAUNCH_CHECK();
+    for (int r = 0; r < kIters; r++) {
+      select_pass(d, kPlainRound, r, st);
+      lengths_pass(d, kPlainRound, r, st);
     }
   }
   k_huff_codes<<<d.nblocks, 32, 0, st>>>(d);

@@ -153,7 +153,8 @@ __device__ __forceinline__ void epilogue_chunk(const uint32_t (&r)[32], float sc
 }
 
 __global__ void __launch_bounds__(kSelThreads, 1)
-    k_mlp_select(SlabDev d, const uint8_t *__restrict__ packed, float *logits) {
+    k_mlp_select(SlabDev d, const uint8_t *__restrict__ packed, float *logits,
+                 int32_t *rfreq_out) {
   extern __shared__ __align__(1024) uint8_t sm[];
   uint8_t *act = sm + kSAct;
   uint8_t *ring = sm + kSRing;
@@ -353,7 +354,7 @@ __global__ void __launch_bounds__(kSelThreads, 1)
         }
       }
       compute_any(false);
-      int32_t *rfreq = d.rfreq + (size_t)b * kMaxGroups * kMaxAlpha;
+      int32_t *rfreq = rfreq_out + (size_t)b * kMaxGroups * kMaxAlpha;
       for (int i = tid; i < kMaxGroups * kMaxAlpha; i += kComputeThreads)
         if (rf[i]) atomicAdd(&rfreq[i], rf[i]);
       compute_any(false);
@@ -724,13 +725,13 @@ void to_bf16(const float *params, bf16 *out, cudaStream_t st) {
 }
 
 void launch_select(const SlabDev &d, const uint8_t *packed, float *logits, int *err,
-                   cudaStream_t st) {
+                   int32_t *rfreq, cudaStream_t st) {
   smem_attr(k_mlp_select, kSelSmem, g_select_attr);
   if (d.n_group_tiles <= 0) return;
   SlabDev dd = d;
   if (err) dd.err = err;
   const int grid = std::min(d.n_group_tiles, num_sms());
-  k_mlp_select<<<grid, kSelThreads, kSelSmem, st>>>(dd, packed, logits);
+  k_mlp_select<<<grid, kSelThreads, kSelSmem, st>>>(dd, packed, logits, rfreq ? rfreq : d.rfreq);
   BZ_LAUNCH_CHECK();
 }
 

@@ -56,11 +56,12 @@ void pack(const float *params, uint8_t *packed, cudaStream_t st);
 void to_bf16(const float *params, __nv_bfloat16 *out, cudaStream_t st);
 
 // Learned selection over the slab's blocks with d.learned[b] != 0: writes
-// d.sel and adds the chosen tables' symbol counts into d.rfreq.  logits
-// (optional, debugging and tests): per group tile, 128 rows x 8 floats.
-// err: device flag, nonzero if a wait inside the kernel timed out.
+// d.sel and adds the chosen tables' symbol counts into rfreq (nullptr:
+// d.rfreq; same layout).  logits (optional, debugging and tests): per group
+// tile, 128 rows x 8 floats.  err: device word (nullptr: d.err), nonzero if a
+// wait inside the kernel timed out.
 void launch_select(const SlabDev &d, const uint8_t *packed, float *logits, int *err,
-                   cudaStream_t st);
+                   int32_t *rfreq, cudaStream_t st);
 
 // ---------------------------------------------------------------- training
 // Training-set tap of the compression pipeline: for every block with six

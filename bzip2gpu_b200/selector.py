@@ -248,10 +248,14 @@ def evaluate(P: np.ndarray, blocks: int = 20000, seed: int = 0xB2C3F, log=print)
             res["blocks"] = int(st["blocks"])
             if mode == "learned":
                 res["learned_blocks"] = int(st["learned_blocks"])
+                res["six_table_blocks"] = int(st["six_table_blocks"])
     finally:
         set_selector("plain")
         set_timing(False)
-    res["fallback_rate"] = 1.0 - res["learned_blocks"] / max(res["blocks"], 1)
+    # fallback: six-table blocks the judge gave back to the plain selector;
+    # blocks with fewer tables always use the plain selector
+    res["fallback_rate"] = 1.0 - res["learned_blocks"] / max(res["six_table_blocks"], 1)
+    res["plain_domain_blocks"] = res["blocks"] - res["six_table_blocks"]
     pick = list(range(0, len(specs), max(1, len(specs) // 64)))
     ok = sum(bz2.decompress(bytes(streams["learned"][i])) == inputs[i].cpu().numpy().tobytes()
              for i in pick)

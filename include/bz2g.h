@@ -88,7 +88,8 @@ int bz2g_set_engine(int slab_blocks, int workers);
  * then device ms of RLE1+CRC, BWT, MTF, RLE2, Huffman, sizes, placement,
  * then the radix-scatter kernel's timed launches, their summed device ms and
  * their algorithmic bytes (items read + written), then the blocks whose
- * tables came from the learned selector; returns the field count.
+ * tables came from the learned selector and the blocks with six tables;
+ * returns the field count.
  * bz2g_launch_count: kernels launched by this library since it was loaded. */
 int bz2g_set_timing(int on);
 int bz2g_last_stats(double *out, int n);

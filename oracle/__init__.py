@@ -60,6 +60,8 @@ def lib():
         L.orc_encode.argtypes = [_vp, _i, _vp, _vp, _vp, _vp]
         L.orc_selector_mtf.argtypes = [_vp, _i, _i, _vp]
         L.orc_huffman_refine.argtypes = [_vp, _i, _i, _vp, _i, _vp, _vp, _vp]
+        L.orc_huffman_learned.argtypes = [_vp, _i, _i, _vp, _vp, _vp, _vp, ctypes.POINTER(_i),
+                                          ctypes.POINTER(_i)]
         L.orc_coded_bits.restype = ctypes.c_int64
         L.orc_coded_bits.argtypes = [_vp, _i, _vp, _i, _i, _vp]
         L.orc_compress_block.argtypes = [_vp, _i, ctypes.POINTER(BlockInfo), _vp, _vp, _vp, _vp,
@@ -186,6 +188,21 @@ def huffman_refine(syms, n_in_use: int, sel_in, n_refine: int = 1):
     nsel = lib().orc_huffman_refine(s.ctypes.data, s.size, n_in_use, si.ctypes.data, n_refine,
                                     ln.ctypes.data, code.ctypes.data, sel.ctypes.data)
     return ln, code, sel[:nsel].copy()
+
+
+def huffman_learned(syms, n_in_use: int, sel_mlp):
+    """The learned form given the MLP's choices: (len, code, selectors,
+    n_groups, fell_back)."""
+    s = np.ascontiguousarray(syms, dtype=np.uint16)
+    sm = np.ascontiguousarray(sel_mlp, dtype=np.uint8)
+    ln = np.zeros((G, A), np.uint8)
+    code = np.zeros((G, A), np.int32)
+    sel = np.zeros(s.size // 50 + 2, np.uint8)
+    ng, fb = _i(), _i()
+    nsel = lib().orc_huffman_learned(s.ctypes.data, s.size, n_in_use, sm.ctypes.data,
+                                     ln.ctypes.data, code.ctypes.data, sel.ctypes.data,
+                                     ctypes.byref(ng), ctypes.byref(fb))
+    return ln, code, sel[:nsel].copy(), ng.value, bool(fb.value)
 
 
 def coded_bits(syms, selectors, n_groups: int, n_in_use: int, len_tab) -> int:

@@ -396,6 +396,63 @@ int orc_huffman_refine(const uint16_t *syms, int s, int alphabet_size, const uin
   return nsel;
 }
 
+/* Predicted coded size of a selection: payload from the per-table counts
+ * and lengths plus the table headers (5-bit start, 2 bits per unit of
+ * length change, 1 terminator bit per symbol); the selector codes are not
+ * counted.  Written from bzip2gpu_b200/csrc/huffman.cu (predicted_bits). */
+static int64_t predicted_bits(int ng, int alpha, int32_t rfreq[ORC_MAX_GROUPS][ORC_MAX_ALPHA],
+                              uint8_t len[ORC_MAX_GROUPS][ORC_MAX_ALPHA]) {
+  int64_t e = 5 * ng;
+  for (int t = 0; t < ng; t++)
+    for (int v = 0; v < alpha; v++) {
+      int l = len[t][v], p = v ? len[t][v - 1] : l;
+      e += (int64_t)rfreq[t][v] * l + 2 * (l > p ? l - p : p - l) + 1;
+    }
+  return e;
+}
+
+/* The learned form for one block given the MLP's choices sel_mlp (written
+ * from bzip2gpu_b200/csrc/huffman.cu's learned schedule): with six tables,
+ * the single-pass estimate is the first plain pass over the initial tables;
+ * the learned tables come from the MLP's choice, one exact selection pass and
+ * code lengths; if their predicted size exceeds the estimate, the block is
+ * coded with the plain selector (orc_huffman_build) and *fell_back = 1.
+ * Blocks with fewer tables are plain.  Returns the selector count. */
+int orc_huffman_learned(const uint16_t *syms, int s, int alphabet_size, const uint8_t *sel_mlp,
+                        uint8_t len[ORC_MAX_GROUPS][ORC_MAX_ALPHA],
+                        int32_t code[ORC_MAX_GROUPS][ORC_MAX_ALPHA], uint8_t *selectors,
+                        int *n_groups_out, int *fell_back) {
+  const int alpha = alphabet_size + 2;
+  const int ng = s < 200 ? 2 : s < 600 ? 3 : s < 1200 ? 4 : s < 2400 ? 5 : 6;
+  *fell_back = 0;
+  if (ng != ORC_MAX_GROUPS)
+    return orc_huffman_build(syms, s, alphabet_size, len, code, selectors, n_groups_out);
+  static __thread int32_t rfreq[ORC_MAX_GROUPS][ORC_MAX_ALPHA];
+  static __thread uint8_t lsp[ORC_MAX_GROUPS][ORC_MAX_ALPHA];
+  uint8_t *tmp_sel = (uint8_t *)malloc((s + 49) / 50 + 1);
+  /* single-pass estimate */
+  for (int g = 0; g < ORC_MAX_GROUPS; g++)
+    for (int v = 0; v < alpha; v++) lsp[g][v] = 15;
+  int32_t freqs[ORC_MAX_ALPHA] = {0};
+  for (int i = 0; i < s; i++) freqs[syms[i]]++;
+  orc_initial_assignment(ng, s, alpha, freqs, lsp);
+  select_pass(syms, s, ng, lsp, tmp_sel, rfreq);
+  for (int t = 0; t < ng; t++) orc_code_lengths(rfreq[t], lsp[t], alpha, 17);
+  const int64_t est = predicted_bits(ng, alpha, rfreq, lsp);
+  free(tmp_sel);
+  /* learned: MLP choice -> tables -> exact pass -> tables */
+  int nsel = orc_huffman_refine(syms, s, alphabet_size, sel_mlp, 0, len, code, selectors);
+  select_pass(syms, s, ng, len, selectors, rfreq);
+  for (int t = 0; t < ng; t++) orc_code_lengths(rfreq[t], len[t], alpha, 17);
+  if (predicted_bits(ng, alpha, rfreq, len) > est) {
+    *fell_back = 1;
+    return orc_huffman_build(syms, s, alphabet_size, len, code, selectors, n_groups_out);
+  }
+  canonical_codes(ng, alpha, len, code);
+  *n_groups_out = ng;
+  return nsel;
+}
+
 /* Bits of one block's coded part that depend on the table selection:
  * payload, the unary selector MTF codes, and the table deltas
  * (src/compression/compress.cu:300-345). */

@@ -86,6 +86,13 @@ int orc_huffman_refine(const uint16_t *syms, int s, int alphabet_size, const uin
                        int n_refine, uint8_t len[ORC_MAX_GROUPS][ORC_MAX_ALPHA],
                        int32_t code[ORC_MAX_GROUPS][ORC_MAX_ALPHA], uint8_t *selectors);
 
+/* The learned form given the MLP's choices, with the single-pass judge and
+ * the plain fallback (*fell_back).  Returns the selector count. */
+int orc_huffman_learned(const uint16_t *syms, int s, int alphabet_size, const uint8_t *sel_mlp,
+                        uint8_t len[ORC_MAX_GROUPS][ORC_MAX_ALPHA],
+                        int32_t code[ORC_MAX_GROUPS][ORC_MAX_ALPHA], uint8_t *selectors,
+                        int *n_groups_out, int *fell_back);
+
 /* Selection-dependent bits of a block: payload + unary selector MTF +
  * table deltas (src/compression/compress.cu:300-345). */
 int64_t orc_coded_bits(const uint16_t *syms, int s, const uint8_t *selectors, int ng,

@@ -146,16 +146,35 @@ def test_learned_build_matches_oracle_given_mlp_choices(torch_cuda, seed, n):
     ln, code, sel, ng, msel = B.huffman_build_learned(d_syms, info.n_in_use, d_P)
     a = info.n_in_use + 2
     if info.n_groups == 6:
-        ref_ln, ref_code, ref_sel = oracle.huffman_refine(syms, info.n_in_use, msel, 1)
         # the MLP's choices are those of the fused kernel
         lg, fsel = B.selector_logits(d_syms, d_P)
         assert np.array_equal(msel, fsel.cpu().numpy())
-    else:
-        ref_ln, ref_code, ref_sel, _ = oracle.huffman_build(syms, info.n_in_use)
-    assert ng == info.n_groups
+    ref_ln, ref_code, ref_sel, ref_ng, _ = oracle.huffman_learned(syms, info.n_in_use, msel)
+    assert ng == ref_ng == info.n_groups
     assert np.array_equal(sel, ref_sel)
     assert np.array_equal(ln[:ng, :a], ref_ln[:ng, :a])
     assert np.array_equal(code[:ng, :a], ref_code[:ng, :a])
+
+
+def test_learned_build_judge_both_ways(torch_cuda):
+    # the shipped parameters keep the learned tables on these blocks, untrained
+    # ones lose to the single-pass estimate and fall back to the plain
+    # selector; every block equals the oracle either way
+    outcomes = set()
+    for P in (S.load(), _params(99)):
+        d_P = torch_cuda.from_numpy(P).cuda()
+        for seed in range(30, 36):
+            st, info = _block_groups(seed, 250000)
+            syms = st["rle2"]
+            d_syms = torch_cuda.from_numpy(syms.astype(np.int16)).cuda()
+            ln, code, sel, ng, msel = B.huffman_build_learned(d_syms, info.n_in_use, d_P)
+            rl, rc, rs, rng_, fb = oracle.huffman_learned(syms, info.n_in_use, msel)
+            a = info.n_in_use + 2
+            assert ng == rng_ and np.array_equal(sel, rs)
+            assert np.array_equal(ln[:ng, :a], rl[:ng, :a])
+            assert np.array_equal(code[:ng, :a], rc[:ng, :a])
+            outcomes.add(fb)
+    assert outcomes == {True, False}
 
 
 def test_dataset_tap_groups_and_labels(torch_cuda):

@@ -105,3 +105,28 @@ def test_selector_specs_reach_block_count():
     # the same draws as the config-2 generator with that seed
     assert [(s.size, s.level) for s in sp[:5]] == \
         [(s.size, s.level) for s in W.batch_specs(5, 0xB2C3)]
+
+
+def test_learned_oracle_judge():
+    # the MLP's choice replaced by the plain selector's own final choice:
+    # one exact pass keeps (or improves) it, so no fallback; a constant
+    # choice (one table for every group) is worse than one plain pass, so the
+    # block falls back and equals the plain selector's coding
+    _, st, info = _groups(9, 600000)
+    syms = st["rle2"]
+    ln, code, sel, ng, fb = oracle.huffman_learned(syms, info.n_in_use, st["sel"])
+    assert not fb and ng == 6
+    ref = oracle.huffman_refine(syms, info.n_in_use, st["sel"], 1)
+    assert np.array_equal(sel, ref[2])
+    ln, code, sel, ng, fb = oracle.huffman_learned(syms, info.n_in_use,
+                                                   np.zeros_like(st["sel"]))
+    assert fb
+    assert np.array_equal(sel, st["sel"])
+    a = info.n_in_use + 2
+    assert np.array_equal(ln[:, :a], st["len"][:, :a])
+    # fewer than six tables: plain
+    _, st2, info2 = _groups(10, 1500)
+    assert info2.n_groups < 6
+    ln, code, sel, ng, fb = oracle.huffman_learned(st2["rle2"], info2.n_in_use,
+                                                   np.zeros(len(st2["sel"]), np.uint8))
+    assert not fb and np.array_equal(sel, st2["sel"])
