@@ -295,7 +295,10 @@ def main():
     assert olen == len(out) and bytes(h_out[:olen].numpy()) == out
     launches = (B.launch_count() - l0) // max(args.steps, 1)
     stats = B.last_stats()
-    # the batched form on the same stream (one input: blocks in one queue)
+    # the batched form on the same stream (one input: blocks in one queue),
+    # warmed like the plain form
+    for _ in range(args.warmup):
+        B.compress_batch([d_in], [9], [900000], out=h_out, on_device=True)
     bt, bout = timed(lambda: B.compress_batch([d_in], [9], [900000], out=h_out, on_device=True))
     assert bytes(bout[0]) == out
     bt = max_over_ranks(bt, world)
@@ -309,7 +312,8 @@ def main():
         SEL.load_default()
         B.set_selector("learned")
         try:
-            B.compress_batch([d_in], [9], [900000], out=h_out, on_device=True)  # warm
+            for _ in range(args.warmup):
+                B.compress_batch([d_in], [9], [900000], out=h_out, on_device=True)
             lt, lout = timed(lambda: B.compress_batch([d_in], [9], [900000], out=h_out,
                                                       on_device=True))
             lbytes = bytes(lout[0])

@@ -81,6 +81,8 @@ Compressor::Compressor(const CompressorConfig &cfg) : cfg_(cfg) {
 
 Compressor::~Compressor() {
   for (uint32_t *c : arena_chunks_) cudaFree(c);
+  if (splice_out_) cudaFree(splice_out_);
+  if (splice_meta_) cudaFree(splice_meta_);
 }
 
 // A run of `words` arena words for one slab (caller holds the batch lock):
@@ -546,12 +548,6 @@ void Compressor::compress_batch(const Item *items, int count, bool on_device, By
     if (err) std::rethrow_exception(err);
   }
 
-  struct Free {
-    void *p;
-    ~Free() {
-      if (p) cudaFree(p);
-    }
-  };
   // stream layout: item i occupies [offsets[i], offsets[i+1]) of the output
   const size_t base = out.size;
   offsets.assign(count + 1, base);
@@ -582,13 +578,24 @@ void Compressor::compress_batch(const Item *items, int count, bool on_device, By
   if (out.owned) out.reserve(base + pos + 8);
   BZ_REQUIRE(base + pos <= out.cap, kErrTooLarge, "output buffer too small");
   const int64_t owords = (int64_t)(pos + 3) / 4 + 1;
-  uint32_t *d_out = nullptr;
-  int64_t *d_meta = nullptr;
   cudaStream_t st = workers_[0]->st;
-  BZ_CUDA(cudaMalloc((void **)&d_out, sizeof(uint32_t) * owords));
-  Free free_out{d_out};
-  BZ_CUDA(cudaMalloc((void **)&d_meta, sizeof(int64_t) * 3 * std::max(nb, 1)));
-  Free free_meta{d_meta};
+  // the splice buffers are kept by the engine and grown when a call needs more
+  if (owords > splice_out_words_) {
+    if (splice_out_) BZ_CUDA(cudaFree(splice_out_));
+    splice_out_ = nullptr;
+    splice_out_words_ = 0;
+    BZ_CUDA(cudaMalloc((void **)&splice_out_, sizeof(uint32_t) * owords));
+    splice_out_words_ = owords;
+  }
+  if (nb > splice_meta_blocks_) {
+    if (splice_meta_) BZ_CUDA(cudaFree(splice_meta_));
+    splice_meta_ = nullptr;
+    splice_meta_blocks_ = 0;
+    BZ_CUDA(cudaMalloc((void **)&splice_meta_, sizeof(int64_t) * 3 * std::max(nb, 1)));
+    splice_meta_blocks_ = std::max(nb, 1);
+  }
+  uint32_t *d_out = splice_out_;
+  int64_t *d_meta = splice_meta_;
   BZ_CUDA(cudaMemsetAsync(d_out, 0, sizeof(uint32_t) * owords, st));
   BZ_CUDA(cudaMemcpyAsync(d_meta, h_src.data(), 8 * nb, cudaMemcpyHostToDevice, st));
   BZ_CUDA(cudaMemcpyAsync(d_meta + nb, h_dst.data(), 8 * nb, cudaMemcpyHostToDevice, st));

@@ -108,6 +108,10 @@ class Compressor {
   std::mutex call_mu_;                         // one call at a time per engine
   std::vector<uint32_t *> arena_chunks_;       // batched form: block bits
   std::vector<int64_t> arena_chunk_words_;
+  uint32_t *splice_out_ = nullptr;             // batched form: spliced streams
+  int64_t splice_out_words_ = 0;
+  int64_t *splice_meta_ = nullptr;             // per block: source, destination bit, bits
+  int64_t splice_meta_blocks_ = 0;
 };
 
 // Upper bound of the stream size for n bytes in nblocks blocks.
