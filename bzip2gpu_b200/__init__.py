@@ -23,7 +23,8 @@ __all__ = [
     "set_engine", "compress_into", "compress_device_into", "compress_batch", "rle1", "crc32", "bwt", "mtf", "symbols_table", "rle2", "huffman_build",
     "huffman_encode", "count_frequencies", "gen_markov", "gen_uniform", "MAX_GROUPS",
     "MAX_ALPHA", "SELECTOR_PARAMS", "selector_load", "set_selector", "get_selector",
-    "selector_logits", "huffman_build_learned", "selector_dataset",
+    "selector_logits", "huffman_build_learned", "selector_dataset", "compress_part",
+    "assemble",
 ]
 
 MAX_GROUPS = 6
@@ -63,6 +64,10 @@ _SIGS = {
     "bz2g_gen_markov": (_i, [_c.c_uint64, _vp, _i, _c.c_double, _c.c_double, _i, _i, _vp,
                              _c.c_int64, _i, _vp]),
     "bz2g_gen_uniform": (_i, [_c.c_uint64, _vp, _c.c_int64, _i, _vp]),
+    "bz2g_part_bound": (_sz, [_sz, _i]),
+    "bz2g_compress_part": (_i, [_vp, _sz, _i, _i, _vp, _sz, _c.POINTER(_c.c_int64),
+                                _c.POINTER(_c.c_uint32), _c.POINTER(_i)]),
+    "bz2g_assemble": (_i, [_i, _vp, _vp, _vp, _vp, _i, _vp, _sz, _c.POINTER(_sz)]),
     "bz2g_selector_load": (_i, [_vp, _sz]),
     "bz2g_set_selector": (_i, [_i]),
     "bz2g_get_selector": (_i, []),
@@ -457,4 +462,44 @@ def selector_dataset(d_inputs, levels, cap: int):
                                        ctypes.byref(got)))
     k = min(cap, got.value)
     return syms[:k], labels[:k], got.value
+
+
+# -------------------------------------------- one stream over several GPUs
+def compress_part(data, block_bytes: int = 900000):
+    """A part of a stream (whole blocks, no header, no end-of-stream marker)
+    in device memory of the current device: (uint8 CUDA tensor whose length
+    is a multiple of 4, bit count, CRC fold, blocks).  data: host bytes /
+    numpy array, or a CUDA uint8 tensor."""
+    import torch
+    on_dev = hasattr(data, "is_cuda") and data.is_cuda
+    if on_dev:
+        ptr, n, keep = data.data_ptr(), data.numel(), data
+    elif hasattr(data, "data_ptr"):
+        ptr, n, keep = data.data_ptr(), data.numel(), data
+    else:
+        keep, ptr = _host_view(data)
+        n = keep.size
+    cap = lib().bz2g_part_bound(n, block_bytes)
+    cap = (cap + 3) // 4 * 4
+    part = torch.empty(cap, dtype=torch.uint8, device="cuda")
+    bits, fold, nb = ctypes.c_int64(), ctypes.c_uint32(), _i()
+    _check(lib().bz2g_compress_part(ptr if n else None, n, block_bytes, int(on_dev), _ptr(part),
+                                    cap, ctypes.byref(bits), ctypes.byref(fold), ctypes.byref(nb)))
+    used = ((bits.value + 7) // 8 + 3) // 4 * 4
+    return part[:used], bits.value, fold.value, nb.value
+
+
+def assemble(parts, bits, folds, nblocks, level: int = 9) -> bytes:
+    """One .bz2 stream from parts (CUDA uint8 tensors on the current device,
+    in stream order) with their bit counts, CRC folds and block counts."""
+    k = len(parts)
+    ptrs = (ctypes.c_void_p * max(k, 1))(*[p.data_ptr() for p in parts])
+    b = (ctypes.c_int64 * max(k, 1))(*[int(x) for x in bits])
+    f = (ctypes.c_uint32 * max(k, 1))(*[int(x) & 0xFFFFFFFF for x in folds])
+    nb = (ctypes.c_int * max(k, 1))(*[int(x) for x in nblocks])
+    cap = int(sum(int(x) for x in bits) // 8) + 64
+    out = np.empty(cap, np.uint8)
+    ln = _sz()
+    _check(lib().bz2g_assemble(k, ptrs, b, f, nb, level, out.ctypes.data, cap, ctypes.byref(ln)))
+    return out[: ln.value].tobytes()
 

@@ -797,3 +797,110 @@ int bz2g_mlp_status(void *stream) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------ one stream over several GPUs
+extern "C" {
+
+size_t bz2g_part_bound(size_t n, int block_bytes) {
+  if (block_bytes <= 0) block_bytes = 900000;
+  size_t nb = (n + block_bytes - 1) / block_bytes;
+  return stream_bound((int64_t)n, (int64_t)nb) + 16;
+}
+
+int bz2g_compress_part(const uint8_t *in, size_t n, int block_bytes, int on_device,
+                       uint8_t *d_part, size_t cap, int64_t *bits, uint32_t *crc_fold,
+                       int *nblocks) {
+  return guard([&] {
+    BZ_REQUIRE(d_part && bits && crc_fold && nblocks, kErrArg, "null output pointer");
+    BZ_REQUIRE(block_bytes > 0 && block_bytes <= (1 << 24), kErrArg,
+               "block_bytes must be in (0, 16 MiB]");
+    BZ_REQUIRE(n == 0 || in != nullptr, kErrArg, "null input");
+    BZ_REQUIRE((uintptr_t)d_part % 4 == 0, kErrArg, "part buffer must be 4-byte aligned");
+    const int64_t nb = ((int64_t)n + block_bytes - 1) / block_bytes;
+    std::vector<const uint8_t *> ptrs(nb);
+    std::vector<int> lens(nb);
+    for (int64_t b = 0; b < nb; b++) {
+      ptrs[b] = in + b * (int64_t)block_bytes;
+      lens[b] = (int)std::min<int64_t>(block_bytes, (int64_t)n - b * (int64_t)block_bytes);
+    }
+    ByteSink sink(d_part, cap);
+    BZ_REQUIRE(sink.device, kErrArg, "the part buffer must be device memory");
+    Compressor &c = engine_for(std::max<int64_t>(block_bytes, 1));
+    const_cast<CompressorConfig &>(c.config()).time_stages = g_timing;
+    const_cast<CompressorConfig &>(c.config()).selector = current_selector();
+    const_cast<CompressorConfig &>(c.config()).plain_passes = current_passes();
+    g_last_stats = StageTimes();
+    int64_t b = 0;
+    uint32_t f = 0;
+    if (nb > 0) c.compress_part(ptrs.data(), lens.data(), (int)nb, on_device != 0, sink, &b, &f,
+                                &g_last_stats);
+    // zero the bytes after the part up to a 4-byte boundary (splice reads words)
+    const size_t used = (size_t)((b + 7) / 8);
+    const size_t end = (used + 3) / 4 * 4;
+    BZ_REQUIRE(end <= cap, kErrTooLarge, "part buffer too small");
+    if (end > used) BZ_CUDA(cudaMemset(d_part + used, 0, end - used));
+    BZ_CUDA(cudaDeviceSynchronize());
+    *bits = b;
+    *crc_fold = f;
+    *nblocks = (int)nb;
+  });
+}
+
+int bz2g_assemble(int nparts, const uint8_t *const *d_parts, const int64_t *bits,
+                  const uint32_t *crc_folds, const int *nblocks, int level, uint8_t *out,
+                  size_t cap, size_t *out_len) {
+  return guard([&] {
+    BZ_REQUIRE(nparts >= 0 && out && out_len && (nparts == 0 || (d_parts && bits && crc_folds &&
+                                                                   nblocks)),
+               kErrArg, "bad arguments");
+    const int lvl = std::min(std::max(level, 1), 9);
+    int64_t total = 32;
+    uint32_t crc = 0;
+    // splice in segments of 2^20 source words, one CTA each
+    const int64_t seg_bits = int64_t(1) << 25;
+    std::vector<int64_t> src, dst, nb;
+    for (int r = 0; r < nparts; r++) {
+      BZ_REQUIRE(bits[r] >= 0 && (bits[r] == 0 || d_parts[r]), kErrArg, "bad part");
+      BZ_REQUIRE((uintptr_t)d_parts[r] % 4 == 0, kErrArg, "parts must be 4-byte aligned");
+      for (int64_t o = 0; o < bits[r]; o += seg_bits) {
+        src.push_back((int64_t)(uintptr_t)(d_parts[r] + o / 8));
+        dst.push_back(total + o);
+        nb.push_back(std::min<int64_t>(seg_bits, bits[r] - o));
+      }
+      total += bits[r];
+      const int k = ((nblocks[r] % 32) + 32) % 32;
+      crc = (k ? ((crc << k) | (crc >> (32 - k))) : crc) ^ crc_folds[r];
+    }
+    const size_t stream_bytes = (size_t)((total + 80 + 7) / 8);
+    BZ_REQUIRE(stream_bytes <= cap, kErrTooLarge, "output buffer too small");
+    const int64_t words = (total + 31) / 32 + 1;
+    const int ns = (int)src.size();
+    cudaStream_t st = 0;
+    uint32_t *d_out = nullptr;
+    int64_t *d_meta = nullptr;
+    BZ_CUDA(cudaMallocAsync((void **)&d_out, sizeof(uint32_t) * words, st));
+    BZ_CUDA(cudaMallocAsync((void **)&d_meta, sizeof(int64_t) * 3 * std::max(ns, 1), st));
+    BZ_CUDA(cudaMemsetAsync(d_out, 0, sizeof(uint32_t) * words, st));
+    if (ns > 0) {
+      BZ_CUDA(cudaMemcpyAsync(d_meta, src.data(), 8 * ns, cudaMemcpyHostToDevice, st));
+      BZ_CUDA(cudaMemcpyAsync(d_meta + ns, dst.data(), 8 * ns, cudaMemcpyHostToDevice, st));
+      BZ_CUDA(cudaMemcpyAsync(d_meta + 2 * ns, nb.data(), 8 * ns, cudaMemcpyHostToDevice, st));
+      launch_splice(d_meta, d_meta + ns, d_meta + 2 * ns, ns, d_out, st);
+    }
+    const size_t body = (size_t)((total + 7) / 8);
+    BZ_CUDA(cudaMemcpyAsync(out, d_out, body, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaFreeAsync(d_meta, st));
+    BZ_CUDA(cudaFreeAsync(d_out, st));
+    BZ_CUDA(cudaStreamSynchronize(st));
+    out[0] = 'B';
+    out[1] = 'Z';
+    out[2] = 'h';
+    out[3] = (uint8_t)('0' + lvl);
+    ByteSink view(out, cap);
+    view.size = body;
+    put_eos(view, 0, total, crc);
+    *out_len = view.size;
+  });
+}
+
+}  // extern "C"

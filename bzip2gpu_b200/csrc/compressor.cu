@@ -110,10 +110,12 @@ uint32_t *Compressor::arena_take(int64_t words, size_t *chunk, int64_t *used, in
 
 ByteSink::ByteSink(uint8_t *p, size_t c) : data(p), size(0), cap(c), owned(false) {
   cudaPointerAttributes a;
-  if (cudaPointerGetAttributes(&a, p) == cudaSuccess)
+  if (cudaPointerGetAttributes(&a, p) == cudaSuccess) {
     pinned = a.type == cudaMemoryTypeHost;
-  else
+    device = a.type == cudaMemoryTypeDevice;
+  } else {
     cudaGetLastError();
+  }
 }
 
 ByteSink::~ByteSink() {
@@ -148,6 +150,16 @@ size_t stream_bound(int64_t n, int64_t nblocks) {
 }
 
 namespace {
+// Device sinks: the first bytes of a slab's part share a word with the
+// previous slab's last bytes; OR them in (or store them past the end).
+__global__ void k_merge_head(uint8_t *dst, uint32_t head, int n, int64_t keep) {
+  for (int i = 0; i < n; i++) {
+    const uint8_t b = (uint8_t)(head >> (8 * i));
+    if (i < keep) dst[i] |= b;
+    else dst[i] = b;
+  }
+}
+
 // The selector's tensor-core kernel bounds every wait; a wait that ran out
 // leaves a nonzero error word in the workspace (read back with the sizes).
 void check_err_word(const int32_t *h_err) {
@@ -155,6 +167,8 @@ void check_err_word(const int32_t *h_err) {
              "learned selector: a tensor-core wait timed out (error word " +
                  std::to_string(*h_err) + ")");
 }
+
+}  // namespace
 
 // 48-bit end-of-stream magic then the 32-bit combined CRC, MSB first, then
 // padding to a byte (src/compression/compress.cu:366-376).
@@ -171,7 +185,6 @@ void put_eos(ByteSink &out, size_t base, int64_t bit, uint32_t crc) {
   put(magic, 48);
   put(crc, 32);
 }
-}  // namespace
 
 void Compressor::compress(const uint8_t *const *ptrs, const int *lens, int nblocks, int level,
                           ByteSink &out, StageTimes *times) {
@@ -190,8 +203,16 @@ void Compressor::compress(const uint8_t *const *ptrs, const int *lens, int nbloc
   out.insert(out.end(), s.data, s.data + s.size);
 }
 
+void Compressor::compress_part(const uint8_t *const *ptrs, const int *lens, int nblocks,
+                               bool on_device, ByteSink &out, int64_t *bits, uint32_t *crc_fold,
+                               StageTimes *times) {
+  BZ_REQUIRE(out.device && !out.owned, kErrArg, "a part is written to a device buffer");
+  run(ptrs, lens, nblocks, 9, on_device, out, times, true, bits, crc_fold);
+}
+
 void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, int level,
-                     bool on_device, ByteSink &out, StageTimes *times) {
+                     bool on_device, ByteSink &out, StageTimes *times, bool part,
+                     int64_t *part_bits, uint32_t *part_crc) {
   std::lock_guard<std::mutex> call_lock(call_mu_);
   int64_t ntot = 0;
   for (int b = 0; b < nblocks; b++) {
@@ -205,18 +226,21 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
   const size_t bound = stream_bound(ntot, nblocks);
   if (out.owned) out.reserve(base + bound);
   BZ_REQUIRE(base + 14 <= out.cap, kErrTooLarge, "output buffer too small");
-  out.data[base + 0] = 'B';
-  out.data[base + 1] = 'Z';
-  out.data[base + 2] = 'h';
-  out.data[base + 3] = (uint8_t)('0' + level);
-  out.size = base + 4;
+  BZ_REQUIRE(!out.device || part, kErrArg, "whole streams are written to host memory");
+  if (!part) {
+    out.data[base + 0] = 'B';
+    out.data[base + 1] = 'Z';
+    out.data[base + 2] = 'h';
+    out.data[base + 3] = (uint8_t)('0' + level);
+    out.size = base + 4;
+  }
   const int B = cfg_.slab_blocks;
   const int nslabs = (nblocks + B - 1) / B;
 
   std::mutex mu;
   std::condition_variable cv;
   int next_offset = 0, next_append = 0;
-  int64_t bit = 32;
+  int64_t bit = part ? 0 : 32;
   uint32_t stream_crc = 0;
   std::exception_ptr err;
   std::atomic<int> next_slab{0};
@@ -326,7 +350,11 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
       const int64_t head = std::min<int64_t>(4, nbytes);
       BZ_CUDA(cudaMemcpyAsync(w.h_out, d.out, head, cudaMemcpyDeviceToHost, w.st));
       if (nbytes > head) {
-        if (out.pinned) {
+        if (out.device) {
+          BZ_CUDA(cudaMemcpyAsync(out.data + at + head, (const uint8_t *)d.out + head,
+                                  nbytes - head, cudaMemcpyDeviceToDevice, w.st));
+          BZ_CUDA(cudaStreamSynchronize(w.st));
+        } else if (out.pinned) {
           BZ_CUDA(cudaMemcpyAsync(out.data + at + head, (const uint8_t *)d.out + head,
                                   nbytes - head, cudaMemcpyDeviceToHost, w.st));
           BZ_CUDA(cudaStreamSynchronize(w.st));
@@ -365,9 +393,18 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
         cv.wait(g, [&] { return next_append == k || err; });
         if (err) return;
         // bytes [at, out.size) hold the previous slab's tail (<= 4 bytes)
-        for (int64_t i = 0; i < head; i++) {
-          if (at + i < out.size) out.data[at + i] |= w.h_out[i];
-          else out.data[at + i] = w.h_out[i];
+        if (out.device) {
+          uint32_t hv = 0;
+          for (int64_t i = 0; i < head; i++) hv |= (uint32_t)w.h_out[i] << (8 * i);
+          const int64_t keep = (int64_t)out.size > (int64_t)at ? (int64_t)out.size - (int64_t)at : 0;
+          k_merge_head<<<1, 1, 0, w.st>>>(out.data + at, hv, (int)head, keep);
+          BZ_LAUNCH_CHECK();
+          BZ_CUDA(cudaStreamSynchronize(w.st));
+        } else {
+          for (int64_t i = 0; i < head; i++) {
+            if (at + i < out.size) out.data[at + i] |= w.h_out[i];
+            else out.data[at + i] = w.h_out[i];
+          }
         }
         out.size = at + (size_t)nbytes;
         next_append++;
@@ -394,7 +431,12 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
     out.size = base;
     std::rethrow_exception(err);
   }
-  put_eos(out, base, bit, stream_crc);
+  if (part) {
+    if (part_bits) *part_bits = bit;
+    if (part_crc) *part_crc = stream_crc;
+  } else {
+    put_eos(out, base, bit, stream_crc);
+  }
   if (times) *times = tsum;
 }
 

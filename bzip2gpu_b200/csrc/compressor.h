@@ -55,6 +55,7 @@ struct ByteSink {
   size_t size = 0, cap = 0;
   bool owned = true;
   bool pinned = false;  // data is page-locked: device copies land in it directly
+  bool device = false;  // data is device memory (caller buffer)
   ByteSink() = default;
   ByteSink(uint8_t *p, size_t c);  // caller buffer
   ~ByteSink();
@@ -77,6 +78,13 @@ class Compressor {
   // d_ptrs[b]).
   void compress_device(const uint8_t *const *d_ptrs, const int *lens, int nblocks, int level,
                        ByteSink &out, StageTimes *times = nullptr);
+  // A part of a stream for sharding one stream over several GPUs: the blocks'
+  // bits from bit 0 of out (device memory, caller buffer), no stream header
+  // and no end-of-stream marker.  *bits: the part's bit count; *crc_fold: the
+  // blocks' CRCs folded as the stream CRC is (rotate left 1, xor) from 0.
+  void compress_part(const uint8_t *const *ptrs, const int *lens, int nblocks, bool on_device,
+                     ByteSink &out, int64_t *bits, uint32_t *crc_fold,
+                     StageTimes *times = nullptr);
   // Convenience for callers holding a std::vector (appends).
   void compress(const uint8_t *const *ptrs, const int *lens, int nblocks, int level,
                 std::vector<uint8_t> &out, StageTimes *times = nullptr);
@@ -99,7 +107,8 @@ class Compressor {
  private:
   struct Worker;
   void run(const uint8_t *const *ptrs, const int *lens, int nblocks, int level, bool on_device,
-           ByteSink &out, StageTimes *times);
+           ByteSink &out, StageTimes *times, bool part = false, int64_t *part_bits = nullptr,
+           uint32_t *part_crc = nullptr);
   uint32_t *arena_take(int64_t words, size_t *chunk, int64_t *used, int64_t *base);
   static constexpr int64_t kArenaChunkWords = int64_t(1) << 28;  // 1 GiB
   CompressorConfig cfg_;
@@ -116,5 +125,9 @@ class Compressor {
 
 // Upper bound of the stream size for n bytes in nblocks blocks.
 size_t stream_bound(int64_t n, int64_t nblocks);
+
+// End-of-stream marker and combined CRC at stream bit `bit` of out (host),
+// counted from out.data + base; grows out.size to the padded end.
+void put_eos(ByteSink &out, size_t base, int64_t bit, uint32_t crc);
 
 }  // namespace bz2g

@@ -177,6 +177,31 @@ int bz2g_huffman_encode(const uint16_t *d_syms, int s, const uint8_t *len, const
  *           src/compression/huffman.cu:126-133 */
 int bz2g_count_frequencies(const uint16_t *d_syms, int s, int32_t *d_freqs, void *stream);
 
+/* ------------------------------------------- one stream over several GPUs */
+/* No counterpart in the reference (one GPU).  Blocks are independent, so a
+ * stream is cut into parts of whole blocks, each compressed on its own GPU;
+ * the only exchange is each part's bit count and CRC fold, then the parts are
+ * spliced at their bit offsets.
+ * bz2g_compress_part: the blocks of in[0..n) (block_bytes raw bytes each;
+ * on_device != 0: in is device memory) compressed into a part starting at
+ * bit 0 of d_part (device memory of the current device, cap bytes, at least
+ * bz2g_part_bound(n, block_bytes)); no stream header, no end-of-stream
+ * marker; the bytes after the part up to the next 4-byte boundary are zero.
+ * *bits: the part's bit count; *crc_fold: its blocks' CRCs folded as the
+ * stream CRC is (rotate left by 1, xor) starting from 0; *nblocks: its blocks.
+ * A stream = header + parts in order + marker; its CRC folds the parts'
+ * folds: crc = rotl(crc, nblocks_r) ^ crc_fold_r. */
+size_t bz2g_part_bound(size_t n, int block_bytes);
+int bz2g_compress_part(const uint8_t *in, size_t n, int block_bytes, int on_device,
+                       uint8_t *d_part, size_t cap, int64_t *bits, uint32_t *crc_fold,
+                       int *nblocks);
+/* The parts (device memory of the current device, each 4-byte aligned) spliced
+ * after 'BZh' + level into one .bz2 stream in host memory out[0..cap), with
+ * the end-of-stream marker and the combined CRC; *out_len: its length. */
+int bz2g_assemble(int nparts, const uint8_t *const *d_parts, const int64_t *bits,
+                  const uint32_t *crc_folds, const int *nblocks, int level, uint8_t *out,
+                  size_t cap, size_t *out_len);
+
 /* ------------------------------------------------- learned table selector */
 /* No counterpart in the reference.  An MLP 258 -> 256 -> 256 -> 6 (ReLU, bf16
  * weights, fp32 accumulation on the tensor cores) over each 50-symbol

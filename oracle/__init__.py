@@ -68,6 +68,12 @@ def lib():
                                          _vp]
         L.orc_compress.restype = ctypes.c_int64
         L.orc_compress.argtypes = [_vp, ctypes.c_int64, _i, _i, _vp, ctypes.c_int64, _i]
+        L.orc_compress_part.restype = ctypes.c_int64
+        L.orc_compress_part.argtypes = [_vp, ctypes.c_int64, _i, _vp, ctypes.c_int64, _i,
+                                        ctypes.POINTER(ctypes.c_int64),
+                                        ctypes.POINTER(ctypes.c_uint32)]
+        L.orc_assemble.restype = ctypes.c_int64
+        L.orc_assemble.argtypes = [_i, _vp, _vp, _vp, _vp, _i, _vp, ctypes.c_int64]
         L.orc_compress_bound.restype = ctypes.c_int64
         L.orc_compress_bound.argtypes = [ctypes.c_int64, _i]
         _lib = L
@@ -249,3 +255,34 @@ def compress(data, level: int = 9, block_bytes: int = 900000, threads: int = 1) 
     if n < 0:
         raise RuntimeError("oracle output buffer too small")
     return out[:n].tobytes()
+
+
+def compress_part(data, block_bytes: int = 900000, threads: int = 1):
+    """(part bytes, bits, crc fold, blocks) of the blocks of data."""
+    a = _u8(data)
+    cap = lib().orc_compress_bound(a.size, block_bytes)
+    out = np.zeros(cap + 8, np.uint8)
+    bits = ctypes.c_int64()
+    fold = ctypes.c_uint32()
+    n = lib().orc_compress_part(a.ctypes.data if a.size else None, a.size, block_bytes,
+                                out.ctypes.data, cap, threads, ctypes.byref(bits),
+                                ctypes.byref(fold))
+    if n < 0:
+        raise RuntimeError("oracle output buffer too small")
+    nb = (a.size + block_bytes - 1) // block_bytes
+    return out[:n].copy(), bits.value, fold.value, nb
+
+
+def assemble(parts, bits, folds, nblocks, level: int = 9) -> bytes:
+    k = len(parts)
+    arrs = [np.ascontiguousarray(p, dtype=np.uint8) for p in parts]
+    ptrs = (ctypes.c_void_p * max(k, 1))(*[p.ctypes.data for p in arrs])
+    b = np.ascontiguousarray(bits, dtype=np.int64)
+    f = np.ascontiguousarray(folds, dtype=np.uint32)
+    nb = np.ascontiguousarray(nblocks, dtype=np.int32)
+    cap = int(sum(p.size for p in arrs)) + 64
+    out = np.zeros(cap, np.uint8)
+    n = lib().orc_assemble(k, ptrs, b.ctypes.data, f.ctypes.data, nb.ctypes.data, level,
+                           out.ctypes.data, cap)
+    return out[:n].tobytes()
+

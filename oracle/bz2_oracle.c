@@ -632,14 +632,19 @@ int64_t orc_compress_bound(int64_t n, int block_bytes) {
   return 64 + nb * 1400 + (n / 4 + 4 * nb) * 17 / 8 + n * 17 / 8;
 }
 
-/* src/compression/compress.cu:184-378 */
-int64_t orc_compress(const uint8_t *in, int64_t n, int level, int block_bytes,
-                     uint8_t *out, int64_t cap, int threads) {
+/* src/compression/compress.cu:184-378.  part != 0: no stream header and no
+ * end-of-stream marker; *part_bits and *part_fold get the bit count and the
+ * blocks' CRC fold. */
+static int64_t compress_impl(const uint8_t *in, int64_t n, int level, int block_bytes,
+                             uint8_t *out, int64_t cap, int threads, int part,
+                             int64_t *part_bits, uint32_t *part_fold) {
   if (level < 1) level = 1;
   if (level > 9) level = 9;
   if (block_bytes <= 0) block_bytes = 900000;
   bitw w = {out, cap, 0, 0, 0, 0};
-  bw_put(&w, 0x42, 8); bw_put(&w, 0x5A, 8); bw_put(&w, 0x68, 8); bw_put(&w, 0x30 + level, 8);
+  if (!part) {
+    bw_put(&w, 0x42, 8); bw_put(&w, 0x5A, 8); bw_put(&w, 0x68, 8); bw_put(&w, 0x30 + level, 8);
+  }
   int nblocks = (int)((n + block_bytes - 1) / block_bytes);
   blk_out *blocks = (blk_out *)calloc(nblocks > 0 ? nblocks : 1, sizeof(blk_out));
   pool_ctx ctx;
@@ -713,9 +718,52 @@ int64_t orc_compress(const uint8_t *in, int64_t n, int level, int block_bytes,
     free(o->payload);
   }
   free(blocks);
+  if (part) {
+    *part_bits = w.pos * 8 + w.nacc;
+    *part_fold = stream_crc;
+    bw_flush(&w);
+    return w.overflow ? -1 : w.pos;
+  }
   bw_put(&w, 0x17, 8); bw_put(&w, 0x72, 8); bw_put(&w, 0x45, 8);
   bw_put(&w, 0x38, 8); bw_put(&w, 0x50, 8); bw_put(&w, 0x90, 8);
   bw_put(&w, stream_crc, 32);
+  bw_flush(&w);
+  return w.overflow ? -1 : w.pos;
+}
+
+int64_t orc_compress(const uint8_t *in, int64_t n, int level, int block_bytes,
+                     uint8_t *out, int64_t cap, int threads) {
+  return compress_impl(in, n, level, block_bytes, out, cap, threads, 0, NULL, NULL);
+}
+
+/* A part: the blocks' bits from bit 0, no header, no marker.  Returns the
+ * bytes written (-1 if cap is too small). */
+int64_t orc_compress_part(const uint8_t *in, int64_t n, int block_bytes, uint8_t *out,
+                          int64_t cap, int threads, int64_t *bits, uint32_t *fold) {
+  return compress_impl(in, n, 9, block_bytes, out, cap, threads, 1, bits, fold);
+}
+
+/* Header + parts in order + end-of-stream marker with the CRC combined from
+ * the parts' folds (crc = rotl(crc, nblocks_r) ^ fold_r). */
+int64_t orc_assemble(int nparts, const uint8_t *const *parts, const int64_t *bits,
+                     const uint32_t *folds, const int *nblocks, int level, uint8_t *out,
+                     int64_t cap) {
+  if (level < 1) level = 1;
+  if (level > 9) level = 9;
+  bitw w = {out, cap, 0, 0, 0, 0};
+  bw_put(&w, 0x42, 8); bw_put(&w, 0x5A, 8); bw_put(&w, 0x68, 8); bw_put(&w, 0x30 + level, 8);
+  uint32_t crc = 0;
+  for (int r = 0; r < nparts; r++) {
+    int64_t full = bits[r] / 8;
+    for (int64_t i = 0; i < full; i++) bw_put(&w, parts[r][i], 8);
+    int rem = (int)(bits[r] % 8);
+    if (rem) bw_put(&w, parts[r][full] >> (8 - rem), rem);
+    int k = nblocks[r] % 32;
+    crc = (k ? ((crc << k) | (crc >> (32 - k))) : crc) ^ folds[r];
+  }
+  bw_put(&w, 0x17, 8); bw_put(&w, 0x72, 8); bw_put(&w, 0x45, 8);
+  bw_put(&w, 0x38, 8); bw_put(&w, 0x50, 8); bw_put(&w, 0x90, 8);
+  bw_put(&w, crc, 32);
   bw_flush(&w);
   return w.overflow ? -1 : w.pos;
 }

@@ -146,6 +146,14 @@ int orc_compress_block(const uint8_t *raw, int n, orc_block_info *info,
 int64_t orc_compress(const uint8_t *in, int64_t n, int level, int block_bytes,
                      uint8_t *out, int64_t cap, int threads);
 
+/* A part of a stream (the blocks' bits from bit 0, no header, no marker) and
+ * the assembly of parts into a stream; see bzip2gpu_b200/shard.py. */
+int64_t orc_compress_part(const uint8_t *in, int64_t n, int block_bytes, uint8_t *out,
+                          int64_t cap, int threads, int64_t *bits, uint32_t *fold);
+int64_t orc_assemble(int nparts, const uint8_t *const *parts, const int64_t *bits,
+                     const uint32_t *folds, const int *nblocks, int level, uint8_t *out,
+                     int64_t cap);
+
 /* Upper bound of orc_compress's output size. */
 int64_t orc_compress_bound(int64_t n, int block_bytes);
 
