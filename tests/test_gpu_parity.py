@@ -220,3 +220,17 @@ def test_levels_set_header_digit_only(torch_cuda):
     for lvl in range(1, 10):
         s = B.compress(a, lvl)
         assert s[:4] == b"BZh" + bytes([48 + lvl]) and s[4:] == base[4:]
+
+
+def test_config1_stress_stream_bit_exact(torch_cuda):
+    # config 1: zeros | periodic-17 | uniform | Markov, 64 MiB each, 900,000-byte
+    # blocks across segment borders; the whole stream byte-identical to the
+    # oracle.  The uniform segment has blocks whose RLE1 output exceeds
+    # 900,000 bytes (the reference's split keeps them; libbz2 would reject
+    # those blocks), counted here.
+    a = W.stress()
+    got = B.compress_device(dev(torch_cuda, a), 9)
+    assert got == oracle.compress(a, 9, threads=16)
+    long_blocks = sum(oracle.rle1(a[i:i + 900000]).size > 900000 for i in range(0, a.size, 900000))
+    print(f"config 1: {len(got)} bytes, {long_blocks} blocks with RLE1 output > 900,000 bytes")
+    assert long_blocks > 0
