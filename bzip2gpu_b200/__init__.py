@@ -24,7 +24,7 @@ __all__ = [
     "huffman_encode", "count_frequencies", "gen_markov", "gen_uniform", "MAX_GROUPS",
     "MAX_ALPHA", "SELECTOR_PARAMS", "selector_load", "set_selector", "get_selector",
     "selector_logits", "huffman_build_learned", "selector_dataset", "compress_part",
-    "assemble",
+    "assemble", "compress_file",
 ]
 
 MAX_GROUPS = 6
@@ -64,6 +64,7 @@ _SIGS = {
     "bz2g_gen_markov": (_i, [_c.c_uint64, _vp, _i, _c.c_double, _c.c_double, _i, _i, _vp,
                              _c.c_int64, _i, _vp]),
     "bz2g_gen_uniform": (_i, [_c.c_uint64, _vp, _c.c_int64, _i, _vp]),
+    "bz2g_compress_file": (_i, [_c.c_char_p, _c.c_char_p, _i, _i]),
     "bz2g_part_bound": (_sz, [_sz, _i]),
     "bz2g_compress_part": (_i, [_vp, _sz, _i, _i, _vp, _sz, _c.POINTER(_c.c_int64),
                                 _c.POINTER(_c.c_uint32), _c.POINTER(_i)]),
@@ -227,6 +228,14 @@ def compress_batch(inputs, levels, block_bytes=None, out=None, on_device=False):
                                      offs))
     buf = memoryview(out.numpy() if hasattr(out, "numpy") else out)
     return [buf[offs[i]:offs[i + 1]] for i in range(count)]
+
+
+def compress_file(in_path, out_path, level: int = 9, group_blocks: int = 0) -> None:
+    """Stream a file (None: stdin) into a .bz2 file (None: stdout) with bounded
+    host memory: pinned input ring, groups of blocks on the GPU, output
+    written as each group finishes (900,000-byte blocks, as the CLI)."""
+    enc = lambda p: None if p is None else str(p).encode()
+    _check(lib().bz2g_compress_file(enc(in_path), enc(out_path), level, group_blocks))
 
 
 def compress_bound(n: int, block_bytes: int = 900000) -> int:

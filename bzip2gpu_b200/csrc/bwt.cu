@@ -88,19 +88,33 @@ __global__ void __launch_bounds__(256) k_radix_scan(SlabDev d) {
   const int nt = (len + kTile - 1) / kTile;
   const int t0 = (int)(d.off[b] / kTile);
   const int dg = threadIdx.x;
+  uint32_t *H = d.tile_hist + (size_t)t0 * kRadix + dg;
+  // eight tiles' counts in flight at a time (the loads are independent)
+  constexpr int kU = 8;
   uint32_t run = 0;
-  for (int k = 0; k < nt; k++) {
-    size_t idx = (size_t)(t0 + k) * kRadix + dg;
-    uint32_t h = d.tile_hist[idx];
-    d.tile_hist[idx] = run;
-    run += h;
+  for (int k0 = 0; k0 < nt; k0 += kU) {
+    uint32_t h[kU];
+#pragma unroll
+    for (int j = 0; j < kU; j++) h[j] = k0 + j < nt ? H[(size_t)(k0 + j) * kRadix] : 0u;
+#pragma unroll
+    for (int j = 0; j < kU; j++) {
+      if (k0 + j < nt) H[(size_t)(k0 + j) * kRadix] = run;
+      run += h[j];
+    }
   }
   uint32_t tot;
   uint32_t base = block_excl_sum(run, scratch, &tot);
   int trivial = __syncthreads_or(run == (uint32_t)len);
   if (!trivial && threadIdx.x == 0) atomicOr(&d.sort_ctl[1], 1);
-  uint32_t add = (uint32_t)d.off[b] + base;
-  for (int k = 0; k < nt; k++) d.tile_hist[(size_t)(t0 + k) * kRadix + dg] += add;
+  const uint32_t add = (uint32_t)d.off[b] + base;
+  for (int k0 = 0; k0 < nt; k0 += kU) {
+    uint32_t h[kU];
+#pragma unroll
+    for (int j = 0; j < kU; j++) h[j] = k0 + j < nt ? H[(size_t)(k0 + j) * kRadix] : 0u;
+#pragma unroll
+    for (int j = 0; j < kU; j++)
+      if (k0 + j < nt) H[(size_t)(k0 + j) * kRadix] = h[j] + add;
+  }
 }
 
 // Stable scatter of one tile by one 8-bit digit.  Elements are warp-striped

@@ -15,6 +15,8 @@
 #include "compressor.h"
 #include "engine.h"
 #include "selector.h"
+#include "stream.h"
+#include "../../include/io.h"
 
 namespace bz2g {
 namespace {
@@ -159,6 +161,18 @@ Compressor &engine_for(int64_t block_bytes) {
   g_engines[EngineKey{dev, g_slab, g_workers, maxb}] = std::move(c);
   return ref;
 }
+
+}  // namespace
+
+Compressor &default_engine(int64_t max_block_bytes) {
+  Compressor &c = engine_for(std::max<int64_t>(max_block_bytes, 1));
+  const_cast<CompressorConfig &>(c.config()).time_stages = g_timing;
+  const_cast<CompressorConfig &>(c.config()).selector = current_selector();
+  const_cast<CompressorConfig &>(c.config()).plain_passes = current_passes();
+  return c;
+}
+
+namespace {
 
 void compress_any(const uint8_t *in, size_t n, int level, int block_bytes, bool on_device,
                   ByteSink &out) {
@@ -904,3 +918,38 @@ int bz2g_assemble(int nparts, const uint8_t *const *d_parts, const int64_t *bits
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------- file streams
+extern "C" int bz2g_compress_file(const char *in_path, const char *out_path, int level,
+                                  int group_blocks) {
+  return guard([&] {
+    const int group = group_blocks > 0 ? group_blocks : kGroupBlocks;
+    std::unique_ptr<BZFileInputStream> in;
+    if (in_path) {
+      FILE *probe = std::fopen(in_path, "rb");
+      BZ_REQUIRE(probe != nullptr, kErrArg, std::string("cannot open input file: ") + in_path);
+      std::fclose(probe);
+      in.reset(new BZFileInputStream(2 * group, 900000, std::string(in_path)));
+    } else {
+      in.reset(new BZFileInputStream(2 * group, 900000));
+    }
+    FILE *out = out_path ? std::fopen(out_path, "wb") : stdout;
+    BZ_REQUIRE(out != nullptr, kErrArg, std::string("cannot open output file: ") + out_path);
+    bool write_failed = false;
+    try {
+      Compressor &c = default_engine(900000);
+      StreamWriter w(c, level, [&](const uint8_t *p, size_t k) {
+        if (!write_failed && std::fwrite(p, 1, k, out) != k) write_failed = true;
+      });
+      compress_input_stream(*in, w, group);
+    } catch (...) {
+      if (out_path) std::fclose(out);
+      throw;
+    }
+    if (std::fflush(out) != 0) write_failed = true;
+    if (out_path && std::fclose(out) != 0) write_failed = true;
+    BZ_REQUIRE(!in->failed(), kErrArg, "reading the input failed");
+    BZ_REQUIRE(!write_failed, kErrArg, "writing the output failed");
+  });
+}
+

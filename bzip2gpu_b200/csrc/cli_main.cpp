@@ -1,26 +1,16 @@
 // bzip2gpu command line tool (reference: src/main.cpp:20-60).  Blocks are
 // 900,000 raw bytes for every level, as in the reference (its input stream
 // always uses 900000-byte buffers); the level only sets the header digit.
+// Input is read ahead into a ring of pinned chunks while earlier groups of
+// blocks compress, and output is written as each group finishes.
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
-#include <fstream>
 #include <iostream>
-#include <vector>
+#include <string>
 
+#include "bz2g.h"
 #include "cli.h"
-#include "compression.h"
-#include "io.h"
-
-static bool write_file(const std::string &name, const std::vector<uint8_t> &data) {
-  std::ofstream f(name, std::ios::out | std::ios::binary);
-  if (!f) {
-    std::cerr << "Failed to open file for writing: " << name << std::endl;
-    return false;
-  }
-  f.write(reinterpret_cast<const char *>(data.data()), (std::streamsize)data.size());
-  return f.good();
-}
 
 int main(int argc, char **argv) {
   CliOptions opt = parse_args(argc, argv);
@@ -28,28 +18,18 @@ int main(int argc, char **argv) {
   auto t0 = std::chrono::steady_clock::now();
   int rc = 0;
   if (opt.input_files.empty()) {
-    BZFileInputStream in(10, 900000);
-    std::vector<uint8_t> out;
-    bzip2_gpu_compress(in, opt.block_size, out);
-    std::cout.write(reinterpret_cast<const char *>(out.data()), (std::streamsize)out.size());
-    if (in.failed()) rc = 1;
+    if (bz2g_compress_file(nullptr, nullptr, opt.block_size, 0) != BZ2G_OK) {
+      std::cerr << "bzip2gpu: " << bz2g_last_error() << std::endl;
+      rc = 1;
+    }
   } else {
     for (const auto &file : opt.input_files) {
-      BZFileInputStream in(10, 900000, file);
-      if (in.failed()) {
+      const std::string out = opt.stdout_output ? std::string() : file + ".bz2";
+      if (bz2g_compress_file(file.c_str(), opt.stdout_output ? nullptr : out.c_str(),
+                             opt.block_size, 0) != BZ2G_OK) {
+        std::cerr << "bzip2gpu: " << file << ": " << bz2g_last_error() << std::endl;
         rc = 1;
-        continue;
       }
-      std::vector<uint8_t> out;
-      bzip2_gpu_compress(in, opt.block_size, out);
-      if (in.failed()) {
-        rc = 1;
-        continue;
-      }
-      if (opt.stdout_output)
-        std::cout.write(reinterpret_cast<const char *>(out.data()), (std::streamsize)out.size());
-      else if (!write_file(file + ".bz2", out))
-        rc = 1;
     }
   }
   std::cout.flush();

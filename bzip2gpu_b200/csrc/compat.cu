@@ -21,6 +21,7 @@
 #include "crc32.h"
 #include "engine.h"
 #include "io.h"
+#include "stream.h"
 
 namespace {
 
@@ -119,34 +120,48 @@ __global__ void count_frequencies(uint16_t *data_in, int data_len, int *freqs) {
   if (idx < data_len) atomicAdd(&freqs[data_in[idx]], 1);
 }
 
+// Streams the input through the GPU in groups of blocks (stream.h): the
+// stream's pinned chunks are reused, at most kGroupBlocks are held at a time,
+// and the output grows as groups finish.
 void bzip2_gpu_compress(BZFileInputStream &in_stream, int n, std::vector<uint8_t> &out) {
-  std::vector<uint8_t *> bufs;
-  std::vector<int> lens;
-  uint8_t *p;
-  int idx;
-  int len;
-  int maxlen = 1;
-  while ((len = in_stream.fetch(p, idx)) >= 0) {
-    if (len == 0) {
-      cudaFreeHost(p);
-      continue;
-    }
-    bufs.push_back(p);
-    lens.push_back(len);
-    maxlen = std::max(maxlen, len);
-  }
   try {
-    bz2g::CompressorConfig cfg;
-    cfg.max_block_bytes = maxlen;
-    bz2g::Compressor c(cfg);
-    std::vector<const uint8_t *> cp(bufs.begin(), bufs.end());
-    c.compress(cp.data(), lens.data(), (int)lens.size(), n, out);
+    bz2g::Compressor &c = bz2g::default_engine(std::max(in_stream.buffer_size(), 1));
+    bz2g::StreamWriter w(c, n, [&](const uint8_t *p, size_t k) { out.insert(out.end(), p, p + k); });
+    bz2g::compress_input_stream(in_stream, w);
   } catch (const std::exception &e) {
     fprintf(stderr, "bzip2_gpu_compress failed: %s\n", e.what());
     exit(EXIT_FAILURE);
   }
-  for (uint8_t *b : bufs) cudaFreeHost(b);
 }
+
+namespace bz2g {
+void compress_input_stream(BZFileInputStream &in, StreamWriter &w, int group_blocks) {
+  std::vector<uint8_t *> bufs;
+  std::vector<const uint8_t *> cbufs;
+  std::vector<int> lens;
+  auto flush = [&] {
+    w.add(cbufs.data(), lens.data(), (int)lens.size(), false);
+    for (uint8_t *b : bufs) in.release(b);
+    bufs.clear();
+    cbufs.clear();
+    lens.clear();
+  };
+  uint8_t *p;
+  int idx, len;
+  while ((len = in.fetch_pooled(p, idx)) >= 0) {
+    if (len == 0) {
+      in.release(p);
+      continue;
+    }
+    bufs.push_back(p);
+    cbufs.push_back(p);
+    lens.push_back(len);
+    if ((int)lens.size() >= group_blocks) flush();
+  }
+  if (!lens.empty()) flush();
+  w.finish();
+}
+}  // namespace bz2g
 
 // --------------------------------------------------------------------- io.h
 
@@ -157,19 +172,24 @@ struct BZFileInputStream::Impl {
   std::mutex mu;
   std::condition_variable cv;
   std::deque<std::pair<uint8_t *, int>> q;
+  std::vector<uint8_t *> free_bufs;  // pinned buffers given back by release()
   bool closed = false, failed = false, stop = false;
   int next_idx = 0;
   std::thread th;
 
   void reader() {
     for (;;) {
+      uint8_t *buf = nullptr;
       {
         std::unique_lock<std::mutex> g(mu);
         cv.wait(g, [&] { return (int)q.size() < n_buffers || stop; });
         if (stop) break;
+        if (!free_bufs.empty()) {
+          buf = free_bufs.back();
+          free_bufs.pop_back();
+        }
       }
-      uint8_t *buf = nullptr;
-      if (cudaMallocHost((void **)&buf, buffer_size) != cudaSuccess) {
+      if (!buf && cudaMallocHost((void **)&buf, buffer_size) != cudaSuccess) {
         std::lock_guard<std::mutex> g(mu);
         failed = true;
         break;
@@ -179,7 +199,7 @@ struct BZFileInputStream::Impl {
       bool bad = in->bad();
       std::lock_guard<std::mutex> g(mu);
       if (got > 0) q.emplace_back(buf, got);
-      else cudaFreeHost(buf);
+      else free_bufs.push_back(buf);
       if (bad) failed = true;
       if (got < buffer_size || bad) break;
       cv.notify_all();
@@ -224,6 +244,7 @@ BZFileInputStream::~BZFileInputStream() {
   }
   if (impl_->th.joinable()) impl_->th.join();
   for (auto &e : impl_->q) cudaFreeHost(e.first);
+  for (uint8_t *b : impl_->free_bufs) cudaFreeHost(b);
   delete impl_;
 }
 
@@ -237,6 +258,17 @@ int BZFileInputStream::fetch(uint8_t *&result, int &chunk_idx) {
   chunk_idx = impl_->next_idx++;
   impl_->cv.notify_all();
   return e.second;
+}
+
+int BZFileInputStream::fetch_pooled(uint8_t *&result, int &chunk_idx) {
+  return fetch(result, chunk_idx);
+}
+
+void BZFileInputStream::release(uint8_t *chunk) {
+  if (!chunk) return;
+  std::lock_guard<std::mutex> g(impl_->mu);
+  impl_->free_bufs.push_back(chunk);
+  impl_->cv.notify_all();
 }
 
 bool BZFileInputStream::failed() const {

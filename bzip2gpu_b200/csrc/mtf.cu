@@ -77,7 +77,7 @@ constexpr int kListStride = 264;      // bytes per lane list (8-aligned, bank sp
 constexpr int kPartStride = kSub + 4;
 
 __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d) {
-  __shared__ int key[256];
+  __shared__ __align__(16) int key[256];
   __shared__ __align__(16) uint8_t sL[kTile];
   __shared__ __align__(16) uint8_t lists[32 * kListStride];
   __shared__ __align__(4) uint8_t part[32 * kPartStride];
@@ -109,12 +109,25 @@ __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d) {
 #pragma unroll
   for (int w = 0; w < 8; w++) pmask[ln][w] = 0;
   __syncwarp();
-  for (int c = ln; c < 256; c += 32) {
-    int kc = key[c];
-    if (kc == INT32_MIN) continue;
-    int r = 0;
-    for (int c2 = 0; c2 < 256; c2++) r += key[c2] > kc;
-    lists[r] = (uint8_t)c;  // list of lane 0
+  {
+    // rank of each of this lane's 8 symbols among all keys (list of lane 0);
+    // the keys are read four at a time and compared against all eight
+    int kc[8], r[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      kc[q] = key[ln + 32 * q];
+      r[q] = 0;
+    }
+    const int4 *k4 = reinterpret_cast<const int4 *>(key);
+    for (int c2 = 0; c2 < 64; c2++) {
+      const int4 v = k4[c2];
+#pragma unroll
+      for (int q = 0; q < 8; q++)
+        r[q] += (v.x > kc[q]) + (v.y > kc[q]) + (v.z > kc[q]) + (v.w > kc[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++)
+      if (kc[q] != INT32_MIN) lists[r[q]] = (uint8_t)(ln + 32 * q);
   }
   // partial lists
   const int a0 = ln * kSub;

@@ -34,7 +34,8 @@ constexpr size_t kOffRtStart = kOffRtBlock + 4 * kNoAllocTiles;
 constexpr size_t kOffTileA = kOffRtStart + 4 * kNoAllocTiles;
 constexpr size_t kOffTileB = kOffTileA + 4 * kNoAllocTiles;
 constexpr size_t kOffTileC = kOffTileB + 4 * kNoAllocTiles;
-constexpr size_t kOffScalars = kOffTileC + 4 * kNoAllocTiles;        // m, crc, crc_acc
+constexpr size_t kOffTileD = kOffTileC + 4 * kNoAllocTiles;          // tile CRCs
+constexpr size_t kOffScalars = kOffTileD + 4 * kNoAllocTiles;        // m, crc, crc_acc
 constexpr size_t kNoAllocBytes = kOffScalars + 256;
 
 static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocBytes];
@@ -118,6 +119,7 @@ extern "C" int bz2g_rle1_noalloc(const uint8_t *d_in, int n, uint8_t *d_out, int
     d.tile_a = reinterpret_cast<int32_t *>(base + kOffTileA);
     d.tile_b = reinterpret_cast<int32_t *>(base + kOffTileB);
     d.tile_c = reinterpret_cast<int32_t *>(base + kOffTileC);
+    d.tile_d = reinterpret_cast<int32_t *>(base + kOffTileD);
     d.m = reinterpret_cast<int32_t *>(base + kOffScalars);
     d.crc = reinterpret_cast<uint32_t *>(base + kOffScalars + 4);
     d.crc_acc = reinterpret_cast<uint32_t *>(base + kOffScalars + 8);

@@ -10,9 +10,12 @@
 // so every output offset is an exclusive scan of a per-position count, and the
 // run start / end of a position are a max-scan / min-scan of run-start flags.
 //
-// CRC: crc0(D) (zero init, no final complement) is linear over GF(2), so each
-// 4096-byte tile's crc0 is shifted by x^(8 * bytes after the tile) mod P and
-// XOR-ed into the block; the init term ~0 * x^(8n) is added at the end.
+// CRC: crc0(D) (zero init, no final complement) is linear over GF(2).  Per
+// 4096-byte tile, thread l takes 16 bytes and multiplies their crc0 by
+// x^(8*16*(255-l)) mod P (a compile-time table), and the XOR of the 256
+// products is the tile's crc0; the per-block kernel shifts each tile's crc0
+// by x^(8 * bytes after the tile) (one thread per tile) and XORs them; the
+// init term ~0 * x^(8n) is added at the end.
 #include "engine.h"
 
 namespace bz2g {
@@ -40,6 +43,21 @@ constexpr uint32_t xpow8_pow2(int i) {
 __constant__ uint32_t c_xpow[32] = {XP4(0),  XP4(4),  XP4(8),  XP4(12),
                                     XP4(16), XP4(20), XP4(24), XP4(28)};
 #undef XP4
+
+// c_klane.v[l] = x^(8 * 16 * (255 - l)) mod P: thread l's 16 bytes sit that
+// far before the end of a 4096-byte tile.
+struct LaneShift {
+  uint32_t v[256];
+  constexpr LaneShift() : v() {
+    uint32_t k = 1u;
+    const uint32_t step = xpow8_pow2(4);  // x^(8*16)
+    for (int l = 255; l >= 0; --l) {
+      v[l] = k;
+      k = gf_mul_c(k, step);
+    }
+  }
+};
+__constant__ LaneShift c_klane{};
 
 __device__ __forceinline__ uint32_t gf_mul(uint32_t a, uint32_t b) {
   uint32_t r = 0;
@@ -86,6 +104,26 @@ __device__ __forceinline__ int load_raw_tile(const SlabDev &d, int t, uint8_t *s
   return len;
 }
 
+// The thread's 16 bytes of the staged tile (positions p0 .. p0 + 15, with
+// p0 = 16 * thread, one 16-byte shared load) and the mask of run starts among
+// them: bit k is set when byte k lies in the tile and differs from the byte
+// before it (`prev` before the tile, -1 at a block start).
+__device__ __forceinline__ uint32_t tile_bytes(const uint8_t *sb, int p0, int len, int prev,
+                                               uint8_t (&c)[kTileItems]) {
+  const uint4 v = *reinterpret_cast<const uint4 *>(sb + p0);
+  const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+  for (int k = 0; k < kTileItems; k++) c[k] = (uint8_t)(w[k >> 2] >> (8 * (k & 3)));
+  int pv = p0 == 0 ? prev : (int)sb[p0 - 1];
+  uint32_t starts = 0;
+#pragma unroll
+  for (int k = 0; k < kTileItems; k++) {
+    if (p0 + k < len && (int)c[k] != pv) starts |= 1u << k;
+    pv = c[k];
+  }
+  return starts;
+}
+
 __global__ void __launch_bounds__(256) k_rle1_scan_tiles(SlabDev d) {
   __shared__ __align__(16) uint8_t sb[kRawTile + 16];
   __shared__ uint32_t tbl[256];
@@ -97,17 +135,11 @@ __global__ void __launch_bounds__(256) k_rle1_scan_tiles(SlabDev d) {
   __syncthreads();
 
   // run starts: first and last in this tile (block-local indices)
-  int first = INT32_MAX, last = -1;
   const int p0 = threadIdx.x * kTileItems;
-  for (int k = 0; k < kTileItems; k++) {
-    int p = p0 + k;
-    if (p >= len) break;
-    int pv = p == 0 ? prev : (int)sb[p - 1];
-    if ((int)sb[p] != pv) {
-      first = min(first, st + p);
-      last = max(last, st + p);
-    }
-  }
+  uint8_t c[kTileItems];
+  const uint32_t sm = tile_bytes(sb, p0, len, prev, c);
+  int first = sm ? st + p0 + __ffs(sm) - 1 : INT32_MAX;
+  int last = sm ? st + p0 + 31 - __clz(sm) : -1;
   // block min / max
   for (int o = 16; o > 0; o >>= 1) {
     first = min(first, __shfl_xor_sync(0xffffffffu, first, o));
@@ -118,39 +150,33 @@ __global__ void __launch_bounds__(256) k_rle1_scan_tiles(SlabDev d) {
     red[1][warp_id()] = last;
   }
 
-  // CRC of the tile, right-aligned into a virtual 4096-byte tile (leading
-  // zeros leave a zero-init CRC unchanged): 16 bytes per lane, a shuffle tree
-  // per warp (512 bytes), then warp 0 joins the eight warp CRCs.
+  // crc0 of the tile, right-aligned into a virtual 4096-byte tile (leading
+  // zeros leave a zero-init CRC unchanged): 16 bytes per thread, each
+  // thread's crc0 moved to the tile's end by one multiplication, then XOR.
   __shared__ uint32_t wcrc[8];
   {
     const int pad = kRawTile - len;
     uint32_t r = 0;
-    const int v0 = warp_id() * 512 + lane_id() * 16;
-    for (int v = max(v0, pad); v < v0 + 16; v++) {
-      uint32_t byte = sb[v - pad];
-      r = (r << 8) ^ tbl[(r >> 24) ^ byte];
-    }
+    const int v0 = threadIdx.x * 16;
+    if (pad == 0) {
 #pragma unroll
-    for (int k = 0; k < 5; k++) {
-      const int dd = 1 << k;
-      const uint32_t o = __shfl_down_sync(0xffffffffu, r, dd);
-      if ((lane_id() & (2 * dd - 1)) == 0) r = gf_mul(r, c_xpow[4 + k]) ^ o;  // x^(8*16*dd)
+      for (int k = 0; k < kTileItems; k++) r = (r << 8) ^ tbl[(r >> 24) ^ c[k]];
+    } else {
+      for (int v = max(v0, pad); v < v0 + 16; v++) {
+        uint32_t byte = sb[v - pad];
+        r = (r << 8) ^ tbl[(r >> 24) ^ byte];
+      }
     }
+    r = r ? gf_mul(r, c_klane.v[threadIdx.x]) : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r ^= __shfl_xor_sync(0xffffffffu, r, o);
     if (lane_id() == 0) wcrc[warp_id()] = r;
   }
   __syncthreads();
-  if (warp_id() == 0) {
-    uint32_t r = lane_id() < 8 ? wcrc[lane_id()] : 0;
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-      const int dd = 1 << k;
-      const uint32_t o = __shfl_down_sync(0xffffffffu, r, dd);
-      if ((lane_id() & (2 * dd - 1)) == 0) r = gf_mul(r, c_xpow[9 + k]) ^ o;  // x^(8*512*dd)
-    }
-    if (lane_id() == 0) {
-      uint64_t after = (uint64_t)(n - (st + len));
-      atomicXor(&d.crc_acc[b], gf_mul(r, xpow8(after)));
-    }
+  if (threadIdx.x == 0) {
+    uint32_t r = 0;
+    for (int w = 0; w < 8; w++) r ^= wcrc[w];
+    d.tile_d[t] = (int32_t)r;  // the tile's crc0 (shifted per block)
   }
   if (threadIdx.x == 0) {
     int f = INT32_MAX, l = -1;
@@ -198,7 +224,22 @@ __global__ void __launch_bounds__(256) k_rle1_block_carry(SlabDev d, const int *
     __syncthreads();
     carry_min = c2;
   }
-  if (threadIdx.x == 0) d.crc[b] = ~(gf_mul(0xFFFFFFFFu, xpow8((uint64_t)n)) ^ d.crc_acc[b]);
+  // block CRC: each tile's crc0 shifted by x^(8 * bytes after it), XOR-ed
+  uint32_t acc = 0;
+  for (int k = threadIdx.x; k < nt; k += blockDim.x) {
+    const int st = d.rt_start[t0 + k];
+    const int len = min(kRawTile, n - st);
+    const uint32_t c = (uint32_t)d.tile_d[t0 + k];
+    if (c) acc ^= gf_mul(c, xpow8((uint64_t)(n - (st + len))));
+  }
+  for (int o = 16; o > 0; o >>= 1) acc ^= __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane_id() == 0) scratch[warp_id()] = (int)acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t a = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) a ^= (uint32_t)scratch[w];
+    d.crc[b] = ~(gf_mul(0xFFFFFFFFu, xpow8((uint64_t)n)) ^ a);
+  }
 }
 
 __device__ __forceinline__ int rle1_count_of(int j) {
@@ -214,13 +255,10 @@ __global__ void __launch_bounds__(256) k_rle1_count(SlabDev d) {
   int len = load_raw_tile(d, t, sb, &b, &st, &n, &prev);
   __syncthreads();
   const int p0 = threadIdx.x * kTileItems;
-  int ls = -1;
-  for (int k = 0; k < kTileItems; k++) {
-    int p = p0 + k;
-    if (p >= len) break;
-    int pv = p == 0 ? prev : (int)sb[p - 1];
-    if ((int)sb[p] != pv) ls = st + p;
-  }
+  uint8_t c[kTileItems];
+  const uint32_t sm = tile_bytes(sb, p0, len, prev, c);
+  const int nv = min(kTileItems, max(0, len - p0));  // bytes of this thread in the tile
+  int ls = sm ? st + p0 + 31 - __clz(sm) : -1;
   int inc = block_incl_max(ls, scratch, -1);
   // exclusive: max over earlier threads, with the tile carry
   int ex = __shfl_up_sync(0xffffffffu, inc, 1);
@@ -230,12 +268,9 @@ __global__ void __launch_bounds__(256) k_rle1_count(SlabDev d) {
   if (lane_id() == 0) ex = warp_id() == 0 ? -1 : wl[warp_id() - 1];
   int cur = max(ex, d.tile_b[t]);
   int cnt = 0;
-  for (int k = 0; k < kTileItems; k++) {
-    int p = p0 + k;
-    if (p >= len) break;
-    int pv = p == 0 ? prev : (int)sb[p - 1];
-    if ((int)sb[p] != pv) cur = st + p;
-    cnt += rle1_count_of(st + p - cur);
+  for (int k = 0; k < nv; k++) {
+    if ((sm >> k) & 1u) cur = st + p0 + k;
+    cnt += rle1_count_of(st + p0 + k - cur);
   }
   int total;
   block_excl_sum(cnt, scratch, &total);
@@ -261,6 +296,7 @@ __global__ void __launch_bounds__(256) k_rle1_block_offsets(SlabDev d, const int
 
 __global__ void __launch_bounds__(256) k_rle1_write(SlabDev d) {
   __shared__ __align__(16) uint8_t sb[kRawTile + 16];
+  __shared__ __align__(16) uint8_t so[kRawTile + kRawTile / 4 + 16];  // the tile's output
   __shared__ int scratch[40];
   __shared__ int wl[8], wf[8];
   const int t = blockIdx.x;
@@ -268,16 +304,11 @@ __global__ void __launch_bounds__(256) k_rle1_write(SlabDev d) {
   int len = load_raw_tile(d, t, sb, &b, &st, &n, &prev);
   __syncthreads();
   const int p0 = threadIdx.x * kTileItems;
-  int ls = -1, fs = INT32_MAX;
-  for (int k = 0; k < kTileItems; k++) {
-    int p = p0 + k;
-    if (p >= len) break;
-    int pv = p == 0 ? prev : (int)sb[p - 1];
-    if ((int)sb[p] != pv) {
-      ls = st + p;
-      fs = min(fs, st + p);
-    }
-  }
+  uint8_t c[kTileItems];
+  const uint32_t sm = tile_bytes(sb, p0, len, prev, c);
+  const int nv = min(kTileItems, max(0, len - p0));
+  int ls = sm ? st + p0 + 31 - __clz(sm) : -1;
+  int fs = sm ? st + p0 + __ffs(sm) - 1 : INT32_MAX;
   // exclusive max of last starts over earlier threads
   int inc = warp_incl_max(ls);
   int exw = __shfl_up_sync(0xffffffffu, inc, 1);
@@ -299,55 +330,48 @@ __global__ void __launch_bounds__(256) k_rle1_write(SlabDev d) {
     int cur = after;
 #pragma unroll
     for (int k = kTileItems - 1; k >= 0; k--) {
-      int p = p0 + k;
       ends[k] = cur;
-      if (p < len) {
-        int pv = p == 0 ? prev : (int)sb[p - 1];
-        if ((int)sb[p] != pv) cur = st + p;
-      }
+      if ((sm >> k) & 1u) cur = st + p0 + k;
     }
   }
   int cnt = 0;
   {
     int cur = before;
-    for (int k = 0; k < kTileItems; k++) {
-      int p = p0 + k;
-      if (p >= len) break;
-      int pv = p == 0 ? prev : (int)sb[p - 1];
-      if ((int)sb[p] != pv) cur = st + p;
-      cnt += rle1_count_of(st + p - cur);
+    for (int k = 0; k < nv; k++) {
+      if ((sm >> k) & 1u) cur = st + p0 + k;
+      cnt += rle1_count_of(st + p0 + k - cur);
     }
   }
   int tot;
   int o = block_excl_sum(cnt, scratch, &tot);
-  uint8_t *out = d.rle1 + d.off[b] + d.tile_c[t] + o;
+  uint8_t *out = so + o;
   int cur = before;
 #pragma unroll
   for (int k = 0; k < kTileItems; k++) {
-    int p = p0 + k;
-    if (p < len) {
-      uint8_t c = sb[p];
-      int pv = p == 0 ? prev : (int)sb[p - 1];
-      if ((int)c != pv) cur = st + p;
-      int j = st + p - cur;
+    if (k < nv) {
+      if ((sm >> k) & 1u) cur = st + p0 + k;
+      int j = st + p0 + k - cur;
       int q = j % 259;
       if (q < 3) {
-        *out++ = c;
+        *out++ = c[k];
       } else if (q == 3) {
         int run_len = ends[k] - cur;
         int chunk_len = min(259, run_len - (j / 259) * 259);
-        *out++ = c;
+        *out++ = c[k];
         *out++ = (uint8_t)(chunk_len - 4);
       }
     }
   }
+  __syncthreads();
+  // coalesced copy of the tile's output to its place in the block
+  uint8_t *dst = d.rle1 + d.off[b] + d.tile_c[t];
+  for (int i = threadIdx.x; i < tot; i += blockDim.x) dst[i] = so[i];
 }
 
 }  // namespace
 
 void stage_rle1_crc(const SlabDev &d, cudaStream_t st) {
   const int *rt_first = d.rt_first;
-  BZ_CUDA(cudaMemsetAsync(d.crc_acc, 0, sizeof(uint32_t) * d.nblocks, st));
   if (d.n_raw_tiles > 0) {
     k_rle1_scan_tiles<<<d.n_raw_tiles, 256, 0, st>>>(d);
     BZ_LAUNCH_CHECK();
@@ -368,7 +392,6 @@ void stage_rle1_crc(const SlabDev &d, cudaStream_t st) {
 
 void launch_crc_only(const SlabDev &d, cudaStream_t st) {
   const int *rt_first = d.rt_first;
-  BZ_CUDA(cudaMemsetAsync(d.crc_acc, 0, sizeof(uint32_t) * d.nblocks, st));
   if (d.n_raw_tiles > 0) {
     k_rle1_scan_tiles<<<d.n_raw_tiles, 256, 0, st>>>(d);
     BZ_LAUNCH_CHECK();

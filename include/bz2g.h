@@ -177,6 +177,18 @@ int bz2g_huffman_encode(const uint16_t *d_syms, int s, const uint8_t *len, const
  *           src/compression/huffman.cu:126-133 */
 int bz2g_count_frequencies(const uint16_t *d_syms, int s, int32_t *d_freqs, void *stream);
 
+/* ------------------------------------------------------------ file streams */
+/* A file (NULL: standard input) compressed to a .bz2 file (NULL: standard
+ * output) with bounded host memory: a reader thread keeps a ring of pinned
+ * 900,000-byte chunks ahead, groups of group_blocks blocks (0: 384) compress
+ * on the GPU while the next group is read, and each group's bytes are written
+ * as it finishes.  Blocks are 900,000 raw bytes and the header digit is the
+ * level, as in the reference's CLI (src/main.cpp:26-45).  A missing input
+ * file is an error (the reference waits forever).
+ * Replaces: main's loop over BZFileInputStream + bzip2_gpu_compress
+ * (src/main.cpp:26-58). */
+int bz2g_compress_file(const char *in_path, const char *out_path, int level, int group_blocks);
+
 /* ------------------------------------------- one stream over several GPUs */
 /* No counterpart in the reference (one GPU).  Blocks are independent, so a
  * stream is cut into parts of whole blocks, each compressed on its own GPU;
