@@ -24,7 +24,7 @@ __all__ = [
     "huffman_encode", "count_frequencies", "gen_markov", "gen_uniform", "MAX_GROUPS",
     "MAX_ALPHA", "SELECTOR_PARAMS", "selector_load", "set_selector", "get_selector",
     "selector_logits", "huffman_build_learned", "selector_dataset", "compress_part",
-    "assemble", "compress_file",
+    "assemble", "compress_file", "decompress", "decompress_device",
 ]
 
 MAX_GROUPS = 6
@@ -65,6 +65,8 @@ _SIGS = {
                              _c.c_int64, _i, _vp]),
     "bz2g_gen_uniform": (_i, [_c.c_uint64, _vp, _c.c_int64, _i, _vp]),
     "bz2g_compress_file": (_i, [_c.c_char_p, _c.c_char_p, _i, _i]),
+    "bz2g_decompress": (_i, [_vp, _sz, _c.POINTER(_u8p), _c.POINTER(_sz)]),
+    "bz2g_decompress_device": (_i, [_vp, _sz, _c.POINTER(_u8p), _c.POINTER(_sz)]),
     "bz2g_part_bound": (_sz, [_sz, _i]),
     "bz2g_compress_part": (_i, [_vp, _sz, _i, _i, _vp, _sz, _c.POINTER(_c.c_int64),
                                 _c.POINTER(_c.c_uint32), _c.POINTER(_i)]),
@@ -228,6 +230,31 @@ def compress_batch(inputs, levels, block_bytes=None, out=None, on_device=False):
                                      offs))
     buf = memoryview(out.numpy() if hasattr(out, "numpy") else out)
     return [buf[offs[i]:offs[i + 1]] for i in range(count)]
+
+
+def decompress(data) -> bytes:
+    """Decode a .bz2 stream (host bytes) on the GPU."""
+    keep, ptr = _host_view(data)
+    out = _u8p()
+    ln = _sz()
+    _check(lib().bz2g_decompress(ptr if keep.size else None, keep.size, ctypes.byref(out),
+                                 ctypes.byref(ln)))
+    try:
+        return ctypes.string_at(out, ln.value)
+    finally:
+        lib().bz2g_free(out)
+
+
+def decompress_device(d_in) -> bytes:
+    """Decode a .bz2 stream held in a CUDA uint8 tensor."""
+    out = _u8p()
+    ln = _sz()
+    _check(lib().bz2g_decompress_device(_ptr(d_in), d_in.numel(), ctypes.byref(out),
+                                        ctypes.byref(ln)))
+    try:
+        return ctypes.string_at(out, ln.value)
+    finally:
+        lib().bz2g_free(out)
 
 
 def compress_file(in_path, out_path, level: int = 9, group_blocks: int = 0) -> None:

@@ -1,0 +1,726 @@
+// GPU decompressor for .bz2 streams (no counterpart in the reference, whose
+// TODO.md:28-34 lists decompression as missing).
+//
+// Blocks are decoded in parallel:
+//   1. k_dec_magic: every bit offset of the stream is tested for the 48-bit
+//      block magic 0x314159265359 and the end-of-stream magic 0x177245385090;
+//      the host then follows the chain (a block starts where the previous one
+//      ended), so a magic that happens to appear inside a payload is ignored.
+//   2. k_dec_block: one warp per candidate block.  All 32 lanes walk the bit
+//      stream in lockstep (the same reads, so shared-memory tables are read as
+//      broadcasts): header (CRC, origPtr, symbol map, tables, selectors),
+//      Huffman symbols via a 10-bit lookup table with the canonical slow path
+//      for longer codes, RUNA/RUNB zero runs, and the inverse move-to-front
+//      with the 256-entry list spread over the lanes (8 bytes each).  Out: the
+//      BWT last column L and, per position, the rank of L[i] among equal
+//      symbols before it.
+//   3. k_dec_lf: LF vector tt[C[L[i]] + rank[i]] = i << 8 | L[i] (parallel).
+//   4. k_dec_walk: per block, the chain from origPtr gives the RLE1 bytes.
+//   5. k_dec_unrle1: per block, RLE1 runs expanded (4 equal bytes then a
+//      count byte), counted first, then written at the block's output offset
+//      with its CRC, checked against the block header.
+// Every field read from the stream is range-checked and every loop is bounded,
+// so a malformed stream gives an error status, not a fault.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/bz2g.h"
+#include "common.cuh"
+#include "compressor.h"
+
+namespace bz2g {
+
+void set_last_error(const std::string &msg);
+
+namespace {
+
+constexpr int kDecMaxGroups = 6;
+constexpr int kDecMaxAlpha = 258;
+constexpr int kDecMaxCode = 20;
+constexpr int kDecMaxSel = 18002;
+constexpr int kLutBits = 10;
+// Per-block capacity of the last column (the reference's 900,000-byte raw
+// blocks can exceed 900,000 RLE1 bytes by up to a quarter).
+constexpr int kDecCap = 1200000;
+
+enum DecStatus {
+  kDecOk = 0,
+  kDecBadHeader = 1,
+  kDecBadTables = 2,
+  kDecBadSymbol = 3,
+  kDecTooLong = 4,
+  kDecBadOrigPtr = 5,
+  kDecBadCrc = 6,
+};
+
+__device__ __forceinline__ uint32_t bswap32(uint32_t x) { return __byte_perm(x, 0, 0x0123); }
+
+// Sequential big-endian bit reader over the stream's words (reads past the end
+// return zeros).
+struct BitReader {
+  const uint32_t *w;
+  int64_t nwords, wpos;
+  uint64_t buf;  // next bits, left-aligned
+  int have;
+  __device__ void init(const uint32_t *words, int64_t nw, int64_t bitpos) {
+    w = words;
+    nwords = nw;
+    wpos = bitpos >> 5;
+    buf = 0;
+    have = 0;
+    refill();
+    const int skip = (int)(bitpos & 31);
+    buf <<= skip;
+    have -= skip;
+    refill();
+  }
+  __device__ __forceinline__ void refill() {
+    while (have <= 32) {
+      const uint32_t v = wpos < nwords ? bswap32(w[wpos]) : 0u;
+      wpos++;
+      buf |= (uint64_t)v << (32 - have);
+      have += 32;
+    }
+  }
+  __device__ __forceinline__ uint32_t peek(int n) { return (uint32_t)(buf >> (64 - n)); }
+  __device__ __forceinline__ void skip(int n) {
+    buf <<= n;
+    have -= n;
+    refill();
+  }
+  __device__ __forceinline__ uint32_t get(int n) {
+    if (n == 0) return 0;
+    const uint32_t v = peek(n);
+    skip(n);
+    return v;
+  }
+  __device__ __forceinline__ int64_t pos() const { return wpos * 32 - have; }
+};
+
+__global__ void k_dec_magic(const uint32_t *words, int64_t nwords, int64_t nbits,
+                            int64_t *blk, int *nblk, int64_t *eos, int *neos, int cap) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nwords) return;
+  const uint64_t a = bswap32(words[i]);
+  const uint64_t b = i + 1 < nwords ? bswap32(words[i + 1]) : 0u;
+  const uint64_t c = i + 2 < nwords ? bswap32(words[i + 2]) : 0u;
+  const uint64_t hi = (a << 32) | b;  // bits 32i .. 32i + 63
+  for (int s = 0; s < 32; s++) {
+    const int64_t p = i * 32 + s;
+    if (p + 48 > nbits) break;
+    const uint64_t v = ((hi << s) | (s ? (c >> (32 - s)) : 0)) >> 16;  // 48 bits at p
+    if (v == 0x314159265359ull) {
+      const int k = atomicAdd(nblk, 1);
+      if (k < cap) blk[k] = p;
+    } else if (v == 0x177245385090ull) {
+      const int k = atomicAdd(neos, 1);
+      if (k < cap) eos[k] = p;
+    }
+  }
+}
+
+// Per-block results of k_dec_block.
+struct DecBlock {
+  int64_t start;    // bit position of the block magic
+  int64_t end;      // bit position after the payload
+  int32_t m;        // last-column length
+  int32_t orig_ptr;
+  uint32_t crc;     // from the header
+  int32_t status;
+};
+
+struct DecShared {
+  uint16_t lut[kDecMaxGroups][1 << kLutBits];  // (len << 9) | symbol; 0 = longer code
+  int32_t limit[kDecMaxGroups][kDecMaxCode + 2];
+  int32_t base[kDecMaxGroups][kDecMaxCode + 2];
+  uint16_t perm[kDecMaxGroups][kDecMaxAlpha];
+  uint8_t minlen[kDecMaxGroups];
+  uint8_t len[kDecMaxGroups][kDecMaxAlpha];
+  int32_t cnt[256];
+  uint8_t seq2unseq[256];
+  int32_t flag;
+};
+
+// One warp per candidate.  sel: per-candidate selector scratch (kDecMaxSel).
+__global__ void __launch_bounds__(32) k_dec_block(const uint32_t *words, int64_t nwords,
+                                                  const int64_t *cand, int ncand,
+                                                  DecBlock *out, uint8_t *Lbuf,
+                                                  int32_t *rank, uint8_t *selbuf, int cap) {
+  __shared__ DecShared sh;
+  const int bi = blockIdx.x;
+  if (bi >= ncand) return;
+  const int ln = threadIdx.x;
+  DecBlock r;
+  r.start = cand[bi];
+  r.end = r.start;
+  r.m = 0;
+  r.orig_ptr = -1;
+  r.crc = 0;
+  r.status = kDecOk;
+  uint8_t *L = Lbuf + (size_t)bi * cap;
+  int32_t *RK = rank + (size_t)bi * cap;
+  uint8_t *sel = selbuf + (size_t)bi * kDecMaxSel;
+  BitReader br;
+  br.init(words, nwords, r.start + 48);
+  r.crc = br.get(32);
+  const uint32_t randomised = br.get(1);
+  r.orig_ptr = (int32_t)br.get(24);
+  // symbol map
+  const uint32_t used16 = br.get(16);
+  int nuse = 0;
+  for (int i = 0; i < 16; i++) {
+    if ((used16 >> (15 - i)) & 1u) {
+      const uint32_t bits = br.get(16);
+      for (int j = 0; j < 16; j++)
+        if ((bits >> (15 - j)) & 1u) {
+          if (ln == 0) sh.seq2unseq[nuse] = (uint8_t)(i * 16 + j);
+          nuse++;
+        }
+    }
+  }
+  const int alpha = nuse + 2;
+  const int ng = (int)br.get(3);
+  const int nsel = (int)br.get(15);
+  if (randomised || nuse == 0 || ng < 2 || ng > 6 || nsel < 1 || nsel > kDecMaxSel) {
+    r.status = kDecBadHeader;
+  }
+  // selectors: unary-coded MTF indices over 0..ng-1
+  if (r.status == kDecOk) {
+    uint32_t lst = 0x543210u;  // nibble k = table at list position k
+    for (int i = 0; i < nsel && r.status == kDecOk; i++) {
+      int j = 0;
+      while (br.get(1)) {
+        if (++j >= ng) {
+          r.status = kDecBadHeader;
+          break;
+        }
+      }
+      if (r.status != kDecOk) break;
+      const uint32_t t = (lst >> (4 * j)) & 0xFu;
+      // move to front: nibbles below j shift up one
+      const uint32_t low = (1u << (4 * j)) - 1u;
+      lst = (lst & ~((low << 4) | 0xFu)) | ((lst & low) << 4) | t;
+      if (ln == 0) sel[i] = (uint8_t)t;
+    }
+  }
+  // code lengths: 5-bit start, then per symbol 1x (x=0: +1, x=1: -1), 0 ends
+  if (r.status == kDecOk) {
+    for (int t = 0; t < ng && r.status == kDecOk; t++) {
+      int cur = (int)br.get(5);
+      for (int v = 0; v < alpha; v++) {
+        int steps = 0;
+        for (;;) {
+          if (cur < 1 || cur > kDecMaxCode || ++steps > 64) {
+            r.status = kDecBadTables;
+            break;
+          }
+          if (!br.get(1)) break;
+          cur += br.get(1) ? -1 : 1;
+        }
+        if (r.status != kDecOk) break;
+        if (ln == 0) sh.len[t][v] = (uint8_t)cur;
+      }
+    }
+  }
+  __syncwarp();
+  // canonical decoding tables: for each length, the symbols of that length in
+  // symbol order get consecutive codes; limit[n] = largest code of length n,
+  // base[n] turns a length-n code into an index into perm.
+  if (r.status == kDecOk) {
+    for (int t = 0; t < ng; t++) {
+      int mn = 32, mx = 0;
+      for (int v = 0; v < alpha; v++) {
+        mn = min(mn, (int)sh.len[t][v]);
+        mx = max(mx, (int)sh.len[t][v]);
+      }
+      if (ln == 0) {
+        sh.minlen[t] = (uint8_t)mn;
+        int pp = 0;
+        for (int l = mn; l <= mx; l++)
+          for (int v = 0; v < alpha; v++)
+            if (sh.len[t][v] == l) sh.perm[t][pp++] = (uint16_t)v;
+        int count[kDecMaxCode + 2];
+        for (int l = 0; l <= kDecMaxCode + 1; l++) count[l] = 0;
+        for (int v = 0; v < alpha; v++) count[sh.len[t][v]]++;
+        int code = 0, idx = 0;
+        for (int l = 0; l <= kDecMaxCode + 1; l++) {
+          sh.limit[t][l] = -1;
+          sh.base[t][l] = 0;
+        }
+        for (int l = mn; l <= mx; l++) {
+          // codes of length l: [code, code + count[l]), perm index idx ..
+          sh.base[t][l] = code - idx;
+          sh.limit[t][l] = code + count[l] - 1;
+          idx += count[l];
+          code = (code + count[l]) << 1;
+        }
+      }
+    }
+  }
+  __syncwarp();
+  if (r.status == kDecOk) {
+    // lookup tables: every 10-bit prefix that starts a code of length <= 10
+    for (int t = 0; t < ng; t++) {
+      for (int p = ln; p < (1 << kLutBits); p += 32) {
+        uint16_t e = 0;
+        for (int l = sh.minlen[t]; l <= kLutBits; l++) {
+          const int code = p >> (kLutBits - l);
+          if (code <= sh.limit[t][l] && sh.limit[t][l] >= 0) {
+            const int idx = code - sh.base[t][l];
+            if (idx >= 0 && idx < alpha) e = (uint16_t)((l << 9) | sh.perm[t][idx]);
+            break;
+          }
+        }
+        sh.lut[t][p] = e;
+      }
+    }
+  }
+  for (int c = ln; c < 256; c += 32) sh.cnt[c] = 0;
+  __syncwarp();
+  // Huffman symbols -> RUNA/RUNB runs and inverse MTF.  The list: lane l
+  // holds positions 8l .. 8l+7, byte k of its word = position 8l + k.
+  uint64_t word = 0;
+  for (int k = 7; k >= 0; k--) {
+    const int p = 8 * ln + k;
+    word = (word << 8) | (uint64_t)(p < nuse ? p : 0);
+  }
+  int m = 0;
+  int64_t zrun = 0;
+  int zbit = 0;
+  const int eob = nuse + 1;
+  int gsel = 0, gleft = 0, tsel = 0;
+  if (r.status == kDecOk) {
+    for (int guard = 0;; guard++) {
+      if (guard > cap + 64) {
+        r.status = kDecTooLong;
+        break;
+      }
+      if (gleft == 0) {
+        if (gsel >= nsel) {
+          r.status = kDecBadSymbol;
+          break;
+        }
+        tsel = sel[gsel++];
+        gleft = 50;
+        __syncwarp();
+      }
+      gleft--;
+      // one symbol with table tsel
+      int sym;
+      const uint32_t e = sh.lut[tsel][br.peek(kLutBits)];
+      if (e) {
+        br.skip((int)(e >> 9));
+        sym = (int)(e & 511u);
+      } else {
+        int n = sh.minlen[tsel];
+        int code = (int)br.get(n);
+        while (n <= kDecMaxCode && code > sh.limit[tsel][n]) {
+          n++;
+          code = (code << 1) | (int)br.get(1);
+        }
+        const int idx = code - sh.base[tsel][n];
+        if (n > kDecMaxCode || idx < 0 || idx >= alpha) {
+          r.status = kDecBadSymbol;
+          break;
+        }
+        sym = sh.perm[tsel][idx];
+      }
+      if (sym <= 1) {  // RUNA / RUNB: bijective base-2 digits, least significant first
+        if (zbit > 40) {
+          r.status = kDecTooLong;
+          break;
+        }
+        zrun += (int64_t)(sym + 1) << zbit;
+        zbit++;
+        continue;
+      }
+      // flush a pending zero run: copies of the list's front symbol
+      if (zrun > 0) {
+        if (zrun > cap - m) {
+          r.status = kDecTooLong;
+          break;
+        }
+        const int front = (int)__shfl_sync(0xffffffffu, (uint32_t)(word & 0xFFu), 0);
+        const uint8_t c = sh.seq2unseq[front];
+        const int base_cnt = sh.cnt[c];
+        for (int64_t o = ln; o < zrun; o += 32) {
+          L[m + o] = c;
+          RK[m + o] = base_cnt + (int)o;
+        }
+        __syncwarp();
+        if (ln == 0) sh.cnt[c] = base_cnt + (int)zrun;
+        __syncwarp();
+        m += (int)zrun;
+        zrun = 0;
+        zbit = 0;
+      }
+      if (sym == eob) break;
+      // value v = sym - 1 >= 1: symbol at list position v moves to the front
+      const int v = sym - 1;
+      if (v >= nuse) {
+        r.status = kDecBadSymbol;
+        break;
+      }
+      if (m >= cap) {
+        r.status = kDecTooLong;
+        break;
+      }
+      const int owner = v >> 3, jb = v & 7;
+      const uint32_t pos = (uint32_t)((__shfl_sync(0xffffffffu, word, owner) >> (8 * jb)) & 0xFFu);
+      const uint64_t top = __shfl_up_sync(0xffffffffu, word >> 56, 1);
+      const uint64_t carry = ln == 0 ? (uint64_t)pos : top;
+      if (ln < owner) {
+        word = (word << 8) | carry;
+      } else if (ln == owner) {
+        const uint64_t lowm = jb == 7 ? ~0ull : ((1ull << (8 * (jb + 1))) - 1);
+        word = (word & ~lowm) | (((word << 8) | carry) & lowm);
+      }
+      const uint8_t c = sh.seq2unseq[pos];
+      if (ln == 0) {
+        L[m] = c;
+        RK[m] = sh.cnt[c]++;
+      }
+      __syncwarp();
+      m++;
+    }
+  }
+  if (r.status == kDecOk && (r.orig_ptr < 0 || r.orig_ptr >= m)) r.status = kDecBadOrigPtr;
+  r.m = m;
+  r.end = br.pos();
+  if (ln == 0) out[bi] = r;
+}
+
+// Cumulative symbol counts of each accepted block: C[b][c] = symbols < c.
+__global__ void k_dec_counts(const int32_t *idx, const DecBlock *db, const uint8_t *Lbuf,
+                             int32_t *C, int cap) {
+  __shared__ int cnt[256];
+  const int k = blockIdx.x;
+  const int bi = idx[k];
+  const int m = db[bi].m;
+  cnt[threadIdx.x] = 0;
+  __syncthreads();
+  const uint8_t *L = Lbuf + (size_t)bi * cap;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) atomicAdd(&cnt[L[i]], 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int c = 0; c < 256; c++) {
+      const int v = cnt[c];
+      cnt[c] = run;
+      run += v;
+    }
+  }
+  __syncthreads();
+  C[(size_t)k * 256 + threadIdx.x] = cnt[threadIdx.x];
+}
+
+// tt[C[L[i]] + rank[i]] = i << 8 | L[i]: for j = LF(i), psi(j) = i and
+// F[j] = L[i]   (grid.y = accepted block)
+__global__ void k_dec_lf(const int32_t *idx, const DecBlock *db, const uint8_t *Lbuf,
+                         const int32_t *rank, const int32_t *C, uint32_t *tt, int cap) {
+  const int k = blockIdx.y;
+  const int bi = idx[k];
+  const int m = db[bi].m;
+  const uint8_t *L = Lbuf + (size_t)bi * cap;
+  const int32_t *RK = rank + (size_t)bi * cap;
+  uint32_t *T = tt + (size_t)k * cap;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    const int c = L[i];
+    const int j = C[(size_t)k * 256 + c] + RK[i];
+    if (j >= 0 && j < m) T[j] = ((uint32_t)i << 8) | (uint32_t)c;
+  }
+}
+
+// The RLE1 bytes of each block: follow tt from origPtr (one thread per block).
+__global__ void k_dec_walk(const int32_t *idx, const DecBlock *db, const uint32_t *tt,
+                           uint8_t *rle, int nacc, int cap) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nacc) return;
+  const DecBlock b = db[idx[k]];
+  const uint32_t *T = tt + (size_t)k * cap;
+  uint8_t *R = rle + (size_t)k * cap;
+  // T[j] = psi(j) << 8 | F[j], psi = LF^-1: the text is F[origPtr],
+  // F[psi(origPtr)], ...
+  uint32_t p = (uint32_t)b.orig_ptr;
+  for (int i = 0; i < b.m; i++) {
+    if (p >= (uint32_t)b.m) break;
+    const uint32_t e = T[p];
+    R[i] = (uint8_t)(e & 0xFFu);
+    p = e >> 8;
+  }
+}
+
+// RLE1 inverse of one block: 4 equal bytes are followed by a count of further
+// copies.  write == 0: count the output bytes; write != 0: write them at
+// out + off[k] and compute the block CRC.
+__device__ __forceinline__ uint32_t crc_byte(uint32_t crc, uint32_t byte, const uint32_t *tbl) {
+  return (crc << 8) ^ tbl[(crc >> 24) ^ byte];
+}
+
+__global__ void k_dec_unrle1(const int32_t *idx, const DecBlock *db, const uint8_t *rle,
+                             int nacc, int cap, int write, int64_t *lens, const int64_t *off,
+                             uint8_t *out, uint32_t *crcs) {
+  __shared__ uint32_t tbl[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+    uint32_t c = (uint32_t)i << 24;
+    for (int q = 0; q < 8; q++) c = (c & 0x80000000u) ? (c << 1) ^ 0x04C11DB7u : (c << 1);
+    tbl[i] = c;
+  }
+  __syncthreads();
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nacc) return;
+  const DecBlock b = db[idx[k]];
+  const uint8_t *R = rle + (size_t)k * cap;
+  uint8_t *O = write ? out + off[k] : nullptr;
+  int64_t n = 0;
+  uint32_t crc = 0xFFFFFFFFu;
+  int prev = -1, run = 0;
+  for (int i = 0; i < b.m; i++) {
+    const int c = R[i];
+    if (run == 4) {
+      for (int q = 0; q < c; q++) {
+        if (write) {
+          O[n] = (uint8_t)prev;
+          crc = crc_byte(crc, (uint32_t)prev, tbl);
+        }
+        n++;
+      }
+      run = 0;
+      prev = -1;
+      continue;
+    }
+    if (c == prev) run++;
+    else {
+      prev = c;
+      run = 1;
+    }
+    if (write) {
+      O[n] = (uint8_t)c;
+      crc = crc_byte(crc, (uint32_t)c, tbl);
+    }
+    n++;
+  }
+  if (write) crcs[k] = ~crc;
+  else lens[k] = n;
+}
+
+cudaStream_t S(void *p) { return reinterpret_cast<cudaStream_t>(p); }
+
+struct DevBuf {
+  void *p = nullptr;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  template <typename T>
+  T *get() const {
+    return static_cast<T *>(p);
+  }
+  void alloc(size_t bytes) {
+    BZ_CUDA(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+  }
+};
+
+// The decoder proper: stream (device) -> output (host vector).
+void decode_stream(const uint8_t *d_in, size_t n, std::vector<uint8_t> &out, cudaStream_t st) {
+  out.clear();
+  BZ_REQUIRE(n >= 14, kErrArg, "not a bzip2 stream (shorter than 14 bytes)");
+  std::vector<uint8_t> head(4);
+  BZ_CUDA(cudaMemcpy(head.data(), d_in, 4, cudaMemcpyDeviceToHost));
+  BZ_REQUIRE(head[0] == 'B' && head[1] == 'Z' && head[2] == 'h' && head[3] >= '1' &&
+                 head[3] <= '9',
+             kErrArg, "not a bzip2 stream (bad header)");
+  // words, padded
+  const int64_t nwords = (int64_t)(n + 3) / 4 + 2;
+  DevBuf words;
+  words.alloc(nwords * 4);
+  BZ_CUDA(cudaMemsetAsync(words.p, 0, nwords * 4, st));
+  BZ_CUDA(cudaMemcpyAsync(words.p, d_in, n, cudaMemcpyDeviceToDevice, st));
+  const int64_t nbits = (int64_t)n * 8;
+  // candidates
+  const int ccap = (int)std::min<int64_t>((int64_t)n / 8 + 64, 1 << 26);
+  DevBuf dblk, deos, dcnt;
+  dblk.alloc(8 * (size_t)ccap);
+  deos.alloc(8 * (size_t)ccap);
+  dcnt.alloc(8);
+  BZ_CUDA(cudaMemsetAsync(dcnt.p, 0, 8, st));
+  k_dec_magic<<<(unsigned)((nwords + 255) / 256), 256, 0, st>>>(
+      words.get<uint32_t>(), nwords, nbits, dblk.get<int64_t>(), dcnt.get<int>(),
+      deos.get<int64_t>(), dcnt.get<int>() + 1, ccap);
+  BZ_LAUNCH_CHECK();
+  int hcnt[2];
+  BZ_CUDA(cudaMemcpyAsync(hcnt, dcnt.p, 8, cudaMemcpyDeviceToHost, st));
+  BZ_CUDA(cudaStreamSynchronize(st));
+  BZ_REQUIRE(hcnt[0] <= ccap && hcnt[1] <= ccap, kErrTooLarge, "too many block candidates");
+  std::vector<int64_t> cands(hcnt[0]), eoss(hcnt[1]);
+  if (hcnt[0]) BZ_CUDA(cudaMemcpy(cands.data(), dblk.p, 8 * hcnt[0], cudaMemcpyDeviceToHost));
+  if (hcnt[1]) BZ_CUDA(cudaMemcpy(eoss.data(), deos.p, 8 * hcnt[1], cudaMemcpyDeviceToHost));
+  std::sort(cands.begin(), cands.end());
+  std::sort(eoss.begin(), eoss.end());
+  // decode candidates in batches; follow the chain of blocks and streams
+  const int batch = 256;
+  const int cap = kDecCap;
+  DevBuf dcand, ddb, dL, drank, dsel, didx, dC, dtt, drle, dlens, doff, dcrc;
+  dcand.alloc(8 * (size_t)batch);
+  ddb.alloc(sizeof(DecBlock) * (size_t)batch);
+  dL.alloc((size_t)batch * cap);
+  drank.alloc((size_t)batch * cap * 4);
+  dsel.alloc((size_t)batch * kDecMaxSel);
+  didx.alloc(4 * (size_t)batch);
+  dC.alloc((size_t)batch * 256 * 4);
+  dtt.alloc((size_t)batch * cap * 4);
+  drle.alloc((size_t)batch * cap);
+  dlens.alloc(8 * (size_t)batch);
+  doff.alloc(8 * (size_t)batch);
+  dcrc.alloc(4 * (size_t)batch);
+  int64_t expect = 32;  // next block or end-of-stream marker
+  uint32_t stream_crc = 0;
+  bool stream_done = false;
+  size_t ci = 0;
+  std::vector<DecBlock> hdb(batch);
+  for (;;) {
+    if (stream_done) {
+      // another stream may follow, from the next byte boundary
+      const int64_t nb = (expect + 7) / 8;
+      if (nb + 14 > (int64_t)n) break;
+      uint8_t h[4];
+      BZ_CUDA(cudaMemcpy(h, d_in + nb, 4, cudaMemcpyDeviceToHost));
+      if (!(h[0] == 'B' && h[1] == 'Z' && h[2] == 'h' && h[3] >= '1' && h[3] <= '9')) break;
+      expect = nb * 8 + 32;
+      stream_crc = 0;
+      stream_done = false;
+    }
+    // the end-of-stream marker at `expect`?
+    if (std::binary_search(eoss.begin(), eoss.end(), expect)) {
+      // combined CRC after the 48-bit marker
+      const int64_t p = expect + 48;
+      uint8_t tail[8] = {0};
+      const int64_t b0 = p / 8;
+      const size_t nb = (size_t)std::min<int64_t>(8, (int64_t)n - b0);
+      BZ_CUDA(cudaMemcpy(tail, d_in + b0, nb, cudaMemcpyDeviceToHost));
+      uint64_t win = 0;
+      for (int q = 0; q < 8; q++) win = (win << 8) | tail[q];
+      const uint32_t got = (uint32_t)((win << (p % 8)) >> 32);
+      BZ_REQUIRE(got == stream_crc, kErrArg, "bzip2 stream CRC mismatch");
+      expect = p + 32;
+      stream_done = true;
+      continue;
+    }
+    // next candidates from `expect` on
+    while (ci < cands.size() && cands[ci] < expect) ci++;
+    BZ_REQUIRE(ci < cands.size() && cands[ci] == expect, kErrArg,
+               "bzip2 stream: no block or end-of-stream marker where one must start");
+    const int nc = (int)std::min<size_t>(batch, cands.size() - ci);
+    BZ_CUDA(cudaMemcpyAsync(dcand.p, cands.data() + ci, 8 * nc, cudaMemcpyHostToDevice, st));
+    k_dec_block<<<nc, 32, 0, st>>>(words.get<uint32_t>(), nwords, dcand.get<int64_t>(), nc,
+                                   ddb.get<DecBlock>(), dL.get<uint8_t>(), drank.get<int32_t>(),
+                                   dsel.get<uint8_t>(), cap);
+    BZ_LAUNCH_CHECK();
+    BZ_CUDA(cudaMemcpyAsync(hdb.data(), ddb.p, sizeof(DecBlock) * nc, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaStreamSynchronize(st));
+    // accept the chain within this batch
+    std::vector<int32_t> acc;
+    size_t used = 0;
+    for (int q = 0; q < nc; q++) {
+      if (hdb[q].start != expect) continue;
+      BZ_REQUIRE(hdb[q].status == kDecOk, kErrArg,
+                 "bzip2 stream: corrupt block (status " + std::to_string(hdb[q].status) + ")");
+      acc.push_back(q);
+      expect = hdb[q].end;
+      used = q + 1;
+      if (std::binary_search(eoss.begin(), eoss.end(), expect)) break;
+    }
+    ci += std::max<size_t>(used, 1);
+    const int na = (int)acc.size();
+    if (na == 0) continue;
+    BZ_CUDA(cudaMemcpyAsync(didx.p, acc.data(), 4 * na, cudaMemcpyHostToDevice, st));
+    k_dec_counts<<<na, 256, 0, st>>>(didx.get<int32_t>(), ddb.get<DecBlock>(), dL.get<uint8_t>(),
+                                     dC.get<int32_t>(), cap);
+    BZ_LAUNCH_CHECK();
+    k_dec_lf<<<dim3(64, na), 256, 0, st>>>(didx.get<int32_t>(), ddb.get<DecBlock>(),
+                                           dL.get<uint8_t>(), drank.get<int32_t>(),
+                                           dC.get<int32_t>(), dtt.get<uint32_t>(), cap);
+    BZ_LAUNCH_CHECK();
+    k_dec_walk<<<(na + 31) / 32, 32, 0, st>>>(didx.get<int32_t>(), ddb.get<DecBlock>(),
+                                              dtt.get<uint32_t>(), drle.get<uint8_t>(), na, cap);
+    BZ_LAUNCH_CHECK();
+    k_dec_unrle1<<<(na + 31) / 32, 32, 0, st>>>(didx.get<int32_t>(), ddb.get<DecBlock>(),
+                                                drle.get<uint8_t>(), na, cap, 0,
+                                                dlens.get<int64_t>(), nullptr, nullptr, nullptr);
+    BZ_LAUNCH_CHECK();
+    std::vector<int64_t> lens(na), offs(na);
+    BZ_CUDA(cudaMemcpyAsync(lens.data(), dlens.p, 8 * na, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaStreamSynchronize(st));
+    int64_t tot = 0;
+    for (int q = 0; q < na; q++) {
+      offs[q] = tot;
+      tot += lens[q];
+    }
+    DevBuf dout;
+    dout.alloc((size_t)tot + 16);
+    BZ_CUDA(cudaMemcpyAsync(doff.p, offs.data(), 8 * na, cudaMemcpyHostToDevice, st));
+    k_dec_unrle1<<<(na + 31) / 32, 32, 0, st>>>(didx.get<int32_t>(), ddb.get<DecBlock>(),
+                                                drle.get<uint8_t>(), na, cap, 1, nullptr,
+                                                doff.get<int64_t>(), dout.get<uint8_t>(),
+                                                dcrc.get<uint32_t>());
+    BZ_LAUNCH_CHECK();
+    std::vector<uint32_t> crcs(na);
+    const size_t base = out.size();
+    out.resize(base + (size_t)tot);
+    BZ_CUDA(cudaMemcpyAsync(out.data() + base, dout.p, (size_t)tot, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaMemcpyAsync(crcs.data(), dcrc.p, 4 * na, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaStreamSynchronize(st));
+    for (int q = 0; q < na; q++) {
+      BZ_REQUIRE(crcs[q] == hdb[acc[q]].crc, kErrArg, "bzip2 stream: block CRC mismatch");
+      stream_crc = ((stream_crc << 1) | (stream_crc >> 31)) ^ crcs[q];
+    }
+  }
+  BZ_REQUIRE(stream_done, kErrArg, "bzip2 stream: no end-of-stream marker");
+}
+
+}  // namespace
+}  // namespace bz2g
+
+using namespace bz2g;
+
+extern "C" int bz2g_decompress_device(const uint8_t *d_in, size_t n, uint8_t **out,
+                                      size_t *out_len) {
+  try {
+    BZ_REQUIRE(out && out_len && (n == 0 || d_in), kErrArg, "bad arguments");
+    std::vector<uint8_t> v;
+    decode_stream(d_in, n, v, 0);
+    uint8_t *p = (uint8_t *)std::malloc(std::max<size_t>(v.size(), 1));
+    BZ_REQUIRE(p != nullptr, kErrAlloc, "host allocation failed");
+    if (!v.empty()) std::memcpy(p, v.data(), v.size());
+    *out = p;
+    *out_len = v.size();
+    set_last_error("");
+    return BZ2G_OK;
+  } catch (const Error &e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return BZ2G_ERR_INTERNAL;
+  }
+}
+
+extern "C" int bz2g_decompress(const uint8_t *in, size_t n, uint8_t **out, size_t *out_len) {
+  try {
+    BZ_REQUIRE(out && out_len && (n == 0 || in), kErrArg, "bad arguments");
+    uint8_t *d = nullptr;
+    BZ_CUDA(cudaMalloc((void **)&d, std::max<size_t>(n, 1)));
+    struct F {
+      uint8_t *p;
+      ~F() { cudaFree(p); }
+    } f{d};
+    if (n) BZ_CUDA(cudaMemcpy(d, in, n, cudaMemcpyHostToDevice));
+    return bz2g_decompress_device(d, n, out, out_len);
+  } catch (const Error &e) {
+    set_last_error(e.what());
+    return e.code;
+  }
+}

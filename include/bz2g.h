@@ -177,6 +177,16 @@ int bz2g_huffman_encode(const uint16_t *d_syms, int s, const uint8_t *len, const
  *           src/compression/huffman.cu:126-133 */
 int bz2g_count_frequencies(const uint16_t *d_syms, int s, int32_t *d_freqs, void *stream);
 
+/* ----------------------------------------------------------- decompression */
+/* No counterpart in the reference (its TODO.md:28-34 lists it as missing).
+ * Decodes a .bz2 stream (or concatenated streams) on the GPU, blocks in
+ * parallel; every block CRC and the stream CRC are checked.  Accepts the
+ * reference's streams whose blocks exceed the header digit's size.  *out is
+ * malloc'ed (release with bz2g_free).  A malformed stream gives an error
+ * status. */
+int bz2g_decompress(const uint8_t *in, size_t n, uint8_t **out, size_t *out_len);
+int bz2g_decompress_device(const uint8_t *d_in, size_t n, uint8_t **out, size_t *out_len);
+
 /* ------------------------------------------------------------ file streams */
 /* A file (NULL: standard input) compressed to a .bz2 file (NULL: standard
  * output) with bounded host memory: a reader thread keeps a ring of pinned
