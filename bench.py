@@ -331,6 +331,7 @@ def main():
     value = n * world * args.steps / dt / 1e6
 
     e2e = None
+    decode = None
     if not args.no_e2e:
         h_in = torch.empty(n, dtype=torch.uint8, pin_memory=True)
         h_in.copy_(d_in)
@@ -339,6 +340,17 @@ def main():
         B.compress_into(h_in, h_out, 9)  # warm the host path
         dte, oute = timed(lambda: B.compress_into(h_in, h_out, 9))
         assert bytes(h_out[:64].numpy()) == out[:64]
+        # the GPU decoder on the same stream (host bytes in, host bytes out;
+        # every block CRC and the stream CRC are checked by the decoder)
+        B.decompress(out)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dec = B.decompress(out)
+        ddt = max_over_ranks(time.perf_counter() - t0, world)
+        assert len(dec) == n and dec[:1 << 20] == h_in[:1 << 20].numpy().tobytes()
+        decode = {"MB/s": round(n * world / ddt / 1e6, 2), "unit": "MB/s of output",
+                  "api": "bz2g_decompress (host stream in, host bytes out)"}
+        del dec
         dte = max_over_ranks(dte, world)
         e2e = {"value": round(n * world * args.steps / dte / 1e6, 2), "unit": "MB/s",
                "h2d_bytes_per_step": n, "d2h_bytes_per_step": int(oute),
@@ -393,6 +405,7 @@ def main():
             "e2e": e2e, "roofline": roof, "pipeline_roofline": pipeline, "cpu_baseline": cpu,
             "forms": {"plain": round(value, 2), "batched": round(batched_value, 2),
                       "learned": learned},
+            "decode": decode,
             "clocks": clk.summary(), "gpu_launches": int(launches),
             "stats": {k: stats[k] for k in ("n", "m", "A", "s", "g", "bits")},
             "stage_ms_sum_over_slabs_last_step": stage_ms,

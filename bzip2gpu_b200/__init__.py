@@ -132,6 +132,17 @@ def _ptr(t) -> int:
     return t.data_ptr()
 
 
+def _take(ptr, n: int) -> bytes:
+    """Bytes of a library-allocated buffer (any size), then free it."""
+    try:
+        if n == 0:
+            return b""
+        addr = ctypes.cast(ptr, ctypes.c_void_p).value
+        return np.ctypeslib.as_array((ctypes.c_uint8 * n).from_address(addr)).tobytes()
+    finally:
+        lib().bz2g_free(ptr)
+
+
 # ------------------------------------------------------------ whole stream
 def _host_view(data) -> tuple[np.ndarray, int]:
     a = np.frombuffer(data, dtype=np.uint8) if isinstance(data, (bytes, bytearray, memoryview)) \
@@ -150,10 +161,7 @@ def compress(data, level: int = 9, block_bytes: int = 900000) -> bytes:
     ln = _sz()
     _check(lib().bz2g_compress(ptr if n else None, n, level, block_bytes, ctypes.byref(out),
                                ctypes.byref(ln)))
-    try:
-        return ctypes.string_at(out, ln.value)
-    finally:
-        lib().bz2g_free(out)
+    return _take(out, ln.value)
 
 
 def compress_into(data, out, level: int = 9, block_bytes: int = 900000) -> int:
@@ -195,10 +203,7 @@ def compress_device(d_in, level: int = 9, block_bytes: int = 900000) -> bytes:
     n = d_in.numel()
     _check(lib().bz2g_compress_device(_ptr(d_in) if n else None, n, level, block_bytes,
                                       ctypes.byref(out), ctypes.byref(ln)))
-    try:
-        return ctypes.string_at(out, ln.value)
-    finally:
-        lib().bz2g_free(out)
+    return _take(out, ln.value)
 
 
 def compress_batch(inputs, levels, block_bytes=None, out=None, on_device=False):
@@ -239,10 +244,7 @@ def decompress(data) -> bytes:
     ln = _sz()
     _check(lib().bz2g_decompress(ptr if keep.size else None, keep.size, ctypes.byref(out),
                                  ctypes.byref(ln)))
-    try:
-        return ctypes.string_at(out, ln.value)
-    finally:
-        lib().bz2g_free(out)
+    return _take(out, ln.value)
 
 
 def decompress_device(d_in) -> bytes:
@@ -251,10 +253,7 @@ def decompress_device(d_in) -> bytes:
     ln = _sz()
     _check(lib().bz2g_decompress_device(_ptr(d_in), d_in.numel(), ctypes.byref(out),
                                         ctypes.byref(ln)))
-    try:
-        return ctypes.string_at(out, ln.value)
-    finally:
-        lib().bz2g_free(out)
+    return _take(out, ln.value)
 
 
 def compress_file(in_path, out_path, level: int = 9, group_blocks: int = 0) -> None:

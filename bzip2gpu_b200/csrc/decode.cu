@@ -435,23 +435,123 @@ __global__ void k_dec_lf(const int32_t *idx, const DecBlock *db, const uint8_t *
   }
 }
 
-// The RLE1 bytes of each block: follow tt from origPtr (one thread per block).
+// The RLE1 bytes of each block follow tt from origPtr:
+// T[j] = psi(j) << 8 | F[j], psi = LF^-1, and the text is F[origPtr],
+// F[psi(origPtr)], ...  One dependent load per byte, so the chain is cut at
+// S splitters per block (origPtr and evenly spaced positions, marked in a
+// bitmap): every walker counts the steps to the next marked position, one
+// thread per block orders the segments along the chain from origPtr, and the
+// walkers walk again writing their segment at its offset.  A periodic block
+// (its cycle closes before m bytes) repeats that one cycle.
+constexpr int kMaxWalkers = 256;
+
+struct WalkCtl {
+  int32_t nw;        // splitters
+  int32_t cycle;     // bytes of the chain from origPtr before it closes (m if it does not)
+  int32_t pos[kMaxWalkers];   // sorted splitter positions
+  int32_t len[kMaxWalkers];   // segment length (steps to the next splitter)
+  int32_t next[kMaxWalkers];  // index of the splitter reached
+  int32_t off[kMaxWalkers];   // output offset, -1 when off the chain
+};
+
+__global__ void k_dec_split(const int32_t *idx, const DecBlock *db, WalkCtl *ctl, uint32_t *mark,
+                            int cap) {
+  const int k = blockIdx.x;
+  const DecBlock b = db[idx[k]];
+  WalkCtl &c = ctl[k];
+  uint32_t *M = mark + (size_t)k * ((cap + 31) / 32);
+  const int m = b.m;
+  for (int i = threadIdx.x; i < (m + 31) / 32; i += blockDim.x) M[i] = 0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int S = max(1, min(kMaxWalkers, m / 4096));
+    int n = 0;
+    bool placed = false;
+    for (int t = 1; t <= S; t++) {
+      const int j = t < S ? (int)((int64_t)t * m / S) : m;  // t == S: sentinel
+      if (!placed && b.orig_ptr <= j) {
+        c.pos[n++] = b.orig_ptr;
+        placed = true;
+      }
+      if (t < S && j != b.orig_ptr && j < m) c.pos[n++] = j;
+    }
+    if (!placed) c.pos[n++] = b.orig_ptr;
+    c.nw = n;
+    for (int q = 0; q < n; q++) atomicOr(&M[c.pos[q] >> 5], 1u << (c.pos[q] & 31));
+  }
+}
+
+__device__ __forceinline__ int splitter_index(const WalkCtl &c, int p) {
+  int lo = 0, hi = c.nw - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (c.pos[mid] < p) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// write == 0: segment lengths and successors; write != 0: the segment bytes.
 __global__ void k_dec_walk(const int32_t *idx, const DecBlock *db, const uint32_t *tt,
-                           uint8_t *rle, int nacc, int cap) {
+                           WalkCtl *ctl, const uint32_t *mark, uint8_t *rle, int cap, int write) {
+  const int k = blockIdx.y;
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  WalkCtl &c = ctl[k];
+  if (w >= c.nw) return;
+  const int m = db[idx[k]].m;
+  const uint32_t *T = tt + (size_t)k * cap;
+  const uint32_t *M = mark + (size_t)k * ((cap + 31) / 32);
+  uint8_t *R = rle + (size_t)k * cap;
+  if (write && c.off[w] < 0) return;
+  uint32_t p = (uint32_t)c.pos[w];
+  int n = 0;
+  const int o = write ? c.off[w] : 0;
+  const int lim = write ? c.len[w] : m;
+  for (;;) {
+    if (p >= (uint32_t)m || n >= lim || o + n >= m) break;
+    const uint32_t e = T[p];
+    if (write) R[o + n] = (uint8_t)(e & 0xFFu);
+    n++;
+    p = e >> 8;
+    if (p < (uint32_t)m && ((M[p >> 5] >> (p & 31)) & 1u)) break;
+  }
+  if (!write) {
+    c.len[w] = n;
+    c.next[w] = (p < (uint32_t)m) ? splitter_index(c, (int)p) : -1;
+  }
+}
+
+// Per block: segment offsets along the chain from origPtr.
+__global__ void k_dec_chain(const int32_t *idx, const DecBlock *db, WalkCtl *ctl, int nacc,
+                            int *bad) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nacc) return;
   const DecBlock b = db[idx[k]];
-  const uint32_t *T = tt + (size_t)k * cap;
-  uint8_t *R = rle + (size_t)k * cap;
-  // T[j] = psi(j) << 8 | F[j], psi = LF^-1: the text is F[origPtr],
-  // F[psi(origPtr)], ...
-  uint32_t p = (uint32_t)b.orig_ptr;
-  for (int i = 0; i < b.m; i++) {
-    if (p >= (uint32_t)b.m) break;
-    const uint32_t e = T[p];
-    R[i] = (uint8_t)(e & 0xFFu);
-    p = e >> 8;
+  WalkCtl &c = ctl[k];
+  for (int q = 0; q < c.nw; q++) c.off[q] = -1;
+  const int w0 = splitter_index(c, b.orig_ptr);
+  int w = w0, off = 0;
+  for (int steps = 0; steps <= c.nw; steps++) {
+    if (w < 0 || w >= c.nw || c.off[w] >= 0) break;
+    c.off[w] = off;
+    off += c.len[w];
+    if (off >= b.m) break;
+    w = c.next[w];
   }
+  c.cycle = min(off, b.m);
+  if (c.cycle <= 0 || b.m % c.cycle != 0) atomicOr(bad, 1);
+}
+
+// A periodic block: the first `cycle` bytes repeated to m.
+__global__ void k_dec_repeat(const int32_t *idx, const DecBlock *db, const WalkCtl *ctl,
+                             uint8_t *rle, int cap) {
+  const int k = blockIdx.y;
+  const int m = db[idx[k]].m;
+  const int cyc = ctl[k].cycle;
+  if (cyc <= 0 || cyc >= m) return;
+  uint8_t *R = rle + (size_t)k * cap;
+  for (int i = cyc + blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+    R[i] = R[i % cyc];
 }
 
 // RLE1 inverse of one block: 4 equal bytes are followed by a count of further
@@ -560,8 +660,9 @@ void decode_stream(const uint8_t *d_in, size_t n, std::vector<uint8_t> &out, cud
   if (hcnt[1]) BZ_CUDA(cudaMemcpy(eoss.data(), deos.p, 8 * hcnt[1], cudaMemcpyDeviceToHost));
   std::sort(cands.begin(), cands.end());
   std::sort(eoss.begin(), eoss.end());
-  // decode candidates in batches; follow the chain of blocks and streams
-  const int batch = 256;
+  // decode candidates in batches (about 12 bytes of scratch per last-column
+  // entry); follow the chain of blocks and streams
+  const int batch = (int)std::min<size_t>(2048, std::max<size_t>(cands.size(), 1));
   const int cap = kDecCap;
   DevBuf dcand, ddb, dL, drank, dsel, didx, dC, dtt, drle, dlens, doff, dcrc;
   dcand.alloc(8 * (size_t)batch);
@@ -576,6 +677,10 @@ void decode_stream(const uint8_t *d_in, size_t n, std::vector<uint8_t> &out, cud
   dlens.alloc(8 * (size_t)batch);
   doff.alloc(8 * (size_t)batch);
   dcrc.alloc(4 * (size_t)batch);
+  DevBuf dctl, dmark, dbad;
+  dctl.alloc(sizeof(WalkCtl) * (size_t)batch);
+  dmark.alloc((size_t)batch * ((cap + 31) / 32) * 4);
+  dbad.alloc(16);
   int64_t expect = 32;  // next block or end-of-stream marker
   uint32_t stream_crc = 0;
   bool stream_done = false;
@@ -644,16 +749,35 @@ void decode_stream(const uint8_t *d_in, size_t n, std::vector<uint8_t> &out, cud
                                            dL.get<uint8_t>(), drank.get<int32_t>(),
                                            dC.get<int32_t>(), dtt.get<uint32_t>(), cap);
     BZ_LAUNCH_CHECK();
-    k_dec_walk<<<(na + 31) / 32, 32, 0, st>>>(didx.get<int32_t>(), ddb.get<DecBlock>(),
-                                              dtt.get<uint32_t>(), drle.get<uint8_t>(), na, cap);
+    k_dec_split<<<na, 256, 0, st>>>(didx.get<int32_t>(), ddb.get<DecBlock>(),
+                                    dctl.get<WalkCtl>(), dmark.get<uint32_t>(), cap);
+    BZ_LAUNCH_CHECK();
+    const dim3 wgrid(kMaxWalkers / 64, na);
+    k_dec_walk<<<wgrid, 64, 0, st>>>(didx.get<int32_t>(), ddb.get<DecBlock>(),
+                                     dtt.get<uint32_t>(), dctl.get<WalkCtl>(),
+                                     dmark.get<uint32_t>(), drle.get<uint8_t>(), cap, 0);
+    BZ_LAUNCH_CHECK();
+    BZ_CUDA(cudaMemsetAsync(dbad.p, 0, 4, st));
+    k_dec_chain<<<(na + 63) / 64, 64, 0, st>>>(didx.get<int32_t>(), ddb.get<DecBlock>(),
+                                               dctl.get<WalkCtl>(), na, dbad.get<int>());
+    BZ_LAUNCH_CHECK();
+    k_dec_walk<<<wgrid, 64, 0, st>>>(didx.get<int32_t>(), ddb.get<DecBlock>(),
+                                     dtt.get<uint32_t>(), dctl.get<WalkCtl>(),
+                                     dmark.get<uint32_t>(), drle.get<uint8_t>(), cap, 1);
+    BZ_LAUNCH_CHECK();
+    k_dec_repeat<<<dim3(16, na), 256, 0, st>>>(didx.get<int32_t>(), ddb.get<DecBlock>(),
+                                               dctl.get<WalkCtl>(), drle.get<uint8_t>(), cap);
     BZ_LAUNCH_CHECK();
     k_dec_unrle1<<<(na + 31) / 32, 32, 0, st>>>(didx.get<int32_t>(), ddb.get<DecBlock>(),
                                                 drle.get<uint8_t>(), na, cap, 0,
                                                 dlens.get<int64_t>(), nullptr, nullptr, nullptr);
     BZ_LAUNCH_CHECK();
     std::vector<int64_t> lens(na), offs(na);
+    int hbad = 0;
     BZ_CUDA(cudaMemcpyAsync(lens.data(), dlens.p, 8 * na, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaMemcpyAsync(&hbad, dbad.p, 4, cudaMemcpyDeviceToHost, st));
     BZ_CUDA(cudaStreamSynchronize(st));
+    BZ_REQUIRE(hbad == 0, kErrArg, "bzip2 stream: inconsistent block (BWT chain)");
     int64_t tot = 0;
     for (int q = 0; q < na; q++) {
       offs[q] = tot;
