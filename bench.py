@@ -340,17 +340,34 @@ def main():
         B.compress_into(h_in, h_out, 9)  # warm the host path
         dte, oute = timed(lambda: B.compress_into(h_in, h_out, 9))
         assert bytes(h_out[:64].numpy()) == out[:64]
-        # the GPU decoder on the same stream (host bytes in, host bytes out;
-        # every block CRC and the stream CRC are checked by the decoder)
-        B.decompress(out)
+        # the GPU decoder on the same stream (every block CRC and the stream
+        # CRC are checked by the decoder): device-resident (stream and output
+        # in HBM) and end to end (pinned host stream in, pinned host bytes out)
+        h_comp = torch.empty(len(out), dtype=torch.uint8, pin_memory=True)
+        h_comp.numpy()[:] = np.frombuffer(out, np.uint8)
+        d_comp = h_comp.cuda()
+        d_dec = torch.empty(n, dtype=torch.uint8, device="cuda")
+        B.decompress_into(d_comp, d_dec)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        dec = B.decompress(out)
+        assert B.decompress_into(d_comp, d_dec) == n
+        torch.cuda.synchronize()
         ddt = max_over_ranks(time.perf_counter() - t0, world)
-        assert len(dec) == n and dec[:1 << 20] == h_in[:1 << 20].numpy().tobytes()
+        same = all(torch.equal(d_dec[i:i + (1 << 30)], h_in[i:i + (1 << 30)].cuda())
+                   for i in range(0, n, 1 << 30))
+        del d_dec, d_comp
+        h_dec = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+        t0 = time.perf_counter()
+        assert B.decompress_into(h_comp, h_dec) == n
+        hdt = max_over_ranks(time.perf_counter() - t0, world)
+        same = same and torch.equal(h_dec[-(1 << 24):], h_in[-(1 << 24):]) and \
+            torch.equal(h_dec[: 1 << 24], h_in[: 1 << 24])
+        del h_dec, h_comp
         decode = {"MB/s": round(n * world / ddt / 1e6, 2), "unit": "MB/s of output",
-                  "api": "bz2g_decompress (host stream in, host bytes out)"}
-        del dec
+                  "api": "bz2g_decompress_device_into (stream and output in HBM)",
+                  "e2e_MB/s": round(n * world / hdt / 1e6, 2),
+                  "e2e_api": "bz2g_decompress_into (pinned host stream in, pinned host out)",
+                  "output_identical": bool(same)}
         dte = max_over_ranks(dte, world)
         e2e = {"value": round(n * world * args.steps / dte / 1e6, 2), "unit": "MB/s",
                "h2d_bytes_per_step": n, "d2h_bytes_per_step": int(oute),

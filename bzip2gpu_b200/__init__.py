@@ -24,7 +24,7 @@ __all__ = [
     "huffman_encode", "count_frequencies", "gen_markov", "gen_uniform", "MAX_GROUPS",
     "MAX_ALPHA", "SELECTOR_PARAMS", "selector_load", "set_selector", "get_selector",
     "selector_logits", "huffman_build_learned", "selector_dataset", "compress_part",
-    "assemble", "compress_file", "decompress", "decompress_device",
+    "assemble", "compress_file", "decompress", "decompress_device", "decompress_into",
 ]
 
 MAX_GROUPS = 6
@@ -67,6 +67,8 @@ _SIGS = {
     "bz2g_compress_file": (_i, [_c.c_char_p, _c.c_char_p, _i, _i]),
     "bz2g_decompress": (_i, [_vp, _sz, _c.POINTER(_u8p), _c.POINTER(_sz)]),
     "bz2g_decompress_device": (_i, [_vp, _sz, _c.POINTER(_u8p), _c.POINTER(_sz)]),
+    "bz2g_decompress_into": (_i, [_vp, _sz, _vp, _sz, _c.POINTER(_sz)]),
+    "bz2g_decompress_device_into": (_i, [_vp, _sz, _vp, _sz, _c.POINTER(_sz)]),
     "bz2g_part_bound": (_sz, [_sz, _i]),
     "bz2g_compress_part": (_i, [_vp, _sz, _i, _i, _vp, _sz, _c.POINTER(_c.c_int64),
                                 _c.POINTER(_c.c_uint32), _c.POINTER(_i)]),
@@ -254,6 +256,28 @@ def decompress_device(d_in) -> bytes:
     _check(lib().bz2g_decompress_device(_ptr(d_in), d_in.numel(), ctypes.byref(out),
                                         ctypes.byref(ln)))
     return _take(out, ln.value)
+
+
+def decompress_into(data, out) -> int:
+    """Decode a .bz2 stream into a preallocated buffer; returns the decoded
+    length (raises if `out` is too small).  `data` and `out` are host buffers
+    (bytes, numpy arrays, CPU tensors; page-locked memory is copied directly)
+    or CUDA uint8 tensors, in any combination."""
+    ln = _sz()
+    if hasattr(data, "data_ptr"):
+        src, n = data.data_ptr(), data.numel()
+        fn = lib().bz2g_decompress_device_into if data.is_cuda else lib().bz2g_decompress_into
+    else:
+        keep, src = _host_view(data)
+        n, fn = keep.size, lib().bz2g_decompress_into
+    if hasattr(out, "data_ptr"):
+        dst, cap = out.data_ptr(), out.numel() * out.element_size()
+    else:
+        arr = out if isinstance(out, np.ndarray) else np.frombuffer(out, dtype=np.uint8)
+        assert arr.flags.c_contiguous and arr.flags.writeable
+        dst, cap = arr.ctypes.data, arr.nbytes
+    _check(fn(src if n else None, n, dst if cap else None, cap, ctypes.byref(ln)))
+    return ln.value
 
 
 def compress_file(in_path, out_path, level: int = 9, group_blocks: int = 0) -> None:

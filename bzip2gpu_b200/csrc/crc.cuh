@@ -1,0 +1,69 @@
+// CRC-32 of the bzip2 format (polynomial 0x04C11DB7, bits taken most
+// significant first; src/compression/crc32.cpp of the reference) and the
+// GF(2) arithmetic that combines the CRCs of separately processed pieces.
+//
+// crc0(D) (zero initial value, no final complement) is linear over GF(2):
+//   crc0(A || B) = crc0(A) * x^(8|B|) ^ crc0(B)        (mod P)
+// and the format's CRC is ~(~0 * x^(8|D|) ^ crc0(D)).
+#pragma once
+
+#include <stdint.h>
+
+namespace bz2g {
+namespace {
+
+constexpr uint32_t kPoly = 0x04C11DB7u;
+
+constexpr uint32_t gf_mul_c(uint32_t a, uint32_t b) {
+  uint32_t r = 0;
+  for (int i = 31; i >= 0; --i) {
+    r = (r << 1) ^ ((r & 0x80000000u) ? kPoly : 0u);
+    if ((b >> i) & 1u) r ^= a;
+  }
+  return r;
+}
+constexpr uint32_t xpow8_pow2(int i) {
+  uint32_t v = 0x100u;  // x^8
+  for (int k = 0; k < i; ++k) v = gf_mul_c(v, v);
+  return v;
+}
+
+#define BZ_XP4(i) xpow8_pow2(i), xpow8_pow2(i + 1), xpow8_pow2(i + 2), xpow8_pow2(i + 3)
+// c_xpow[i] = x^(8 * 2^i) mod P
+__constant__ uint32_t c_xpow[32] = {BZ_XP4(0),  BZ_XP4(4),  BZ_XP4(8),  BZ_XP4(12),
+                                    BZ_XP4(16), BZ_XP4(20), BZ_XP4(24), BZ_XP4(28)};
+#undef BZ_XP4
+
+__device__ __forceinline__ uint32_t gf_mul(uint32_t a, uint32_t b) {
+  uint32_t r = 0;
+#pragma unroll 8
+  for (int i = 31; i >= 0; --i) {
+    r = (r << 1) ^ ((r & 0x80000000u) ? kPoly : 0u);
+    if ((b >> i) & 1u) r ^= a;
+  }
+  return r;
+}
+
+// x^(8j) mod P
+__device__ __forceinline__ uint32_t xpow8(uint64_t j) {
+  uint32_t r = 1u;
+  for (int i = 0; j; ++i, j >>= 1)
+    if (j & 1u) r = gf_mul(r, c_xpow[i]);
+  return r;
+}
+
+// tbl[b] = crc0 of the single byte b
+__device__ __forceinline__ void crc_table_fill(uint32_t *tbl) {
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+    uint32_t c = (uint32_t)i << 24;
+    for (int k = 0; k < 8; k++) c = (c & 0x80000000u) ? (c << 1) ^ kPoly : (c << 1);
+    tbl[i] = c;
+  }
+}
+
+__device__ __forceinline__ uint32_t crc_byte(uint32_t crc, uint32_t byte, const uint32_t *tbl) {
+  return (crc << 8) ^ tbl[(crc >> 24) ^ byte];
+}
+
+}  // namespace
+}  // namespace bz2g

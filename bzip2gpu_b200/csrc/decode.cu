@@ -15,22 +15,29 @@
 //      BWT last column L and, per position, the rank of L[i] among equal
 //      symbols before it.
 //   3. k_dec_lf: LF vector tt[C[L[i]] + rank[i]] = i << 8 | L[i] (parallel).
-//   4. k_dec_walk: per block, the chain from origPtr gives the RLE1 bytes.
-//   5. k_dec_unrle1: per block, RLE1 runs expanded (4 equal bytes then a
-//      count byte), counted first, then written at the block's output offset
-//      with its CRC, checked against the block header.
+//   4. k_dec_split / k_dec_walk / k_dec_chain: per block, the chain from
+//      origPtr gives the RLE1 bytes, cut at up to 256 splitters that are
+//      walked in parallel.
+//   5. k_dec_unrle1_count / _write: per block, one warp expands the RLE1 runs
+//      (4 equal bytes then a count byte) from 32 segments at once, and the
+//      block CRC is checked against the header.
+// Batches of blocks go through steps 2-5 while the previous batch's bytes are
+// copied out on a second stream.
 // Every field read from the stream is range-checked and every loop is bounded,
 // so a malformed stream gives an error status, not a fault.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
 #include "../../include/bz2g.h"
 #include "common.cuh"
 #include "compressor.h"
+#include "crc.cuh"
 
 namespace bz2g {
 
@@ -501,7 +508,7 @@ __global__ void k_dec_walk(const int32_t *idx, const DecBlock *db, const uint32_
   const int m = db[idx[k]].m;
   const uint32_t *T = tt + (size_t)k * cap;
   const uint32_t *M = mark + (size_t)k * ((cap + 31) / 32);
-  uint8_t *R = rle + (size_t)k * cap;
+  uint8_t *R = rle + (size_t)idx[k] * cap;
   if (write && c.off[w] < 0) return;
   uint32_t p = (uint32_t)c.pos[w];
   int n = 0;
@@ -549,163 +556,388 @@ __global__ void k_dec_repeat(const int32_t *idx, const DecBlock *db, const WalkC
   const int m = db[idx[k]].m;
   const int cyc = ctl[k].cycle;
   if (cyc <= 0 || cyc >= m) return;
-  uint8_t *R = rle + (size_t)k * cap;
+  uint8_t *R = rle + (size_t)idx[k] * cap;
   for (int i = cyc + blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
     R[i] = R[i % cyc];
 }
 
-// RLE1 inverse of one block: 4 equal bytes are followed by a count of further
-// copies.  write == 0: count the output bytes; write != 0: write them at
-// out + off[k] and compute the block CRC.
-__device__ __forceinline__ uint32_t crc_byte(uint32_t crc, uint32_t byte, const uint32_t *tbl) {
-  return (crc << 8) ^ tbl[(crc >> 24) ^ byte];
-}
 
-__global__ void k_dec_unrle1(const int32_t *idx, const DecBlock *db, const uint8_t *rle,
-                             int nacc, int cap, int write, int64_t *lens, const int64_t *off,
-                             uint8_t *out, uint32_t *crcs) {
-  __shared__ uint32_t tbl[256];
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) {
-    uint32_t c = (uint32_t)i << 24;
-    for (int q = 0; q < 8; q++) c = (c & 0x80000000u) ? (c << 1) ^ 0x04C11DB7u : (c << 1);
-    tbl[i] = c;
-  }
-  __syncthreads();
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nacc) return;
-  const DecBlock b = db[idx[k]];
-  const uint8_t *R = rle + (size_t)k * cap;
-  uint8_t *O = write ? out + off[k] : nullptr;
-  int64_t n = 0;
-  uint32_t crc = 0xFFFFFFFFu;
-  int prev = -1, run = 0;
-  for (int i = 0; i < b.m; i++) {
-    const int c = R[i];
-    if (run == 4) {
-      for (int q = 0; q < c; q++) {
-        if (write) {
-          O[n] = (uint8_t)prev;
-          crc = crc_byte(crc, (uint32_t)prev, tbl);
-        }
-        n++;
-      }
-      run = 0;
-      prev = -1;
-      continue;
-    }
-    if (c == prev) run++;
-    else {
-      prev = c;
-      run = 1;
-    }
-    if (write) {
-      O[n] = (uint8_t)c;
-      crc = crc_byte(crc, (uint32_t)c, tbl);
-    }
+// Inverse RLE1 (4 equal bytes are followed by a count of further copies), one
+// warp per block.  The block's RLE1 bytes are cut into 32 lane segments.  What
+// a segment produces depends only on the run state it starts in: 0 = no run
+// (block start, or just after a count byte), 1..3 = the byte before the
+// segment closes a run of that length, 4 = the next byte is a count.  The
+// count pass follows each segment from all five states at once until they
+// merge (typically within a few bytes: at a byte that differs from the one
+// before it), chains the lanes' state maps from state 0 across the warp and
+// keeps each lane's entry state and output offset; the write pass expands
+// every segment at its offset and combines the lanes' CRCs over GF(2).
+constexpr int kUnrleWarps = 8;
+
+struct LaneStart {
+  int32_t state;
+  int32_t off;  // output offset of the segment within its block
+};
+
+__device__ __forceinline__ void rle1_step(int &r, int &n, int c, int p) {
+  if (r == 4) {
+    n += c;
+    r = 0;
+  } else if (r >= 1 && c == p) {
+    r++;
+    n++;
+  } else {
+    r = 1;
     n++;
   }
-  if (write) crcs[k] = ~crc;
-  else lens[k] = n;
 }
 
-cudaStream_t S(void *p) { return reinterpret_cast<cudaStream_t>(p); }
+__device__ __forceinline__ int pick5(int x, int a0, int a1, int a2, int a3, int a4) {
+  return x == 0 ? a0 : x == 1 ? a1 : x == 2 ? a2 : x == 3 ? a3 : a4;
+}
 
+__global__ void __launch_bounds__(32 * kUnrleWarps)
+    k_dec_unrle1_count(const int32_t *idx, const DecBlock *db, const uint8_t *rle, int nacc,
+                       int cap, LaneStart *lanes, int64_t *lens) {
+  const int k = blockIdx.x * kUnrleWarps + (threadIdx.x >> 5);
+  const int ln = threadIdx.x & 31;
+  if (k >= nacc) return;  // the whole warp
+  const int bi = idx[k];
+  const int m = db[bi].m;
+  const uint8_t *R = rle + (size_t)bi * cap;
+  const int seg = (m + 31) / 32;
+  const int s0 = min(ln * seg, m), e0 = min(s0 + seg, m);
+  int p = s0 > 0 ? R[s0 - 1] : -1;
+  int r0 = 0, r1 = 1, r2 = 2, r3 = 3, r4 = 4;
+  int n0 = 0, n1 = 0, n2 = 0, n3 = 0, n4 = 0;
+  int i = s0;
+  bool merged = false;
+  while (i < e0 && !merged) {
+    const int c = R[i++];
+    rle1_step(r0, n0, c, p);
+    rle1_step(r1, n1, c, p);
+    rle1_step(r2, n2, c, p);
+    rle1_step(r3, n3, c, p);
+    rle1_step(r4, n4, c, p);
+    p = c;
+    merged = r0 == r1 && r0 == r2 && r0 == r3 && r0 == r4;
+  }
+  int r = r0, nb = 0;
+  while (i < e0) {
+    const int c = R[i++];
+    rle1_step(r, nb, c, p);
+    p = c;
+  }
+  if (merged) {
+    r0 = r1 = r2 = r3 = r4 = r;
+    n0 += nb;
+    n1 += nb;
+    n2 += nb;
+    n3 += nb;
+    n4 += nb;
+  }
+  int state = 0, off = 0, my_state = 0, my_off = 0;
+  for (int l = 0; l < 32; l++) {
+    if (ln == l) {
+      my_state = state;
+      my_off = off;
+    }
+    const int ro = __shfl_sync(0xffffffffu, pick5(state, r0, r1, r2, r3, r4), l);
+    const int no = __shfl_sync(0xffffffffu, pick5(state, n0, n1, n2, n3, n4), l);
+    state = ro;
+    off += no;
+  }
+  lanes[(size_t)k * 32 + ln] = LaneStart{my_state, my_off};
+  if (ln == 0) lens[k] = off;
+}
+
+__global__ void __launch_bounds__(32 * kUnrleWarps)
+    k_dec_unrle1_write(const int32_t *idx, const DecBlock *db, const uint8_t *rle, int nacc,
+                       int cap, const LaneStart *lanes, const int64_t *lens, const int64_t *off,
+                       uint8_t *out, uint32_t *crcs) {
+  __shared__ uint32_t tbl[256];
+  crc_table_fill(tbl);
+  __syncthreads();
+  const int k = blockIdx.x * kUnrleWarps + (threadIdx.x >> 5);
+  const int ln = threadIdx.x & 31;
+  if (k >= nacc) return;
+  const int bi = idx[k];
+  const int m = db[bi].m;
+  const uint8_t *R = rle + (size_t)bi * cap;
+  const int seg = (m + 31) / 32;
+  const int s0 = min(ln * seg, m), e0 = min(s0 + seg, m);
+  int p = s0 > 0 ? R[s0 - 1] : -1;
+  const LaneStart ls = lanes[(size_t)k * 32 + ln];
+  int r = ls.state;
+  int64_t pos = ls.off;
+  uint8_t *O = out + off[k];
+  uint32_t crc = 0;
+  for (int i = s0; i < e0; i++) {
+    const int c = R[i];
+    if (r == 4) {
+      for (int q = 0; q < c; q++) {
+        O[pos++] = (uint8_t)p;
+        crc = crc_byte(crc, (uint32_t)p, tbl);
+      }
+      r = 0;
+    } else {
+      r = (r >= 1 && c == p) ? r + 1 : 1;
+      O[pos++] = (uint8_t)c;
+      crc = crc_byte(crc, (uint32_t)c, tbl);
+    }
+    p = c;
+  }
+  const int64_t total = lens[k];
+  uint32_t v = crc ? gf_mul(crc, xpow8((uint64_t)(total - pos))) : 0u;
+  for (int o = 16; o; o >>= 1) v ^= __shfl_xor_sync(0xffffffffu, v, o);
+  if (ln == 0) crcs[k] = ~(gf_mul(0xFFFFFFFFu, xpow8((uint64_t)total)) ^ v);
+}
+
+// Device buffer that only grows (contents are not kept).
 struct DevBuf {
   void *p = nullptr;
-  ~DevBuf() {
-    if (p) cudaFree(p);
-  }
+  size_t cap = 0;
   template <typename T>
   T *get() const {
     return static_cast<T *>(p);
   }
-  void alloc(size_t bytes) {
-    BZ_CUDA(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+  void reserve(size_t bytes) {
+    bytes = std::max<size_t>(bytes, 16);
+    if (bytes <= cap) return;
+    if (p) BZ_CUDA(cudaFree(p));
+    p = nullptr;
+    cap = 0;
+    BZ_CUDA(cudaMalloc(&p, bytes));
+    cap = bytes;
   }
 };
 
-// The decoder proper: stream (device) -> output (host vector).
-void decode_stream(const uint8_t *d_in, size_t n, std::vector<uint8_t> &out, cudaStream_t st) {
-  out.clear();
-  BZ_REQUIRE(n >= 14, kErrArg, "not a bzip2 stream (shorter than 14 bytes)");
-  std::vector<uint8_t> head(4);
-  BZ_CUDA(cudaMemcpy(head.data(), d_in, 4, cudaMemcpyDeviceToHost));
-  BZ_REQUIRE(head[0] == 'B' && head[1] == 'Z' && head[2] == 'h' && head[3] >= '1' &&
-                 head[3] <= '9',
-             kErrArg, "not a bzip2 stream (bad header)");
-  // words, padded
+// Where decoded bytes go, batch by batch, in stream order.
+struct DecSink {
+  size_t size = 0;
+  virtual ~DecSink() = default;
+  // Queue the copy of n device bytes to the end of the output on stream cs.
+  virtual void put(const uint8_t *d_src, size_t n, cudaStream_t cs) = 0;
+};
+
+// A caller's buffer of cap bytes (host or device memory).
+struct BufferSink : DecSink {
+  uint8_t *dst;
+  size_t cap;
+  BufferSink(uint8_t *d, size_t c) : dst(d), cap(c) {}
+  void put(const uint8_t *d_src, size_t n, cudaStream_t cs) override {
+    BZ_REQUIRE(n <= cap - size, kErrTooLarge,
+               "decoded data larger than the output buffer (" + std::to_string(cap) + " bytes)");
+    if (n) BZ_CUDA(cudaMemcpyAsync(dst + size, d_src, n, cudaMemcpyDefault, cs));
+    size += n;
+  }
+};
+
+// A malloc'ed host buffer grown by realloc (large blocks are remapped, not
+// copied, and pages are touched only by the copies into them).
+struct MallocSink : DecSink {
+  uint8_t *buf = nullptr;
+  size_t cap = 0;
+  ~MallocSink() override { std::free(buf); }
+  void put(const uint8_t *d_src, size_t n, cudaStream_t cs) override {
+    if (n > cap - size) {
+      BZ_CUDA(cudaStreamSynchronize(cs));  // no copy into the old buffer in flight
+      const size_t nc = std::max(size + n, 2 * cap);
+      void *q = std::realloc(buf, nc);
+      BZ_REQUIRE(q != nullptr, kErrAlloc, "host allocation failed");
+      buf = static_cast<uint8_t *>(q);
+      cap = nc;
+    }
+    if (n) BZ_CUDA(cudaMemcpyAsync(buf + size, d_src, n, cudaMemcpyDefault, cs));
+    size += n;
+  }
+  uint8_t *release() {
+    uint8_t *p = buf;
+    if (!p) p = static_cast<uint8_t *>(std::malloc(1));
+    else if (size && size < cap) p = static_cast<uint8_t *>(std::realloc(buf, size));
+    BZ_REQUIRE(p != nullptr, kErrAlloc, "host allocation failed");
+    buf = nullptr;
+    cap = 0;
+    return p;
+  }
+};
+
+// The decoder's device scratch, one per device, grown on demand and kept
+// between calls.  Output batches alternate between two device buffers: the
+// copy of one batch to the sink (stream cs) overlaps the decoding of the next
+// (stream st).
+struct DecWork {
+  std::mutex mu;
+  DevBuf words, blk, eos, cnt, cand, db, L, rank, sel, idx, C, tt, lens, off, crc, ctl, mark,
+      bad, lanes;
+  DevBuf out[2];
+  cudaStream_t st = nullptr, cs = nullptr;
+  cudaEvent_t written[2] = {nullptr, nullptr}, copied[2] = {nullptr, nullptr};
+  bool used[2] = {false, false};
+  uint32_t *h_crc = nullptr;  // pinned
+  size_t h_crc_cap = 0;
+  int resident = 0;  // k_dec_block warps resident on the whole device
+
+  void init() {
+    if (st) return;
+    BZ_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    BZ_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    for (int q = 0; q < 2; q++) {
+      BZ_CUDA(cudaEventCreateWithFlags(&written[q], cudaEventDisableTiming));
+      BZ_CUDA(cudaEventCreateWithFlags(&copied[q], cudaEventDisableTiming));
+    }
+    int dev = 0, sms = 0, per_sm = 0;
+    BZ_CUDA(cudaGetDevice(&dev));
+    BZ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    BZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dec_block, 32, 0));
+    resident = std::max(1, sms * per_sm);
+  }
+  size_t held() const {
+    size_t s = 0;
+    for (const DevBuf *b : {&L, &rank, &tt, &sel, &mark, &out[0], &out[1]}) s += b->cap;
+    return s;
+  }
+};
+
+DecWork &dec_work() {
+  static std::mutex mu;
+  static std::vector<DecWork *> per_device;  // kept for the process lifetime
+  int dev = 0;
+  BZ_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  if ((int)per_device.size() <= dev) per_device.resize(dev + 1, nullptr);
+  if (!per_device[dev]) per_device[dev] = new DecWork();
+  return *per_device[dev];
+}
+
+// Device bytes of one candidate slot: last column (later the RLE1 bytes),
+// ranks, LF vector, selectors, visited marks.
+constexpr size_t kSlotBytes = (size_t)kDecCap * 9 + kDecMaxSel + (kDecCap + 31) / 32 * 4 +
+                              sizeof(WalkCtl) + sizeof(DecBlock) + 256 * 4 + 32 * 8 + 64;
+constexpr int kMaxBatch = 4096;
+
+bool is_header(const uint8_t *h) {
+  return h[0] == 'B' && h[1] == 'Z' && h[2] == 'h' && h[3] >= '1' && h[3] <= '9';
+}
+
+// The decoder proper.  w.words holds the n stream bytes, zero-padded to whole
+// words plus two.
+void decode_words(DecWork &w, size_t n, DecSink &sink) {
+  cudaStream_t st = w.st, cs = w.cs;
+  // on every exit no kernel or copy is left in flight (the sink's memory may
+  // be released by the caller)
+  struct Drain {
+    cudaStream_t a, b;
+    ~Drain() {
+      cudaStreamSynchronize(a);
+      cudaStreamSynchronize(b);
+    }
+  } drain{st, cs};
+  const uint8_t *bytes = w.words.get<uint8_t>();
   const int64_t nwords = (int64_t)(n + 3) / 4 + 2;
-  DevBuf words;
-  words.alloc(nwords * 4);
-  BZ_CUDA(cudaMemsetAsync(words.p, 0, nwords * 4, st));
-  BZ_CUDA(cudaMemcpyAsync(words.p, d_in, n, cudaMemcpyDeviceToDevice, st));
+  uint8_t head[4];
+  BZ_CUDA(cudaMemcpyAsync(head, bytes, 4, cudaMemcpyDeviceToHost, st));
+  BZ_CUDA(cudaStreamSynchronize(st));
+  BZ_REQUIRE(is_header(head), kErrArg, "not a bzip2 stream (bad header)");
   const int64_t nbits = (int64_t)n * 8;
   // candidates
   const int ccap = (int)std::min<int64_t>((int64_t)n / 8 + 64, 1 << 26);
-  DevBuf dblk, deos, dcnt;
-  dblk.alloc(8 * (size_t)ccap);
-  deos.alloc(8 * (size_t)ccap);
-  dcnt.alloc(8);
-  BZ_CUDA(cudaMemsetAsync(dcnt.p, 0, 8, st));
+  w.blk.reserve(8 * (size_t)ccap);
+  w.eos.reserve(8 * (size_t)ccap);
+  w.cnt.reserve(8);
+  BZ_CUDA(cudaMemsetAsync(w.cnt.p, 0, 8, st));
   k_dec_magic<<<(unsigned)((nwords + 255) / 256), 256, 0, st>>>(
-      words.get<uint32_t>(), nwords, nbits, dblk.get<int64_t>(), dcnt.get<int>(),
-      deos.get<int64_t>(), dcnt.get<int>() + 1, ccap);
+      w.words.get<uint32_t>(), nwords, nbits, w.blk.get<int64_t>(), w.cnt.get<int>(),
+      w.eos.get<int64_t>(), w.cnt.get<int>() + 1, ccap);
   BZ_LAUNCH_CHECK();
   int hcnt[2];
-  BZ_CUDA(cudaMemcpyAsync(hcnt, dcnt.p, 8, cudaMemcpyDeviceToHost, st));
+  BZ_CUDA(cudaMemcpyAsync(hcnt, w.cnt.p, 8, cudaMemcpyDeviceToHost, st));
   BZ_CUDA(cudaStreamSynchronize(st));
   BZ_REQUIRE(hcnt[0] <= ccap && hcnt[1] <= ccap, kErrTooLarge, "too many block candidates");
   std::vector<int64_t> cands(hcnt[0]), eoss(hcnt[1]);
-  if (hcnt[0]) BZ_CUDA(cudaMemcpy(cands.data(), dblk.p, 8 * hcnt[0], cudaMemcpyDeviceToHost));
-  if (hcnt[1]) BZ_CUDA(cudaMemcpy(eoss.data(), deos.p, 8 * hcnt[1], cudaMemcpyDeviceToHost));
+  if (hcnt[0])
+    BZ_CUDA(cudaMemcpyAsync(cands.data(), w.blk.p, 8 * hcnt[0], cudaMemcpyDeviceToHost, st));
+  if (hcnt[1])
+    BZ_CUDA(cudaMemcpyAsync(eoss.data(), w.eos.p, 8 * hcnt[1], cudaMemcpyDeviceToHost, st));
+  BZ_CUDA(cudaStreamSynchronize(st));
   std::sort(cands.begin(), cands.end());
   std::sort(eoss.begin(), eoss.end());
-  // decode candidates in batches (about 12 bytes of scratch per last-column
-  // entry); follow the chain of blocks and streams
-  const int batch = (int)std::min<size_t>(2048, std::max<size_t>(cands.size(), 1));
+  // batch: whole waves of resident k_dec_block warps where memory allows
+  size_t freeb = 0, totb = 0;
+  BZ_CUDA(cudaMemGetInfo(&freeb, &totb));
+  int bmax = (int)std::min<size_t>(kMaxBatch, (freeb + w.held()) / 3 / kSlotBytes);
+  bmax = std::max(bmax, 32);
+  if (bmax >= w.resident) bmax = bmax / w.resident * w.resident;
+  // BZ2G_DECODE_BATCH caps the blocks per batch (smaller batches, less memory)
+  if (const char *e = std::getenv("BZ2G_DECODE_BATCH")) {
+    const int v = std::atoi(e);
+    if (v > 0) bmax = std::min(bmax, v);
+  }
+  const int batch = (int)std::min<size_t>(bmax, std::max<size_t>(cands.size(), 1));
   const int cap = kDecCap;
-  DevBuf dcand, ddb, dL, drank, dsel, didx, dC, dtt, drle, dlens, doff, dcrc;
-  dcand.alloc(8 * (size_t)batch);
-  ddb.alloc(sizeof(DecBlock) * (size_t)batch);
-  dL.alloc((size_t)batch * cap);
-  drank.alloc((size_t)batch * cap * 4);
-  dsel.alloc((size_t)batch * kDecMaxSel);
-  didx.alloc(4 * (size_t)batch);
-  dC.alloc((size_t)batch * 256 * 4);
-  dtt.alloc((size_t)batch * cap * 4);
-  drle.alloc((size_t)batch * cap);
-  dlens.alloc(8 * (size_t)batch);
-  doff.alloc(8 * (size_t)batch);
-  dcrc.alloc(4 * (size_t)batch);
-  DevBuf dctl, dmark, dbad;
-  dctl.alloc(sizeof(WalkCtl) * (size_t)batch);
-  dmark.alloc((size_t)batch * ((cap + 31) / 32) * 4);
-  dbad.alloc(16);
-  int64_t expect = 32;  // next block or end-of-stream marker
+  w.cand.reserve(8 * (size_t)batch);
+  w.db.reserve(sizeof(DecBlock) * (size_t)batch);
+  w.L.reserve((size_t)batch * cap);
+  w.rank.reserve((size_t)batch * cap * 4);
+  w.sel.reserve((size_t)batch * kDecMaxSel);
+  w.idx.reserve(4 * (size_t)batch);
+  w.C.reserve((size_t)batch * 256 * 4);
+  w.tt.reserve((size_t)batch * cap * 4);
+  w.lens.reserve(8 * (size_t)batch);
+  w.off.reserve(8 * (size_t)batch);
+  w.crc.reserve(4 * (size_t)batch);
+  w.ctl.reserve(sizeof(WalkCtl) * (size_t)batch);
+  w.mark.reserve((size_t)batch * ((cap + 31) / 32) * 4);
+  w.bad.reserve(16);
+  w.lanes.reserve(sizeof(LaneStart) * 32 * (size_t)batch);
+  if (w.h_crc_cap < (size_t)batch) {
+    if (w.h_crc) BZ_CUDA(cudaFreeHost(w.h_crc));
+    w.h_crc = nullptr;
+    w.h_crc_cap = 0;
+    BZ_CUDA(cudaMallocHost((void **)&w.h_crc, 4 * (size_t)batch));
+    w.h_crc_cap = batch;
+  }
+  uint8_t *L = w.L.get<uint8_t>();  // the RLE1 bytes overwrite the last column
+  int64_t expect = 32;              // next block or end-of-stream marker
   uint32_t stream_crc = 0;
   bool stream_done = false;
   size_t ci = 0;
+  int nbatch = 0;
   std::vector<DecBlock> hdb(batch);
+  // block CRCs of the last batch, checked once st has caught up
+  std::vector<uint32_t> want;
+  auto settle = [&]() {
+    if (want.empty()) return;
+    BZ_CUDA(cudaStreamSynchronize(st));
+    for (size_t q = 0; q < want.size(); q++) {
+      BZ_REQUIRE(w.h_crc[q] == want[q], kErrArg, "bzip2 stream: block CRC mismatch");
+      stream_crc = ((stream_crc << 1) | (stream_crc >> 31)) ^ w.h_crc[q];
+    }
+    want.clear();
+  };
   for (;;) {
     if (stream_done) {
       // another stream may follow, from the next byte boundary
       const int64_t nb = (expect + 7) / 8;
       if (nb + 14 > (int64_t)n) break;
       uint8_t h[4];
-      BZ_CUDA(cudaMemcpy(h, d_in + nb, 4, cudaMemcpyDeviceToHost));
-      if (!(h[0] == 'B' && h[1] == 'Z' && h[2] == 'h' && h[3] >= '1' && h[3] <= '9')) break;
+      BZ_CUDA(cudaMemcpyAsync(h, bytes + nb, 4, cudaMemcpyDeviceToHost, st));
+      BZ_CUDA(cudaStreamSynchronize(st));
+      if (!is_header(h)) break;
       expect = nb * 8 + 32;
       stream_crc = 0;
       stream_done = false;
     }
     // the end-of-stream marker at `expect`?
     if (std::binary_search(eoss.begin(), eoss.end(), expect)) {
+      settle();
       // combined CRC after the 48-bit marker
       const int64_t p = expect + 48;
       uint8_t tail[8] = {0};
       const int64_t b0 = p / 8;
       const size_t nb = (size_t)std::min<int64_t>(8, (int64_t)n - b0);
-      BZ_CUDA(cudaMemcpy(tail, d_in + b0, nb, cudaMemcpyDeviceToHost));
+      BZ_CUDA(cudaMemcpyAsync(tail, bytes + b0, nb, cudaMemcpyDeviceToHost, st));
+      BZ_CUDA(cudaStreamSynchronize(st));
       uint64_t win = 0;
       for (int q = 0; q < 8; q++) win = (win << 8) | tail[q];
       const uint32_t got = (uint32_t)((win << (p % 8)) >> 32);
@@ -719,13 +951,15 @@ void decode_stream(const uint8_t *d_in, size_t n, std::vector<uint8_t> &out, cud
     BZ_REQUIRE(ci < cands.size() && cands[ci] == expect, kErrArg,
                "bzip2 stream: no block or end-of-stream marker where one must start");
     const int nc = (int)std::min<size_t>(batch, cands.size() - ci);
-    BZ_CUDA(cudaMemcpyAsync(dcand.p, cands.data() + ci, 8 * nc, cudaMemcpyHostToDevice, st));
-    k_dec_block<<<nc, 32, 0, st>>>(words.get<uint32_t>(), nwords, dcand.get<int64_t>(), nc,
-                                   ddb.get<DecBlock>(), dL.get<uint8_t>(), drank.get<int32_t>(),
-                                   dsel.get<uint8_t>(), cap);
+    BZ_CUDA(cudaMemcpyAsync(w.cand.p, cands.data() + ci, 8 * nc, cudaMemcpyHostToDevice, st));
+    k_dec_block<<<nc, 32, 0, st>>>(w.words.get<uint32_t>(), nwords, w.cand.get<int64_t>(), nc,
+                                   w.db.get<DecBlock>(), L, w.rank.get<int32_t>(),
+                                   w.sel.get<uint8_t>(), cap);
     BZ_LAUNCH_CHECK();
-    BZ_CUDA(cudaMemcpyAsync(hdb.data(), ddb.p, sizeof(DecBlock) * nc, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaMemcpyAsync(hdb.data(), w.db.p, sizeof(DecBlock) * nc, cudaMemcpyDeviceToHost,
+                            st));
     BZ_CUDA(cudaStreamSynchronize(st));
+    settle();
     // accept the chain within this batch
     std::vector<int32_t> acc;
     size_t used = 0;
@@ -741,41 +975,38 @@ void decode_stream(const uint8_t *d_in, size_t n, std::vector<uint8_t> &out, cud
     ci += std::max<size_t>(used, 1);
     const int na = (int)acc.size();
     if (na == 0) continue;
-    BZ_CUDA(cudaMemcpyAsync(didx.p, acc.data(), 4 * na, cudaMemcpyHostToDevice, st));
-    k_dec_counts<<<na, 256, 0, st>>>(didx.get<int32_t>(), ddb.get<DecBlock>(), dL.get<uint8_t>(),
-                                     dC.get<int32_t>(), cap);
+    const int32_t *didx = w.idx.get<int32_t>();
+    const DecBlock *ddb = w.db.get<DecBlock>();
+    BZ_CUDA(cudaMemcpyAsync(w.idx.p, acc.data(), 4 * na, cudaMemcpyHostToDevice, st));
+    k_dec_counts<<<na, 256, 0, st>>>(didx, ddb, L, w.C.get<int32_t>(), cap);
     BZ_LAUNCH_CHECK();
-    k_dec_lf<<<dim3(64, na), 256, 0, st>>>(didx.get<int32_t>(), ddb.get<DecBlock>(),
-                                           dL.get<uint8_t>(), drank.get<int32_t>(),
-                                           dC.get<int32_t>(), dtt.get<uint32_t>(), cap);
+    k_dec_lf<<<dim3(64, na), 256, 0, st>>>(didx, ddb, L, w.rank.get<int32_t>(),
+                                           w.C.get<int32_t>(), w.tt.get<uint32_t>(), cap);
     BZ_LAUNCH_CHECK();
-    k_dec_split<<<na, 256, 0, st>>>(didx.get<int32_t>(), ddb.get<DecBlock>(),
-                                    dctl.get<WalkCtl>(), dmark.get<uint32_t>(), cap);
+    k_dec_split<<<na, 256, 0, st>>>(didx, ddb, w.ctl.get<WalkCtl>(), w.mark.get<uint32_t>(),
+                                    cap);
     BZ_LAUNCH_CHECK();
     const dim3 wgrid(kMaxWalkers / 64, na);
-    k_dec_walk<<<wgrid, 64, 0, st>>>(didx.get<int32_t>(), ddb.get<DecBlock>(),
-                                     dtt.get<uint32_t>(), dctl.get<WalkCtl>(),
-                                     dmark.get<uint32_t>(), drle.get<uint8_t>(), cap, 0);
+    k_dec_walk<<<wgrid, 64, 0, st>>>(didx, ddb, w.tt.get<uint32_t>(), w.ctl.get<WalkCtl>(),
+                                     w.mark.get<uint32_t>(), L, cap, 0);
     BZ_LAUNCH_CHECK();
-    BZ_CUDA(cudaMemsetAsync(dbad.p, 0, 4, st));
-    k_dec_chain<<<(na + 63) / 64, 64, 0, st>>>(didx.get<int32_t>(), ddb.get<DecBlock>(),
-                                               dctl.get<WalkCtl>(), na, dbad.get<int>());
+    BZ_CUDA(cudaMemsetAsync(w.bad.p, 0, 4, st));
+    k_dec_chain<<<(na + 63) / 64, 64, 0, st>>>(didx, ddb, w.ctl.get<WalkCtl>(), na,
+                                               w.bad.get<int>());
     BZ_LAUNCH_CHECK();
-    k_dec_walk<<<wgrid, 64, 0, st>>>(didx.get<int32_t>(), ddb.get<DecBlock>(),
-                                     dtt.get<uint32_t>(), dctl.get<WalkCtl>(),
-                                     dmark.get<uint32_t>(), drle.get<uint8_t>(), cap, 1);
+    k_dec_walk<<<wgrid, 64, 0, st>>>(didx, ddb, w.tt.get<uint32_t>(), w.ctl.get<WalkCtl>(),
+                                     w.mark.get<uint32_t>(), L, cap, 1);
     BZ_LAUNCH_CHECK();
-    k_dec_repeat<<<dim3(16, na), 256, 0, st>>>(didx.get<int32_t>(), ddb.get<DecBlock>(),
-                                               dctl.get<WalkCtl>(), drle.get<uint8_t>(), cap);
+    k_dec_repeat<<<dim3(16, na), 256, 0, st>>>(didx, ddb, w.ctl.get<WalkCtl>(), L, cap);
     BZ_LAUNCH_CHECK();
-    k_dec_unrle1<<<(na + 31) / 32, 32, 0, st>>>(didx.get<int32_t>(), ddb.get<DecBlock>(),
-                                                drle.get<uint8_t>(), na, cap, 0,
-                                                dlens.get<int64_t>(), nullptr, nullptr, nullptr);
+    const unsigned ugrid = (unsigned)((na + kUnrleWarps - 1) / kUnrleWarps);
+    k_dec_unrle1_count<<<ugrid, 32 * kUnrleWarps, 0, st>>>(
+        didx, ddb, L, na, cap, w.lanes.get<LaneStart>(), w.lens.get<int64_t>());
     BZ_LAUNCH_CHECK();
     std::vector<int64_t> lens(na), offs(na);
     int hbad = 0;
-    BZ_CUDA(cudaMemcpyAsync(lens.data(), dlens.p, 8 * na, cudaMemcpyDeviceToHost, st));
-    BZ_CUDA(cudaMemcpyAsync(&hbad, dbad.p, 4, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaMemcpyAsync(lens.data(), w.lens.p, 8 * na, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaMemcpyAsync(&hbad, w.bad.p, 4, cudaMemcpyDeviceToHost, st));
     BZ_CUDA(cudaStreamSynchronize(st));
     BZ_REQUIRE(hbad == 0, kErrArg, "bzip2 stream: inconsistent block (BWT chain)");
     int64_t tot = 0;
@@ -783,44 +1014,49 @@ void decode_stream(const uint8_t *d_in, size_t n, std::vector<uint8_t> &out, cud
       offs[q] = tot;
       tot += lens[q];
     }
-    DevBuf dout;
-    dout.alloc((size_t)tot + 16);
-    BZ_CUDA(cudaMemcpyAsync(doff.p, offs.data(), 8 * na, cudaMemcpyHostToDevice, st));
-    k_dec_unrle1<<<(na + 31) / 32, 32, 0, st>>>(didx.get<int32_t>(), ddb.get<DecBlock>(),
-                                                drle.get<uint8_t>(), na, cap, 1, nullptr,
-                                                doff.get<int64_t>(), dout.get<uint8_t>(),
-                                                dcrc.get<uint32_t>());
-    BZ_LAUNCH_CHECK();
-    std::vector<uint32_t> crcs(na);
-    const size_t base = out.size();
-    out.resize(base + (size_t)tot);
-    BZ_CUDA(cudaMemcpyAsync(out.data() + base, dout.p, (size_t)tot, cudaMemcpyDeviceToHost, st));
-    BZ_CUDA(cudaMemcpyAsync(crcs.data(), dcrc.p, 4 * na, cudaMemcpyDeviceToHost, st));
-    BZ_CUDA(cudaStreamSynchronize(st));
-    for (int q = 0; q < na; q++) {
-      BZ_REQUIRE(crcs[q] == hdb[acc[q]].crc, kErrArg, "bzip2 stream: block CRC mismatch");
-      stream_crc = ((stream_crc << 1) | (stream_crc >> 31)) ^ crcs[q];
+    const int slot = nbatch++ & 1;
+    if (w.used[slot]) {
+      if ((size_t)tot + 16 > w.out[slot].cap) BZ_CUDA(cudaEventSynchronize(w.copied[slot]));
+      BZ_CUDA(cudaStreamWaitEvent(st, w.copied[slot], 0));
     }
+    w.out[slot].reserve((size_t)tot + 16);
+    BZ_CUDA(cudaMemcpyAsync(w.off.p, offs.data(), 8 * na, cudaMemcpyHostToDevice, st));
+    k_dec_unrle1_write<<<ugrid, 32 * kUnrleWarps, 0, st>>>(
+        didx, ddb, L, na, cap, w.lanes.get<LaneStart>(), w.lens.get<int64_t>(),
+        w.off.get<int64_t>(), w.out[slot].get<uint8_t>(), w.crc.get<uint32_t>());
+    BZ_LAUNCH_CHECK();
+    BZ_CUDA(cudaMemcpyAsync(w.h_crc, w.crc.p, 4 * na, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaEventRecord(w.written[slot], st));
+    BZ_CUDA(cudaStreamWaitEvent(cs, w.written[slot], 0));
+    sink.put(w.out[slot].get<uint8_t>(), (size_t)tot, cs);
+    BZ_CUDA(cudaEventRecord(w.copied[slot], cs));
+    w.used[slot] = true;
+    want.resize(na);
+    for (int q = 0; q < na; q++) want[q] = hdb[acc[q]].crc;
   }
+  settle();
   BZ_REQUIRE(stream_done, kErrArg, "bzip2 stream: no end-of-stream marker");
+  BZ_CUDA(cudaStreamSynchronize(cs));
 }
 
-}  // namespace
-}  // namespace bz2g
+// Stages the stream (host or device memory) in the workspace and decodes it.
+void decode_into_sink(const uint8_t *in, size_t n, DecSink &sink) {
+  BZ_REQUIRE(n >= 14, kErrArg, "not a bzip2 stream (shorter than 14 bytes)");
+  DecWork &w = dec_work();
+  std::lock_guard<std::mutex> g(w.mu);
+  w.init();
+  const size_t nwords = (n + 3) / 4 + 2;
+  w.words.reserve(nwords * 4);
+  const size_t body = n / 4 * 4;
+  BZ_CUDA(cudaMemsetAsync(w.words.get<uint8_t>() + body, 0, nwords * 4 - body, w.st));
+  BZ_CUDA(cudaMemcpyAsync(w.words.p, in, n, cudaMemcpyDefault, w.st));
+  decode_words(w, n, sink);
+}
 
-using namespace bz2g;
-
-extern "C" int bz2g_decompress_device(const uint8_t *d_in, size_t n, uint8_t **out,
-                                      size_t *out_len) {
+template <typename F>
+int guarded(F f) {
   try {
-    BZ_REQUIRE(out && out_len && (n == 0 || d_in), kErrArg, "bad arguments");
-    std::vector<uint8_t> v;
-    decode_stream(d_in, n, v, 0);
-    uint8_t *p = (uint8_t *)std::malloc(std::max<size_t>(v.size(), 1));
-    BZ_REQUIRE(p != nullptr, kErrAlloc, "host allocation failed");
-    if (!v.empty()) std::memcpy(p, v.data(), v.size());
-    *out = p;
-    *out_len = v.size();
+    f();
     set_last_error("");
     return BZ2G_OK;
   } catch (const Error &e) {
@@ -832,19 +1068,46 @@ extern "C" int bz2g_decompress_device(const uint8_t *d_in, size_t n, uint8_t **o
   }
 }
 
-extern "C" int bz2g_decompress(const uint8_t *in, size_t n, uint8_t **out, size_t *out_len) {
-  try {
+int decompress_malloc(const uint8_t *in, size_t n, uint8_t **out, size_t *out_len) {
+  return guarded([&] {
     BZ_REQUIRE(out && out_len && (n == 0 || in), kErrArg, "bad arguments");
-    uint8_t *d = nullptr;
-    BZ_CUDA(cudaMalloc((void **)&d, std::max<size_t>(n, 1)));
-    struct F {
-      uint8_t *p;
-      ~F() { cudaFree(p); }
-    } f{d};
-    if (n) BZ_CUDA(cudaMemcpy(d, in, n, cudaMemcpyHostToDevice));
-    return bz2g_decompress_device(d, n, out, out_len);
-  } catch (const Error &e) {
-    set_last_error(e.what());
-    return e.code;
-  }
+    MallocSink sink;
+    decode_into_sink(in, n, sink);
+    *out_len = sink.size;
+    *out = sink.release();
+  });
+}
+
+int decompress_buffer(const uint8_t *in, size_t n, uint8_t *out, size_t cap,
+                      size_t *out_len) {
+  return guarded([&] {
+    BZ_REQUIRE(out_len && (n == 0 || in) && (cap == 0 || out), kErrArg, "bad arguments");
+    BufferSink sink(out, cap);
+    decode_into_sink(in, n, sink);
+    *out_len = sink.size;
+  });
+}
+
+}  // namespace
+}  // namespace bz2g
+
+using namespace bz2g;
+
+extern "C" int bz2g_decompress(const uint8_t *in, size_t n, uint8_t **out, size_t *out_len) {
+  return decompress_malloc(in, n, out, out_len);
+}
+
+extern "C" int bz2g_decompress_device(const uint8_t *d_in, size_t n, uint8_t **out,
+                                      size_t *out_len) {
+  return decompress_malloc(d_in, n, out, out_len);
+}
+
+extern "C" int bz2g_decompress_into(const uint8_t *in, size_t n, uint8_t *out, size_t cap,
+                                    size_t *out_len) {
+  return decompress_buffer(in, n, out, cap, out_len);
+}
+
+extern "C" int bz2g_decompress_device_into(const uint8_t *d_in, size_t n, uint8_t *d_out,
+                                           size_t cap, size_t *out_len) {
+  return decompress_buffer(d_in, n, d_out, cap, out_len);
 }

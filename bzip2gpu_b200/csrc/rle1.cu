@@ -16,33 +16,12 @@
 // products is the tile's crc0; the per-block kernel shifts each tile's crc0
 // by x^(8 * bytes after the tile) (one thread per tile) and XORs them; the
 // init term ~0 * x^(8n) is added at the end.
+#include "crc.cuh"
 #include "engine.h"
 
 namespace bz2g {
 
 namespace {
-
-constexpr uint32_t kPoly = 0x04C11DB7u;
-
-constexpr uint32_t gf_mul_c(uint32_t a, uint32_t b) {
-  uint32_t r = 0;
-  for (int i = 31; i >= 0; --i) {
-    r = (r << 1) ^ ((r & 0x80000000u) ? kPoly : 0u);
-    if ((b >> i) & 1u) r ^= a;
-  }
-  return r;
-}
-constexpr uint32_t xpow8_pow2(int i) {
-  uint32_t v = 0x100u;  // x^8
-  for (int k = 0; k < i; ++k) v = gf_mul_c(v, v);
-  return v;
-}
-
-#define XP4(i) xpow8_pow2(i), xpow8_pow2(i + 1), xpow8_pow2(i + 2), xpow8_pow2(i + 3)
-// c_xpow[i] = x^(8 * 2^i) mod P
-__constant__ uint32_t c_xpow[32] = {XP4(0),  XP4(4),  XP4(8),  XP4(12),
-                                    XP4(16), XP4(20), XP4(24), XP4(28)};
-#undef XP4
 
 // c_klane.v[l] = x^(8 * 16 * (255 - l)) mod P: thread l's 16 bytes sit that
 // far before the end of a 4096-byte tile.
@@ -58,32 +37,6 @@ struct LaneShift {
   }
 };
 __constant__ LaneShift c_klane{};
-
-__device__ __forceinline__ uint32_t gf_mul(uint32_t a, uint32_t b) {
-  uint32_t r = 0;
-#pragma unroll 8
-  for (int i = 31; i >= 0; --i) {
-    r = (r << 1) ^ ((r & 0x80000000u) ? kPoly : 0u);
-    if ((b >> i) & 1u) r ^= a;
-  }
-  return r;
-}
-
-// x^(8j) mod P
-__device__ __forceinline__ uint32_t xpow8(uint64_t j) {
-  uint32_t r = 1u;
-  for (int i = 0; j; ++i, j >>= 1)
-    if (j & 1u) r = gf_mul(r, c_xpow[i]);
-  return r;
-}
-
-__device__ __forceinline__ void crc_table_fill(uint32_t *tbl) {
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) {
-    uint32_t c = (uint32_t)i << 24;
-    for (int k = 0; k < 8; k++) c = (c & 0x80000000u) ? (c << 1) ^ kPoly : (c << 1);
-    tbl[i] = c;
-  }
-}
 
 // Stage one raw tile into shared memory: sb[0..len) = bytes, *prev = byte
 // before the tile (or -1 at the block start).

@@ -186,6 +186,13 @@ int bz2g_count_frequencies(const uint16_t *d_syms, int s, int32_t *d_freqs, void
  * status. */
 int bz2g_decompress(const uint8_t *in, size_t n, uint8_t **out, size_t *out_len);
 int bz2g_decompress_device(const uint8_t *d_in, size_t n, uint8_t **out, size_t *out_len);
+/* As above into a caller buffer of `cap` bytes, host (pinned or pageable) or
+ * device memory; *out_len = decoded bytes.  BZ2G_ERR_TOO_LARGE if they do not
+ * fit (the buffer then holds a prefix of the output). */
+int bz2g_decompress_into(const uint8_t *in, size_t n, uint8_t *out, size_t cap,
+                         size_t *out_len);
+int bz2g_decompress_device_into(const uint8_t *d_in, size_t n, uint8_t *d_out, size_t cap,
+                                size_t *out_len);
 
 /* ------------------------------------------------------------ file streams */
 /* A file (NULL: standard input) compressed to a .bz2 file (NULL: standard

@@ -87,3 +87,51 @@ def test_malformed_streams_are_errors(torch_cuda, how):
         s = s[:-10]
     with pytest.raises(B.Bz2gError):
         B.decompress(bytes(s))
+
+
+def test_decompress_into_buffers(torch_cuda):
+    torch = torch_cuda
+    a = W.small_markov(2000000, seed=88)
+    s = B.compress(a, 9)
+    want = a.tobytes()
+    out = np.empty(len(want), np.uint8)
+    assert B.decompress_into(s, out) == len(want) and out.tobytes() == want
+    pin = torch.empty(len(want) + 100, dtype=torch.uint8, pin_memory=True)
+    assert B.decompress_into(s, pin) == len(want) and pin[: len(want)].numpy().tobytes() == want
+    d_in = torch.from_numpy(np.frombuffer(s, np.uint8).copy()).cuda()
+    d_out = torch.empty(len(want), dtype=torch.uint8, device="cuda")
+    assert B.decompress_into(d_in, d_out) == len(want)
+    assert d_out.cpu().numpy().tobytes() == want
+    with pytest.raises(B.Bz2gError):
+        B.decompress_into(s, np.empty(len(want) - 1, np.uint8))
+    assert B.decompress(B.compress(np.zeros(0, np.uint8))) == b""
+    assert B.decompress_into(B.compress(np.zeros(0, np.uint8)), np.empty(0, np.uint8)) == 0
+
+
+def _count_equals_byte_runs(n_runs: int, seed: int) -> np.ndarray:
+    # runs of 4 + b copies of byte b: every RLE1 count byte equals the byte
+    # of its run, the case where a segment's entry state stays ambiguous
+    rng = np.random.default_rng(seed)
+    vals = rng.integers(0, 40, n_runs).astype(np.uint8)
+    return np.repeat(vals, vals.astype(np.int64) + 4)
+
+
+@pytest.mark.parametrize("batch", ["1", "3", "64"])
+def test_small_decode_batches(torch_cuda, monkeypatch, batch):
+    monkeypatch.setenv("BZ2G_DECODE_BATCH", batch)
+    a = np.concatenate([W.small_markov(150000, seed=89), _count_equals_byte_runs(3000, 90)])
+    s = B.compress(a, 3, 7000)  # 33 blocks
+    assert B.decompress(s) == a.tobytes()
+    out = np.empty(a.size, np.uint8)
+    assert B.decompress_into(s, out) == a.size and np.array_equal(out, a)
+
+
+@pytest.mark.parametrize("seed", [91, 92])
+def test_rle1_segments_with_ambiguous_states(torch_cuda, seed):
+    a = _count_equals_byte_runs(60000, seed)
+    assert B.decompress(B.compress(a, 9)) == a.tobytes()
+    assert B.decompress(bz2.compress(a.tobytes(), 9)) == a.tobytes()
+    # single runs of every length around the 4-byte threshold and 259 cut
+    b = np.concatenate([np.full(L, L % 251, np.uint8) for L in range(1, 600)])
+    assert B.decompress(B.compress(b, 9)) == b.tobytes()
+    assert B.decompress(bz2.compress(b.tobytes(), 1)) == b.tobytes()
