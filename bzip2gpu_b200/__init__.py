@@ -25,8 +25,12 @@ __all__ = [
     "MAX_ALPHA", "SELECTOR_PARAMS", "selector_load", "set_selector", "get_selector",
     "selector_logits", "huffman_build_learned", "selector_dataset", "compress_part",
     "assemble", "compress_file", "decompress", "decompress_device", "decompress_into",
+    "bzip2_split", "BZIP2_BLOCKS",
 ]
 
+# block_bytes value selecting bzip2 1.0.8's block format (blocks cut by RLE1
+# length, runs cut at 255): streams byte-identical to libbz2's
+BZIP2_BLOCKS = -1
 MAX_GROUPS = 6
 MAX_ALPHA = 258
 SELECTOR_PARAMS = 139792
@@ -68,6 +72,8 @@ _SIGS = {
     "bz2g_decompress": (_i, [_vp, _sz, _c.POINTER(_u8p), _c.POINTER(_sz)]),
     "bz2g_decompress_device": (_i, [_vp, _sz, _c.POINTER(_u8p), _c.POINTER(_sz)]),
     "bz2g_decompress_into": (_i, [_vp, _sz, _vp, _sz, _c.POINTER(_sz)]),
+    "bz2g_bzip2_split": (_i, [_vp, _sz, _i, _vp, _sz, _c.POINTER(_sz), _vp]),
+    "bz2g_bzip2_split_bound": (_sz, [_sz, _i]),
     "bz2g_decompress_device_into": (_i, [_vp, _sz, _vp, _sz, _c.POINTER(_sz)]),
     "bz2g_part_bound": (_sz, [_sz, _i]),
     "bz2g_compress_part": (_i, [_vp, _sz, _i, _i, _vp, _sz, _c.POINTER(_c.c_int64),
@@ -256,6 +262,17 @@ def decompress_device(d_in) -> bytes:
     _check(lib().bz2g_decompress_device(_ptr(d_in), d_in.numel(), ctypes.byref(out),
                                         ctypes.byref(ln)))
     return _take(out, ln.value)
+
+
+def bzip2_split(d_in, level: int = 9) -> np.ndarray:
+    """Block end offsets of bzip2 1.0.8's split of a CUDA uint8 tensor."""
+    n = d_in.numel()
+    cap = lib().bz2g_bzip2_split_bound(n, level)
+    ends = np.zeros(max(cap, 1), np.int64)
+    cnt = _sz()
+    _check(lib().bz2g_bzip2_split(_ptr(d_in) if n else None, n, level, ends.ctypes.data, cap,
+                                  ctypes.byref(cnt), _stream(None)))
+    return ends[: cnt.value].copy()
 
 
 def decompress_into(data, out) -> int:

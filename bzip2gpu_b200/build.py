@@ -30,7 +30,8 @@ NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler"
            "--expt-relaxed-constexpr", f"-I{INC}", f"-I{CSRC}"] + ARCH
 
 LIB_SOURCES = ["engine.cu", "rle1.cu", "bwt.cu", "mtf.cu", "rle2.cu", "huffman.cu", "pack.cu",
-               "compressor.cu", "capi.cu", "compat.cu", "gen.cu", "noalloc.cu", "mlp.cu", "stream.cu", "decode.cu"]
+               "compressor.cu", "capi.cu", "compat.cu", "gen.cu", "noalloc.cu", "mlp.cu", "stream.cu", "decode.cu",
+               "split.cu"]
 CLI_SOURCES = ["cli_main.cpp"]
 
 

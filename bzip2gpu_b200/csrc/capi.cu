@@ -15,6 +15,7 @@
 #include "compressor.h"
 #include "engine.h"
 #include "selector.h"
+#include "split.h"
 #include "stream.h"
 #include "../../include/io.h"
 
@@ -162,23 +163,68 @@ Compressor &engine_for(int64_t block_bytes) {
   return ref;
 }
 
+// Per-call settings of an engine: timing, selector, and the block format
+// (run cut 259 and raw-size blocks, or 255 and RLE1 bytes capped at m_cap).
+void set_format(Compressor &c, int run_cut = 259, int64_t m_cap = 0) {
+  auto &cfg = const_cast<CompressorConfig &>(c.config());
+  cfg.time_stages = g_timing;
+  cfg.selector = current_selector();
+  cfg.plain_passes = current_passes();
+  cfg.run_cut = run_cut;
+  cfg.m_cap = m_cap;
+}
+
 }  // namespace
 
 Compressor &default_engine(int64_t max_block_bytes) {
   Compressor &c = engine_for(std::max<int64_t>(max_block_bytes, 1));
-  const_cast<CompressorConfig &>(c.config()).time_stages = g_timing;
-  const_cast<CompressorConfig &>(c.config()).selector = current_selector();
-  const_cast<CompressorConfig &>(c.config()).plain_passes = current_passes();
+  set_format(c);
   return c;
 }
 
 namespace {
 
+// bzip2 1.0.8's blocks: the split runs on the device copy of the input.
+void compress_bzip2(const uint8_t *in, size_t n, int level, bool on_device, ByteSink &out) {
+  level = std::min(std::max(level, 1), 9);
+  cudaStream_t st = nullptr;
+  BZ_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  uint8_t *staged = nullptr;
+  struct Cleanup {
+    cudaStream_t st;
+    uint8_t **staged;
+    ~Cleanup() {
+      if (*staged) cudaFree(*staged);
+      cudaStreamDestroy(st);
+    }
+  } cleanup{st, &staged};
+  const uint8_t *d = in;
+  if (!on_device && n > 0) {
+    BZ_CUDA(cudaMalloc((void **)&staged, n));
+    BZ_CUDA(cudaMemcpyAsync(staged, in, n, cudaMemcpyHostToDevice, st));
+    d = staged;
+  }
+  const std::vector<int64_t> ends = bzip2_split(d, (int64_t)n, level, st);
+  std::vector<const uint8_t *> ptrs(ends.size());
+  std::vector<int> lens(ends.size());
+  int64_t at = 0;
+  for (size_t b = 0; b < ends.size(); b++) {
+    ptrs[b] = d + at;
+    lens[b] = (int)(ends[b] - at);
+    at = ends[b];
+  }
+  Compressor &c = engine_for(900000);
+  set_format(c, 255, 100000LL * level);
+  g_last_stats = StageTimes();
+  c.compress_device(ptrs.data(), lens.data(), (int)ptrs.size(), level, out, &g_last_stats);
+}
+
 void compress_any(const uint8_t *in, size_t n, int level, int block_bytes, bool on_device,
                   ByteSink &out) {
-  BZ_REQUIRE(block_bytes > 0 && block_bytes <= (1 << 24), kErrArg,
-             "block_bytes must be in (0, 16 MiB]");
   BZ_REQUIRE(n == 0 || in != nullptr, kErrArg, "null input");
+  if (block_bytes == BZ2G_BZIP2_BLOCKS) return compress_bzip2(in, n, level, on_device, out);
+  BZ_REQUIRE(block_bytes > 0 && block_bytes <= (1 << 24), kErrArg,
+             "block_bytes must be in (0, 16 MiB], or BZ2G_BZIP2_BLOCKS");
   const int64_t nb = ((int64_t)n + block_bytes - 1) / block_bytes;
   std::vector<const uint8_t *> ptrs(nb);
   std::vector<int> lens(nb);
@@ -187,9 +233,7 @@ void compress_any(const uint8_t *in, size_t n, int level, int block_bytes, bool 
     lens[b] = (int)std::min<int64_t>(block_bytes, (int64_t)n - b * (int64_t)block_bytes);
   }
   Compressor &c = engine_for(std::max<int64_t>(block_bytes, 1));
-  const_cast<CompressorConfig &>(c.config()).time_stages = g_timing;
-  const_cast<CompressorConfig &>(c.config()).selector = current_selector();
-  const_cast<CompressorConfig &>(c.config()).plain_passes = current_passes();
+  set_format(c, 259, 0);
   g_last_stats = StageTimes();
   if (on_device)
     c.compress_device(ptrs.data(), lens.data(), (int)nb, level, out, &g_last_stats);
@@ -214,6 +258,8 @@ int bz2g_version(void) { return 1; }
 size_t bz2g_rle1_bound(size_t n) { return (size_t)rle1_bound((int64_t)n); }
 
 size_t bz2g_compress_bound(size_t n, int block_bytes) {
+  if (block_bytes == BZ2G_BZIP2_BLOCKS)
+    return stream_bound((int64_t)n, bzip2_split_max_blocks((int64_t)n, 1));
   if (block_bytes <= 0) block_bytes = 900000;
   size_t nb = (n + block_bytes - 1) / block_bytes;
   return stream_bound((int64_t)n, (int64_t)nb);
@@ -272,6 +318,20 @@ int bz2g_compress_device_into(const uint8_t *d_in, size_t n, int level, int bloc
 
 void bz2g_free(void *p) { std::free(p); }
 
+int bz2g_bzip2_split(const uint8_t *d_in, size_t n, int level, int64_t *ends, size_t cap,
+                     size_t *count, void *stream) {
+  return guard([&] {
+    BZ_REQUIRE(count && (n == 0 || d_in) && (cap == 0 || ends), kErrArg, "bad arguments");
+    const std::vector<int64_t> e = bzip2_split(d_in, (int64_t)n, level, S(stream));
+    *count = e.size();
+    std::memcpy(ends, e.data(), sizeof(int64_t) * std::min(cap, e.size()));
+  });
+}
+
+size_t bz2g_bzip2_split_bound(size_t n, int level) {
+  return (size_t)bzip2_split_max_blocks((int64_t)n, std::min(std::max(level, 1), 9));
+}
+
 size_t bz2g_compress_batch_bound(int count, const size_t *sizes, const int *levels,
                                  const int *block_bytes) {
   size_t tot = 0;
@@ -303,9 +363,7 @@ int bz2g_compress_batch(int count, const uint8_t *const *inputs, const size_t *s
     ByteSink sink(out, cap);
     std::vector<size_t> offs;
     g_last_stats = StageTimes();
-    const_cast<CompressorConfig &>(c.config()).time_stages = g_timing;
-    const_cast<CompressorConfig &>(c.config()).selector = current_selector();
-  const_cast<CompressorConfig &>(c.config()).plain_passes = current_passes();
+    set_format(c);
     c.compress_batch(items.data(), count, on_device != 0, sink, offs, &g_last_stats);
     for (int i = 0; i <= count; i++) offsets[i] = offs[i];
   });
@@ -840,9 +898,7 @@ int bz2g_compress_part(const uint8_t *in, size_t n, int block_bytes, int on_devi
     ByteSink sink(d_part, cap);
     BZ_REQUIRE(sink.device, kErrArg, "the part buffer must be device memory");
     Compressor &c = engine_for(std::max<int64_t>(block_bytes, 1));
-    const_cast<CompressorConfig &>(c.config()).time_stages = g_timing;
-    const_cast<CompressorConfig &>(c.config()).selector = current_selector();
-    const_cast<CompressorConfig &>(c.config()).plain_passes = current_passes();
+    set_format(c);
     g_last_stats = StageTimes();
     int64_t b = 0;
     uint32_t f = 0;

@@ -214,9 +214,13 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
                      bool on_device, ByteSink &out, StageTimes *times, bool part,
                      int64_t *part_bits, uint32_t *part_crc) {
   std::lock_guard<std::mutex> call_lock(call_mu_);
+  const Workspace &ws0 = *workers_[0]->ws;
+  const int64_t raw_max = cfg_.m_cap > 0 ? ws0.max_raw : cfg_.max_block_bytes;
+  BZ_REQUIRE(cfg_.m_cap <= rle1_bound(cfg_.max_block_bytes), kErrArg,
+             "RLE1 cap above the workspace's block size");
   int64_t ntot = 0;
   for (int b = 0; b < nblocks; b++) {
-    BZ_REQUIRE(lens[b] > 0 && lens[b] <= cfg_.max_block_bytes, kErrArg,
+    BZ_REQUIRE(lens[b] > 0 && lens[b] <= raw_max, kErrArg,
                "block length outside (0, max_block_bytes]");
     ntot += lens[b];
   }
@@ -235,7 +239,34 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
     out.size = base + 4;
   }
   const int B = cfg_.slab_blocks;
-  const int nslabs = (nblocks + B - 1) / B;
+  // slabs: up to B blocks, fewer where long blocks would overflow a workspace
+  std::vector<int> slab_at{0};
+  {
+    int64_t raw = 0, elems = 0;
+    int rt = 0, tiles = 0, gt = 0, cnt = 0;
+    for (int b = 0; b < nblocks; b++) {
+      const BlockNeeds q = block_needs(lens[b], cfg_.m_cap);
+      BZ_REQUIRE(q.raw <= ws0.max_raw && q.raw_tiles <= ws0.max_raw_tiles &&
+                     q.elems <= ws0.max_elems && q.tiles <= ws0.max_tiles &&
+                     q.group_tiles <= ws0.max_group_tiles,
+                 kErrArg, "block larger than a slab");
+      if (cnt == B || raw + q.raw > ws0.max_raw || rt + q.raw_tiles > ws0.max_raw_tiles ||
+          elems + q.elems > ws0.max_elems || tiles + q.tiles > ws0.max_tiles ||
+          gt + q.group_tiles > ws0.max_group_tiles) {
+        slab_at.push_back(b);
+        raw = elems = 0;
+        rt = tiles = gt = cnt = 0;
+      }
+      raw += q.raw;
+      elems += q.elems;
+      rt += q.raw_tiles;
+      tiles += q.tiles;
+      gt += q.group_tiles;
+      cnt++;
+    }
+    if (nblocks > 0) slab_at.push_back(nblocks);
+  }
+  const int nslabs = (int)slab_at.size() - 1;
 
   std::mutex mu;
   std::condition_variable cv;
@@ -256,8 +287,8 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
       }
       const int k = next_slab.fetch_add(1);
       if (k >= nslabs) return;
-      const int b0 = k * B, nb = std::min(B, nblocks - b0);
-      plan.build(lens + b0, nb);
+      const int b0 = slab_at[k], nb = slab_at[k + 1] - b0;
+      plan.build(lens + b0, nb, cfg_.run_cut, cfg_.m_cap);
       w.ws->upload_plan(plan, w.st);
       const SlabDev &d = w.ws->dev;
       // raw bytes: one copy when the blocks are back to back and 16-aligned

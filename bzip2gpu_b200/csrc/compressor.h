@@ -46,6 +46,12 @@ struct CompressorConfig {
   // Training-set tap: every block with six tables appends its groups and the
   // plain selector's choices (deterministic order with one worker).
   const mlp::SelectorTap *tap = nullptr;
+  // Block format of compress / compress_device.  Reference: runs cut at 259
+  // and blocks of at most max_block_bytes raw bytes.  bzip2 1.0.8: runs cut
+  // at 255 and blocks of any raw length whose RLE1 output is at most m_cap
+  // bytes (the bzip2 split; slabs take fewer blocks when they are long).
+  int run_cut = 259;
+  int64_t m_cap = 0;
 };
 
 // Destination of a stream: a malloc'd buffer that this library grows (and

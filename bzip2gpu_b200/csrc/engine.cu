@@ -19,13 +19,30 @@ int64_t launch_count() { return g_launches.load(); }
   throw Error(kErrCuda, os.str());
 }
 
-static int64_t groups_bound(int64_t raw_len) {
-  // symbols <= RLE1 bytes + 1 (EOB), 50 symbols per group
-  return (rle1_bound(raw_len) + 1 + kGroupSize - 1) / kGroupSize;
+static int64_t m_bound(int64_t raw_len, int64_t m_cap) {
+  const int64_t b = rle1_bound(raw_len);
+  return m_cap > 0 ? std::min(b, m_cap) : b;
 }
 
-void SlabPlan::build(const int *lens, int n) {
+static int64_t groups_bound(int64_t raw_len, int64_t m_cap = 0) {
+  // symbols <= RLE1 bytes + 1 (EOB), 50 symbols per group
+  return (m_bound(raw_len, m_cap) + 1 + kGroupSize - 1) / kGroupSize;
+}
+
+BlockNeeds block_needs(int64_t L, int64_t m_cap) {
+  BlockNeeds r;
+  r.raw = align_up(L, 16);
+  r.raw_tiles = (int)((L + kRawTile - 1) / kRawTile);
+  r.elems = align_up(std::max<int64_t>(m_bound(L, m_cap), 1), kTile);
+  r.tiles = (int)(r.elems / kTile);
+  r.group_tiles = (int)((groups_bound(L, m_cap) + kGroupTile - 1) / kGroupTile);
+  return r;
+}
+
+void SlabPlan::build(const int *lens, int n, int cut, int64_t mcap) {
   nblocks = n;
+  run_cut = cut;
+  m_cap = mcap;
   raw_off.assign(n, 0);
   off.assign(n, 0);
   cap.assign(n, 0);
@@ -49,18 +66,18 @@ void SlabPlan::build(const int *lens, int n) {
       rt_block.push_back(b);
       rt_start.push_back((int)st);
     }
-    const int64_t c = align_up(std::max<int64_t>(rle1_bound(L), 1), kTile);
+    const int64_t c = align_up(std::max<int64_t>(m_bound(L, m_cap), 1), kTile);
     off[b] = elem_total;
     cap[b] = c;
     for (int64_t k = 0; k < c / kTile; k++) tile_block.push_back(b);
     elem_total += c;
     gt_begin[b] = (int)gt_block.size();
-    const int64_t G = groups_bound(L);
+    const int64_t G = groups_bound(L, m_cap);
     for (int64_t g = 0; g < G; g += kGroupTile) {
       gt_block.push_back(b);
       gt_first.push_back((int)g);
     }
-    max_m_bound = std::max<int>(max_m_bound, (int)rle1_bound(L));
+    max_m_bound = std::max<int>(max_m_bound, (int)m_bound(L, m_cap));
   }
   rt_first[n] = (int)rt_block.size();
   gt_begin[n] = (int)gt_block.size();
@@ -189,6 +206,7 @@ void Workspace::upload_plan(const SlabPlan &p, cudaStream_t st) {
   BZ_REQUIRE(pos <= pinned_plan_bytes, kErrInternal, "plan staging overflow");
   BZ_CUDA(cudaMemcpyAsync(plan_dev_, pinned_plan, pos, cudaMemcpyHostToDevice, st));
   dev.nblocks = n;
+  dev.run_cut = p.run_cut;
   dev.ntiles = (int)p.tile_block.size();
   dev.n_raw_tiles = (int)p.rt_block.size();
   dev.n_group_tiles = (int)p.gt_block.size();

@@ -24,8 +24,19 @@
 namespace bz2g {
 
 // Per-slab plan, built on the host from the raw block lengths.
+// Workspace a block of L raw bytes takes in a slab.  m_cap > 0 bounds its
+// RLE1 bytes (the bzip2 split's blocks: many raw bytes, bounded RLE1 output).
+struct BlockNeeds {
+  int64_t raw, elems;
+  int raw_tiles, tiles, group_tiles;
+};
+BlockNeeds block_needs(int64_t L, int64_t m_cap);
+
 struct SlabPlan {
   int nblocks = 0;
+  // RLE1 run cut: 259 (the reference: 4 + 255) or 255 (bzip2 1.0.8)
+  int run_cut = 259;
+  int64_t m_cap = 0;
   std::vector<int64_t> raw_off, off, cap;
   std::vector<int> raw_len;
   std::vector<int> rt_block, rt_start, rt_first;  // raw tiles (rt_first: nblocks+1)
@@ -34,7 +45,7 @@ struct SlabPlan {
   std::vector<int> gt_begin;            // first group tile of each block (nblocks+1)
   int64_t raw_total = 0, elem_total = 0;
   int max_m_bound = 0;
-  void build(const int *lens, int n);
+  void build(const int *lens, int n, int run_cut = 259, int64_t m_cap = 0);
 };
 
 constexpr int kGroupTile = 128;  // 50-symbol groups per group tile
@@ -42,6 +53,7 @@ constexpr int kGroupTile = 128;  // 50-symbol groups per group tile
 // Device pointers of one slab, passed to kernels by value.
 struct SlabDev {
   int nblocks, ntiles, n_raw_tiles, n_group_tiles;
+  int run_cut;  // RLE1 run cut (259 or 255)
   // plan
   const int64_t *raw_off, *off, *cap;
   const int *raw_len, *rt_block, *rt_start, *rt_first, *tile_block, *gt_block, *gt_first, *gt_begin;

@@ -107,6 +107,7 @@ extern "C" int bz2g_rle1_noalloc(const uint8_t *d_in, int n, uint8_t *d_out, int
     SlabDev d;
     std::memset(&d, 0, sizeof(d));
     d.nblocks = 1;
+    d.run_cut = 259;
     d.n_raw_tiles = (n + kRawTile - 1) / kRawTile;
     d.raw = base + kOffRaw;
     d.raw_off = reinterpret_cast<const int64_t *>(base + kOffPlan64);

@@ -1,11 +1,12 @@
-// RLE1 (runs cut at 259) and the block CRC-32, over every block of a slab.
+// RLE1 (runs cut at C = 259, or 255 for bzip2 1.0.8's format) and the block
+// CRC-32, over every block of a slab.
 //
 // Reference: src/compression/rle1.cu:13-113 (RLE1), src/compression/crc32.cpp
-// (CRC).  A maximal run of length L is emitted as floor(L/259) chunks
-// "cccc 255" followed by the remainder r = L mod 259: r < 4 copies of c, or
+// (CRC).  A maximal run of length L is emitted as floor(L/C) chunks
+// "cccc (C-4)" followed by the remainder r = L mod C: r < 4 copies of c, or
 // "cccc (r-4)".  Position j of a run (j = i - run_start) emits
-//   1 byte (c)            if j mod 259 < 3,
-//   2 bytes (c, len-4)    if j mod 259 == 3,  len = length of its 259-chunk,
+//   1 byte (c)            if j mod C < 3,
+//   2 bytes (c, len-4)    if j mod C == 3,  len = length of its C-chunk,
 //   nothing               otherwise,
 // so every output offset is an exclusive scan of a per-position count, and the
 // run start / end of a position are a max-scan / min-scan of run-start flags.
@@ -195,8 +196,8 @@ __global__ void __launch_bounds__(256) k_rle1_block_carry(SlabDev d, const int *
   }
 }
 
-__device__ __forceinline__ int rle1_count_of(int j) {
-  int q = j % 259;
+__device__ __forceinline__ int rle1_count_of(int j, int cut) {
+  int q = j % cut;
   return q < 3 ? 1 : (q == 3 ? 2 : 0);
 }
 
@@ -223,7 +224,7 @@ __global__ void __launch_bounds__(256) k_rle1_count(SlabDev d) {
   int cnt = 0;
   for (int k = 0; k < nv; k++) {
     if ((sm >> k) & 1u) cur = st + p0 + k;
-    cnt += rle1_count_of(st + p0 + k - cur);
+    cnt += rle1_count_of(st + p0 + k - cur, d.run_cut);
   }
   int total;
   block_excl_sum(cnt, scratch, &total);
@@ -292,24 +293,25 @@ __global__ void __launch_bounds__(256) k_rle1_write(SlabDev d) {
     int cur = before;
     for (int k = 0; k < nv; k++) {
       if ((sm >> k) & 1u) cur = st + p0 + k;
-      cnt += rle1_count_of(st + p0 + k - cur);
+      cnt += rle1_count_of(st + p0 + k - cur, d.run_cut);
     }
   }
   int tot;
   int o = block_excl_sum(cnt, scratch, &tot);
   uint8_t *out = so + o;
+  const int cut = d.run_cut;
   int cur = before;
 #pragma unroll
   for (int k = 0; k < kTileItems; k++) {
     if (k < nv) {
       if ((sm >> k) & 1u) cur = st + p0 + k;
       int j = st + p0 + k - cur;
-      int q = j % 259;
+      int q = j % cut;
       if (q < 3) {
         *out++ = c[k];
       } else if (q == 3) {
         int run_len = ends[k] - cur;
-        int chunk_len = min(259, run_len - (j / 259) * 259);
+        int chunk_len = min(cut, run_len - (j / cut) * cut);
         *out++ = c[k];
         *out++ = (uint8_t)(chunk_len - 4);
       }

@@ -37,9 +37,28 @@ int bz2g_version(void);
 
 /* ----------------------------------------------------------- whole stream */
 
+/* block_bytes value selecting bzip2 1.0.8's block format instead of the
+ * reference's: runs cut at 255 (not 259) and blocks cut where their RLE1
+ * output reaches 100000 * level - 19 bytes, as libbz2 cuts them.  The stream
+ * is then byte-identical to libbz2's at the same level, except that a block
+ * whose RLE1 output is periodic (equal rotations) may carry another origPtr
+ * among the equal rotations, which decodes the same.  No counterpart in the
+ * reference, whose TODO.md:38-40 lists the split as missing and which cuts
+ * 900000 raw bytes for every level, src/main.cpp:26,36. */
+#define BZ2G_BZIP2_BLOCKS (-1)
+
+/* The block ends (raw offsets, ascending, the last one n) of bzip2 1.0.8's
+ * split of n device bytes at `level`: *count blocks, the first min(count, cap)
+ * ends stored in host array ends.  bz2g_bzip2_split_bound gives a sufficient
+ * cap.  stream: a cudaStream_t (NULL: the legacy default stream). */
+int bz2g_bzip2_split(const uint8_t *d_in, size_t n, int level, int64_t *ends, size_t cap,
+                     size_t *count, void *stream);
+size_t bz2g_bzip2_split_bound(size_t n, int level);
+
 /* Compress n host bytes into a complete .bz2 stream: header "BZh" + level
  * digit, one block per block_bytes raw bytes (the reference always splits at
- * its input buffer size, 900000), end-of-stream marker and combined CRC.
+ * its input buffer size, 900000) or bzip2's blocks (BZ2G_BZIP2_BLOCKS),
+ * end-of-stream marker and combined CRC.
  * *out is allocated here (release with bz2g_free).  Empty input gives the
  * 14-byte empty stream.
  * Replaces: bzip2_gpu_compress(BZFileInputStream&, int n, std::vector<uint8_t>&)

@@ -74,6 +74,9 @@ def lib():
                                         ctypes.POINTER(ctypes.c_uint32)]
         L.orc_assemble.restype = ctypes.c_int64
         L.orc_assemble.argtypes = [_i, _vp, _vp, _vp, _vp, _i, _vp, ctypes.c_int64]
+        L.orc_rle1_cut.argtypes = [_vp, _i, _vp, _i]
+        L.orc_bzip2_split.restype = ctypes.c_int64
+        L.orc_bzip2_split.argtypes = [_vp, ctypes.c_int64, _i, _vp, ctypes.c_int64]
         L.orc_compress_bound.restype = ctypes.c_int64
         L.orc_compress_bound.argtypes = [ctypes.c_int64, _i]
         _lib = L
@@ -244,6 +247,26 @@ def compress_block(raw):
     return {"rle1": r1[:m].copy(), "sa": sa[:m].copy(), "mtf": mt[:m].copy(),
             "rle2": r2[:s].copy(), "sel": sel[: info.n_selectors].copy(),
             "len": np.array(info.len, np.uint8), "code": np.array(info.code, np.int32)}, info
+
+
+BZIP2_BLOCKS = -1  # block_bytes value: bzip2 1.0.8's blocks and 255-byte runs
+
+
+def rle1_cut(data, cut: int) -> np.ndarray:
+    a = _u8(data)
+    out = np.zeros(a.size + a.size // 4 + 8, np.uint8)
+    m = lib().orc_rle1_cut(a.ctypes.data if a.size else None, a.size, out.ctypes.data, cut)
+    return out[:m].copy()
+
+
+def bzip2_split(data, level: int = 9) -> np.ndarray:
+    """Block end offsets of bzip2 1.0.8's split of data at `level`."""
+    a = _u8(data)
+    p = a.ctypes.data if a.size else None
+    nb = lib().orc_bzip2_split(p, a.size, level, None, 0)
+    ends = np.zeros(max(nb, 1), np.int64)
+    lib().orc_bzip2_split(p, a.size, level, ends.ctypes.data, nb)
+    return ends[:nb]
 
 
 def compress(data, level: int = 9, block_bytes: int = 900000, threads: int = 1) -> bytes:

@@ -34,12 +34,16 @@ uint32_t orc_crc32(const uint8_t *data, size_t n) {
 /* Runs are cut greedily at 259 = 4 + 255 (tests/compression/rle1.cu:15), a cut
  * of length < 4 is copied, otherwise 4 copies + (len - 4)
  * (src/compression/rle1.cu:34-57). */
-int orc_rle1(const uint8_t *in, int n, uint8_t *out) {
+int orc_rle1(const uint8_t *in, int n, uint8_t *out) { return orc_rle1_cut(in, n, out, 259); }
+
+/* The same with runs cut at `cut` (bzip2 1.0.8 cuts at 255: its pending run
+ * is written when it reaches 255, bzlib.c ADD_CHAR_TO_BLOCK). */
+int orc_rle1_cut(const uint8_t *in, int n, uint8_t *out, int cut) {
   int o = 0, i = 0;
   while (i < n) {
     uint8_t c = in[i];
     int j = i + 1;
-    while (j < n && in[j] == c && j - i < 259) j++;
+    while (j < n && in[j] == c && j - i < cut) j++;
     int run = j - i;
     if (run < 4) {
       for (int k = 0; k < run; k++) out[o++] = c;
@@ -554,14 +558,14 @@ typedef struct {
   uint32_t *payload;
 } blk_out;
 
-int orc_compress_block(const uint8_t *raw, int n, orc_block_info *info,
-                       uint8_t *rle1_out, int32_t *sa_out, uint8_t *mtf_out,
-                       uint16_t *rle2_out, uint8_t *sel_out) {
+static int compress_block_cut(const uint8_t *raw, int n, int cut, orc_block_info *info,
+                              uint8_t *rle1_out, int32_t *sa_out, uint8_t *mtf_out,
+                              uint16_t *rle2_out, uint8_t *sel_out) {
   memset(info, 0, sizeof(*info));
   info->n = n;
   info->crc = orc_crc32(raw, (size_t)n);
   uint8_t *rle1 = rle1_out ? rle1_out : (uint8_t *)malloc((size_t)n + n / 4 + 8);
-  int m = orc_rle1(raw, n, rle1);
+  int m = orc_rle1_cut(raw, n, rle1, cut);
   info->m = m;
   int32_t *sa = sa_out ? sa_out : (int32_t *)malloc(sizeof(int32_t) * (m > 0 ? m : 1));
   int rounds = 0;
@@ -585,14 +589,20 @@ int orc_compress_block(const uint8_t *raw, int n, orc_block_info *info,
   return 0;
 }
 
+int orc_compress_block(const uint8_t *raw, int n, orc_block_info *info,
+                       uint8_t *rle1_out, int32_t *sa_out, uint8_t *mtf_out,
+                       uint16_t *rle2_out, uint8_t *sel_out) {
+  return compress_block_cut(raw, n, 259, info, rle1_out, sa_out, mtf_out, rle2_out, sel_out);
+}
+
 /* Whole block, keeping what the container needs. */
-static void run_block(const uint8_t *raw, int n, blk_out *o) {
+static void run_block(const uint8_t *raw, int n, int cut, blk_out *o) {
   uint8_t *rle1 = (uint8_t *)malloc((size_t)n + n / 4 + 8);
   int32_t *sa = (int32_t *)malloc(sizeof(int32_t) * ((size_t)n + n / 4 + 8));
   uint8_t *mtf = (uint8_t *)malloc((size_t)n + n / 4 + 8);
   uint16_t *rle2 = (uint16_t *)malloc(sizeof(uint16_t) * ((size_t)n + n / 4 + 8));
   uint8_t *sel = (uint8_t *)malloc((size_t)n / 40 + 64);
-  orc_compress_block(raw, n, &o->info, rle1, sa, mtf, rle2, sel);
+  compress_block_cut(raw, n, cut, &o->info, rle1, sa, mtf, rle2, sel);
   o->sel_mtf = (uint8_t *)malloc((size_t)o->info.n_selectors + 1);
   orc_selector_mtf(sel, o->info.n_selectors, o->info.n_groups, o->sel_mtf);
   size_t nw = (size_t)(o->info.payload_bits + 31) / 32 + 1;
@@ -604,8 +614,8 @@ static void run_block(const uint8_t *raw, int n, blk_out *o) {
 
 typedef struct {
   const uint8_t *in;
-  int64_t n;
-  int block_bytes;
+  const int64_t *ends;  /* block b = [ends[b-1], ends[b]) */
+  int cut;
   int nblocks;
   blk_out *blocks;
   int next;
@@ -619,14 +629,56 @@ static void *pool_worker(void *arg) {
     int b = c->next++;
     pthread_mutex_unlock(&c->mu);
     if (b >= c->nblocks) return NULL;
-    int64_t off = (int64_t)b * c->block_bytes;
-    int64_t len = c->n - off < c->block_bytes ? c->n - off : c->block_bytes;
-    run_block(c->in + off, (int)len, &c->blocks[b]);
+    int64_t off = b ? c->ends[b - 1] : 0;
+    run_block(c->in + off, (int)(c->ends[b] - off), c->cut, &c->blocks[b]);
   }
 }
 
+/* bzip2 1.0.8's block split (bzlib.c: ADD_CHAR_TO_BLOCK, add_pair_to_block,
+ * copy_input_until_stop, handle_compress), restated as the state machine it
+ * runs over the input: a pending run of at most 255 equal bytes is written
+ * (L bytes for L <= 3, else 4 + a count byte) when a different byte arrives or
+ * it is 255 long; before each byte, a block holding 100000 * level - 19 or
+ * more written bytes is closed without the pending run, which begins the next
+ * block; the last block takes what is left.  ends[k] = end of block k.
+ * Returns the number of blocks (ends[] needs that many entries; entries past
+ * cap are not stored). */
+int64_t orc_bzip2_split(const uint8_t *in, int64_t n, int level, int64_t *ends,
+                        int64_t cap) {
+  if (level < 1) level = 1;
+  if (level > 9) level = 9;
+  const int64_t max_written = 100000LL * level - 19;
+  int64_t nb = 0, written = 0;
+  int ch = -1, len = 0;
+  for (int64_t i = 0; i < n; i++) {
+    if (written >= max_written) {
+      if (nb < cap) ends[nb] = i - len;
+      nb++;
+      written = 0;
+    }
+    if (in[i] == ch && len < 255) {
+      len++;
+    } else {
+      if (ch >= 0) written += len < 4 ? len : 5;
+      ch = in[i];
+      len = 1;
+    }
+  }
+  if (n > 0) {
+    if (nb < cap) ends[nb] = n;
+    nb++;
+  }
+  return nb;
+}
+
+static int64_t split_bound(int64_t n) {
+  /* blocks hold >= 99981 RLE1 bytes (level 1) and RLE1 writes <= 5 per 4 */
+  return n * 5 / 4 / 99981 + 2;
+}
+
 int64_t orc_compress_bound(int64_t n, int block_bytes) {
-  int64_t nb = (n + block_bytes - 1) / block_bytes;
+  int64_t nb = block_bytes == ORC_BZIP2_BLOCKS ? split_bound(n)
+                                               : (n + block_bytes - 1) / block_bytes;
   /* per block: header <= 1300 bytes; payload <= 17 bits per symbol, and
    * symbols <= 5/4 raw bytes + 2 */
   return 64 + nb * 1400 + (n / 4 + 4 * nb) * 17 / 8 + n * 17 / 8;
@@ -640,15 +692,29 @@ static int64_t compress_impl(const uint8_t *in, int64_t n, int level, int block_
                              int64_t *part_bits, uint32_t *part_fold) {
   if (level < 1) level = 1;
   if (level > 9) level = 9;
-  if (block_bytes <= 0) block_bytes = 900000;
+  int cut = 259;
+  int64_t *ends;
+  int nblocks;
+  if (block_bytes == ORC_BZIP2_BLOCKS) {
+    cut = 255;
+    int64_t nb = orc_bzip2_split(in, n, level, NULL, 0);
+    ends = (int64_t *)malloc(sizeof(int64_t) * (nb > 0 ? nb : 1));
+    orc_bzip2_split(in, n, level, ends, nb);
+    nblocks = (int)nb;
+  } else {
+    if (block_bytes <= 0) block_bytes = 900000;
+    nblocks = (int)((n + block_bytes - 1) / block_bytes);
+    ends = (int64_t *)malloc(sizeof(int64_t) * (nblocks > 0 ? nblocks : 1));
+    for (int b = 0; b < nblocks; b++)
+      ends[b] = (int64_t)(b + 1) * block_bytes < n ? (int64_t)(b + 1) * block_bytes : n;
+  }
   bitw w = {out, cap, 0, 0, 0, 0};
   if (!part) {
     bw_put(&w, 0x42, 8); bw_put(&w, 0x5A, 8); bw_put(&w, 0x68, 8); bw_put(&w, 0x30 + level, 8);
   }
-  int nblocks = (int)((n + block_bytes - 1) / block_bytes);
   blk_out *blocks = (blk_out *)calloc(nblocks > 0 ? nblocks : 1, sizeof(blk_out));
   pool_ctx ctx;
-  ctx.in = in; ctx.n = n; ctx.block_bytes = block_bytes; ctx.nblocks = nblocks;
+  ctx.in = in; ctx.ends = ends; ctx.cut = cut; ctx.nblocks = nblocks;
   ctx.blocks = blocks; ctx.next = 0;
   pthread_mutex_init(&ctx.mu, NULL);
   if (threads < 1) threads = 1;
@@ -718,6 +784,7 @@ static int64_t compress_impl(const uint8_t *in, int64_t n, int level, int block_
     free(o->payload);
   }
   free(blocks);
+  free(ends);
   if (part) {
     *part_bits = w.pos * 8 + w.nacc;
     *part_fold = stream_crc;

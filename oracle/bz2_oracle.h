@@ -37,6 +37,18 @@ uint32_t orc_crc32(const uint8_t *data, size_t n);
 /* RLE1 with runs split at 259.  out needs n + n/4 + 4 bytes.  Returns m.
  * src/compression/rle1.cu:13-58, tests/compression/rle1.cu:8-32 */
 int orc_rle1(const uint8_t *in, int n, uint8_t *out);
+/* The same with runs split at `cut` (255: bzip2 1.0.8). */
+int orc_rle1_cut(const uint8_t *in, int n, uint8_t *out, int cut);
+
+/* block_bytes value of orc_compress / orc_compress_bound selecting bzip2
+ * 1.0.8's blocks (orc_bzip2_split) and runs split at 255.  Not a reference
+ * mode: this restatement of libbz2's split is pinned to libbz2 itself. */
+#define ORC_BZIP2_BLOCKS (-1)
+
+/* bzip2 1.0.8's block split of in[0..n) at `level`: ends[k] = end offset of
+ * block k (up to cap entries stored).  Returns the number of blocks. */
+int64_t orc_bzip2_split(const uint8_t *in, int64_t n, int level, int64_t *ends,
+                        int64_t cap);
 
 /* Sorted cyclic rotations of in[0..m), equal rotations by index ascending.
  * src/compression/fbwt.cu:47-106, tests/compression/fbwt.cu:12-24 */
@@ -139,8 +151,8 @@ int orc_compress_block(const uint8_t *raw, int n, orc_block_info *info,
                        uint8_t *rle1, int32_t *sa, uint8_t *mtf, uint16_t *rle2,
                        uint8_t *selectors);
 
-/* Whole .bz2 stream: 'BZh' + level digit, blocks of block_bytes raw bytes,
- * end-of-stream marker and combined CRC.  Empty input gives the 14-byte empty
+/* Whole .bz2 stream: 'BZh' + level digit, blocks of block_bytes raw bytes
+ * (or bzip2's blocks: ORC_BZIP2_BLOCKS), end-of-stream marker and combined CRC.  Empty input gives the 14-byte empty
  * stream.  Returns the byte length, or -1 if cap is too small.
  * src/compression/compress.cu:184-378 */
 int64_t orc_compress(const uint8_t *in, int64_t n, int level, int block_bytes,
