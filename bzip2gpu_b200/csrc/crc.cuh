@@ -34,6 +34,21 @@ __constant__ uint32_t c_xpow[32] = {BZ_XP4(0),  BZ_XP4(4),  BZ_XP4(8),  BZ_XP4(1
                                     BZ_XP4(16), BZ_XP4(20), BZ_XP4(24), BZ_XP4(28)};
 #undef BZ_XP4
 
+// c_klane.v[l] = x^(8 * 16 * (255 - l)) mod P: thread l's 16 bytes sit that
+// far before the end of a 4096-byte tile.
+struct LaneShift {
+  uint32_t v[256];
+  constexpr LaneShift() : v() {
+    uint32_t k = 1u;
+    const uint32_t step = xpow8_pow2(4);  // x^(8*16)
+    for (int l = 255; l >= 0; --l) {
+      v[l] = k;
+      k = gf_mul_c(k, step);
+    }
+  }
+};
+__constant__ LaneShift c_klane{};
+
 __device__ __forceinline__ uint32_t gf_mul(uint32_t a, uint32_t b) {
   uint32_t r = 0;
 #pragma unroll 8

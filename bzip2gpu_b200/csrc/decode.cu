@@ -19,8 +19,9 @@
 //      origPtr gives the RLE1 bytes, cut at up to 256 splitters that are
 //      walked in parallel.
 //   5. k_dec_unrle1_count / _write: per block, one warp expands the RLE1 runs
-//      (4 equal bytes then a count byte) from 32 segments at once, and the
-//      block CRC is checked against the header.
+//      (4 equal bytes then a count byte) from 32 segments at once; k_dec_crc
+//      computes each block's CRC over its output (4096-byte chunks combined
+//      over GF(2)), checked against the header.
 // Batches of blocks go through steps 2-5 while the previous batch's bytes are
 // copied out on a second stream.
 // Every field read from the stream is range-checked and every loop is bounded,
@@ -445,12 +446,17 @@ __global__ void k_dec_lf(const int32_t *idx, const DecBlock *db, const uint8_t *
 // The RLE1 bytes of each block follow tt from origPtr:
 // T[j] = psi(j) << 8 | F[j], psi = LF^-1, and the text is F[origPtr],
 // F[psi(origPtr)], ...  One dependent load per byte, so the chain is cut at
-// S splitters per block (origPtr and evenly spaced positions, marked in a
-// bitmap): every walker counts the steps to the next marked position, one
-// thread per block orders the segments along the chain from origPtr, and the
-// walkers walk again writing their segment at its offset.  A periodic block
-// (its cycle closes before m bytes) repeats that one cycle.
-constexpr int kMaxWalkers = 256;
+// S splitters per block (origPtr and evenly spaced positions, marked in bit
+// 31 of their T entry, which the walk loads anyway): every walker counts the
+// steps to the next marked position, the segments are ordered along the chain
+// from origPtr, and the walkers walk again writing their segment at its
+// offset.  Segment lengths along the chain are close to exponential, so the
+// longest is about ln(S) times the mean (m / S, about 512 here).  A periodic
+// block (its cycle closes before m bytes) repeats that one cycle.
+constexpr int kMaxWalkers = 2048;
+constexpr int kWalkSpan = 512;
+constexpr uint32_t kMark = 0x80000000u;
+constexpr uint32_t kPsiMask = 0x7FFFFF00u;
 
 struct WalkCtl {
   int32_t nw;        // splitters
@@ -461,17 +467,16 @@ struct WalkCtl {
   int32_t off[kMaxWalkers];   // output offset, -1 when off the chain
 };
 
-__global__ void k_dec_split(const int32_t *idx, const DecBlock *db, WalkCtl *ctl, uint32_t *mark,
+// Splitter positions (one thread) and their marks in T (all threads).
+__global__ void k_dec_split(const int32_t *idx, const DecBlock *db, WalkCtl *ctl, uint32_t *tt,
                             int cap) {
   const int k = blockIdx.x;
   const DecBlock b = db[idx[k]];
   WalkCtl &c = ctl[k];
-  uint32_t *M = mark + (size_t)k * ((cap + 31) / 32);
+  uint32_t *T = tt + (size_t)k * cap;
   const int m = b.m;
-  for (int i = threadIdx.x; i < (m + 31) / 32; i += blockDim.x) M[i] = 0;
-  __syncthreads();
   if (threadIdx.x == 0) {
-    const int S = max(1, min(kMaxWalkers, m / 4096));
+    const int S = max(1, min(kMaxWalkers, m / kWalkSpan));
     int n = 0;
     bool placed = false;
     for (int t = 1; t <= S; t++) {
@@ -484,7 +489,11 @@ __global__ void k_dec_split(const int32_t *idx, const DecBlock *db, WalkCtl *ctl
     }
     if (!placed) c.pos[n++] = b.orig_ptr;
     c.nw = n;
-    for (int q = 0; q < n; q++) atomicOr(&M[c.pos[q] >> 5], 1u << (c.pos[q] & 31));
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < c.nw; q += blockDim.x) {
+    const int p = c.pos[q];
+    if (p >= 0 && p < m) T[p] |= kMark;
   }
 }
 
@@ -500,53 +509,67 @@ __device__ __forceinline__ int splitter_index(const WalkCtl &c, int p) {
 
 // write == 0: segment lengths and successors; write != 0: the segment bytes.
 __global__ void k_dec_walk(const int32_t *idx, const DecBlock *db, const uint32_t *tt,
-                           WalkCtl *ctl, const uint32_t *mark, uint8_t *rle, int cap, int write) {
+                           WalkCtl *ctl, uint8_t *rle, int cap, int write) {
   const int k = blockIdx.y;
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   WalkCtl &c = ctl[k];
   if (w >= c.nw) return;
   const int m = db[idx[k]].m;
   const uint32_t *T = tt + (size_t)k * cap;
-  const uint32_t *M = mark + (size_t)k * ((cap + 31) / 32);
   uint8_t *R = rle + (size_t)idx[k] * cap;
   if (write && c.off[w] < 0) return;
   uint32_t p = (uint32_t)c.pos[w];
   int n = 0;
   const int o = write ? c.off[w] : 0;
   const int lim = write ? c.len[w] : m;
+  bool at_mark = false;
   for (;;) {
     if (p >= (uint32_t)m || n >= lim || o + n >= m) break;
     const uint32_t e = T[p];
+    if (n > 0 && (e & kMark)) {
+      at_mark = true;
+      break;
+    }
     if (write) R[o + n] = (uint8_t)(e & 0xFFu);
     n++;
-    p = e >> 8;
-    if (p < (uint32_t)m && ((M[p >> 5] >> (p & 31)) & 1u)) break;
+    p = (e & kPsiMask) >> 8;
   }
   if (!write) {
     c.len[w] = n;
-    c.next[w] = (p < (uint32_t)m) ? splitter_index(c, (int)p) : -1;
+    c.next[w] = at_mark ? splitter_index(c, (int)p) : -1;
   }
 }
 
-// Per block: segment offsets along the chain from origPtr.
-__global__ void k_dec_chain(const int32_t *idx, const DecBlock *db, WalkCtl *ctl, int nacc,
-                            int *bad) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nacc) return;
+// Per block: segment offsets along the chain from origPtr (one thread walks
+// the segments, held in shared memory).
+__global__ void __launch_bounds__(256) k_dec_chain(const int32_t *idx, const DecBlock *db,
+                                                   WalkCtl *ctl, int *bad) {
+  __shared__ int32_t len[kMaxWalkers], nxt[kMaxWalkers], off[kMaxWalkers];
+  const int k = blockIdx.x;
   const DecBlock b = db[idx[k]];
   WalkCtl &c = ctl[k];
-  for (int q = 0; q < c.nw; q++) c.off[q] = -1;
-  const int w0 = splitter_index(c, b.orig_ptr);
-  int w = w0, off = 0;
-  for (int steps = 0; steps <= c.nw; steps++) {
-    if (w < 0 || w >= c.nw || c.off[w] >= 0) break;
-    c.off[w] = off;
-    off += c.len[w];
-    if (off >= b.m) break;
-    w = c.next[w];
+  const int nw = c.nw;
+  for (int q = threadIdx.x; q < nw; q += blockDim.x) {
+    len[q] = c.len[q];
+    nxt[q] = c.next[q];
+    off[q] = -1;
   }
-  c.cycle = min(off, b.m);
-  if (c.cycle <= 0 || b.m % c.cycle != 0) atomicOr(bad, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int w0 = splitter_index(c, b.orig_ptr);
+    int w = w0, o = 0;
+    for (int steps = 0; steps <= nw; steps++) {
+      if (w < 0 || w >= nw || off[w] >= 0) break;
+      off[w] = o;
+      o += len[w];
+      if (o >= b.m) break;
+      w = nxt[w];
+    }
+    c.cycle = min(o, b.m);
+    if (c.cycle <= 0 || b.m % c.cycle != 0) atomicOr(bad, 1);
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < nw; q += blockDim.x) c.off[q] = off[q];
 }
 
 // A periodic block: the first `cycle` bytes repeated to m.
@@ -571,7 +594,8 @@ __global__ void k_dec_repeat(const int32_t *idx, const DecBlock *db, const WalkC
 // merge (typically within a few bytes: at a byte that differs from the one
 // before it), chains the lanes' state maps from state 0 across the warp and
 // keeps each lane's entry state and output offset; the write pass expands
-// every segment at its offset and combines the lanes' CRCs over GF(2).
+// every segment at its offset (runs with word stores), and k_dec_crc computes
+// the block CRCs over the output.
 constexpr int kUnrleWarps = 8;
 
 struct LaneStart {
@@ -651,13 +675,20 @@ __global__ void __launch_bounds__(32 * kUnrleWarps)
   if (ln == 0) lens[k] = off;
 }
 
+// c copies of byte v at d (word stores between unaligned ends).
+__device__ __forceinline__ void fill_bytes(uint8_t *d, int c, uint8_t v) {
+  while (c > 0 && (reinterpret_cast<uintptr_t>(d) & 3u)) {
+    *d++ = v;
+    c--;
+  }
+  const uint32_t wv = 0x01010101u * v;
+  for (; c >= 4; c -= 4, d += 4) *reinterpret_cast<uint32_t *>(d) = wv;
+  while (c-- > 0) *d++ = v;
+}
+
 __global__ void __launch_bounds__(32 * kUnrleWarps)
     k_dec_unrle1_write(const int32_t *idx, const DecBlock *db, const uint8_t *rle, int nacc,
-                       int cap, const LaneStart *lanes, const int64_t *lens, const int64_t *off,
-                       uint8_t *out, uint32_t *crcs) {
-  __shared__ uint32_t tbl[256];
-  crc_table_fill(tbl);
-  __syncthreads();
+                       int cap, const LaneStart *lanes, const int64_t *off, uint8_t *out) {
   const int k = blockIdx.x * kUnrleWarps + (threadIdx.x >> 5);
   const int ln = threadIdx.x & 31;
   if (k >= nacc) return;
@@ -669,28 +700,59 @@ __global__ void __launch_bounds__(32 * kUnrleWarps)
   int p = s0 > 0 ? R[s0 - 1] : -1;
   const LaneStart ls = lanes[(size_t)k * 32 + ln];
   int r = ls.state;
-  int64_t pos = ls.off;
-  uint8_t *O = out + off[k];
-  uint32_t crc = 0;
+  uint8_t *O = out + off[k] + ls.off;
   for (int i = s0; i < e0; i++) {
     const int c = R[i];
     if (r == 4) {
-      for (int q = 0; q < c; q++) {
-        O[pos++] = (uint8_t)p;
-        crc = crc_byte(crc, (uint32_t)p, tbl);
-      }
+      fill_bytes(O, c, (uint8_t)p);
+      O += c;
       r = 0;
     } else {
       r = (r >= 1 && c == p) ? r + 1 : 1;
-      O[pos++] = (uint8_t)c;
-      crc = crc_byte(crc, (uint32_t)c, tbl);
+      *O++ = (uint8_t)c;
     }
     p = c;
   }
-  const int64_t total = lens[k];
-  uint32_t v = crc ? gf_mul(crc, xpow8((uint64_t)(total - pos))) : 0u;
-  for (int o = 16; o; o >>= 1) v ^= __shfl_xor_sync(0xffffffffu, v, o);
-  if (ln == 0) crcs[k] = ~(gf_mul(0xFFFFFFFFu, xpow8((uint64_t)total)) ^ v);
+}
+
+// Block CRCs of the expanded output, one thread block per block: 4096-byte
+// chunks staged in shared memory, thread l's 16 bytes give crc0 * x^(8*16*(255-l))
+// (the chunk right-aligned in 4096 bytes when shorter), the XOR is the
+// chunk's crc0, and the block's crc0 accumulates chunk by chunk.
+__global__ void __launch_bounds__(256) k_dec_crc(const int64_t *lens, const int64_t *off,
+                                                 const uint8_t *out, uint32_t *crcs) {
+  __shared__ uint32_t tbl[256];
+  __shared__ __align__(16) uint8_t chunk[4096];
+  __shared__ uint32_t part[2][8];
+  crc_table_fill(tbl);
+  const int k = blockIdx.x;
+  const int64_t n = lens[k];
+  const uint8_t *src = out + off[k];
+  uint32_t acc = 0;  // thread 0
+  int it = 0;
+  for (int64_t base = 0; base < n; base += 4096, it++) {
+    const int len = n - base < 4096 ? (int)(n - base) : 4096;
+    const int pad = 4096 - len;
+    __syncthreads();  // chunk free
+    for (int i = threadIdx.x; i < 4096; i += 256) chunk[i] = i >= pad ? src[base + i - pad] : 0;
+    __syncthreads();
+    uint32_t r = 0;
+    const uint4 v = *reinterpret_cast<const uint4 *>(chunk + 16 * threadIdx.x);
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int q = 0; q < 16; q++) r = crc_byte(r, (w[q >> 2] >> (8 * (q & 3))) & 0xFFu, tbl);
+    r = r ? gf_mul(r, c_klane.v[threadIdx.x]) : 0u;
+    for (int o = 16; o; o >>= 1) r ^= __shfl_xor_sync(0xffffffffu, r, o);
+    if ((threadIdx.x & 31) == 0) part[it & 1][threadIdx.x >> 5] = r;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t c = 0;
+      for (int q = 0; q < 8; q++) c ^= part[it & 1][q];
+      // acc * x^(8 len) ^ c
+      acc = (acc ? gf_mul(acc, len == 4096 ? c_xpow[12] : xpow8((uint64_t)len)) : 0u) ^ c;
+    }
+  }
+  if (threadIdx.x == 0) crcs[k] = ~(gf_mul(0xFFFFFFFFu, xpow8((uint64_t)n)) ^ acc);
 }
 
 // Device buffer that only grows (contents are not kept).
@@ -768,8 +830,8 @@ struct MallocSink : DecSink {
 // (stream st).
 struct DecWork {
   std::mutex mu;
-  DevBuf words, blk, eos, cnt, cand, db, L, rank, sel, idx, C, tt, lens, off, crc, ctl, mark,
-      bad, lanes;
+  DevBuf words, blk, eos, cnt, cand, db, L, rank, sel, idx, C, tt, lens, off, crc, ctl, bad,
+      lanes;
   DevBuf out[2];
   cudaStream_t st = nullptr, cs = nullptr;
   cudaEvent_t written[2] = {nullptr, nullptr}, copied[2] = {nullptr, nullptr};
@@ -794,7 +856,7 @@ struct DecWork {
   }
   size_t held() const {
     size_t s = 0;
-    for (const DevBuf *b : {&L, &rank, &tt, &sel, &mark, &out[0], &out[1]}) s += b->cap;
+    for (const DevBuf *b : {&L, &rank, &tt, &sel, &ctl, &out[0], &out[1]}) s += b->cap;
     return s;
   }
 };
@@ -812,8 +874,8 @@ DecWork &dec_work() {
 
 // Device bytes of one candidate slot: last column (later the RLE1 bytes),
 // ranks, LF vector, selectors, visited marks.
-constexpr size_t kSlotBytes = (size_t)kDecCap * 9 + kDecMaxSel + (kDecCap + 31) / 32 * 4 +
-                              sizeof(WalkCtl) + sizeof(DecBlock) + 256 * 4 + 32 * 8 + 64;
+constexpr size_t kSlotBytes = (size_t)kDecCap * 9 + kDecMaxSel + sizeof(WalkCtl) +
+                              sizeof(DecBlock) + 256 * 4 + 32 * 8 + 64;
 constexpr int kMaxBatch = 4096;
 
 bool is_header(const uint8_t *h) {
@@ -887,7 +949,6 @@ void decode_words(DecWork &w, size_t n, DecSink &sink) {
   w.off.reserve(8 * (size_t)batch);
   w.crc.reserve(4 * (size_t)batch);
   w.ctl.reserve(sizeof(WalkCtl) * (size_t)batch);
-  w.mark.reserve((size_t)batch * ((cap + 31) / 32) * 4);
   w.bad.reserve(16);
   w.lanes.reserve(sizeof(LaneStart) * 32 * (size_t)batch);
   if (w.h_crc_cap < (size_t)batch) {
@@ -983,19 +1044,17 @@ void decode_words(DecWork &w, size_t n, DecSink &sink) {
     k_dec_lf<<<dim3(64, na), 256, 0, st>>>(didx, ddb, L, w.rank.get<int32_t>(),
                                            w.C.get<int32_t>(), w.tt.get<uint32_t>(), cap);
     BZ_LAUNCH_CHECK();
-    k_dec_split<<<na, 256, 0, st>>>(didx, ddb, w.ctl.get<WalkCtl>(), w.mark.get<uint32_t>(),
-                                    cap);
+    k_dec_split<<<na, 256, 0, st>>>(didx, ddb, w.ctl.get<WalkCtl>(), w.tt.get<uint32_t>(), cap);
     BZ_LAUNCH_CHECK();
     const dim3 wgrid(kMaxWalkers / 64, na);
-    k_dec_walk<<<wgrid, 64, 0, st>>>(didx, ddb, w.tt.get<uint32_t>(), w.ctl.get<WalkCtl>(),
-                                     w.mark.get<uint32_t>(), L, cap, 0);
+    k_dec_walk<<<wgrid, 64, 0, st>>>(didx, ddb, w.tt.get<uint32_t>(), w.ctl.get<WalkCtl>(), L,
+                                     cap, 0);
     BZ_LAUNCH_CHECK();
     BZ_CUDA(cudaMemsetAsync(w.bad.p, 0, 4, st));
-    k_dec_chain<<<(na + 63) / 64, 64, 0, st>>>(didx, ddb, w.ctl.get<WalkCtl>(), na,
-                                               w.bad.get<int>());
+    k_dec_chain<<<na, 256, 0, st>>>(didx, ddb, w.ctl.get<WalkCtl>(), w.bad.get<int>());
     BZ_LAUNCH_CHECK();
-    k_dec_walk<<<wgrid, 64, 0, st>>>(didx, ddb, w.tt.get<uint32_t>(), w.ctl.get<WalkCtl>(),
-                                     w.mark.get<uint32_t>(), L, cap, 1);
+    k_dec_walk<<<wgrid, 64, 0, st>>>(didx, ddb, w.tt.get<uint32_t>(), w.ctl.get<WalkCtl>(), L,
+                                     cap, 1);
     BZ_LAUNCH_CHECK();
     k_dec_repeat<<<dim3(16, na), 256, 0, st>>>(didx, ddb, w.ctl.get<WalkCtl>(), L, cap);
     BZ_LAUNCH_CHECK();
@@ -1022,8 +1081,11 @@ void decode_words(DecWork &w, size_t n, DecSink &sink) {
     w.out[slot].reserve((size_t)tot + 16);
     BZ_CUDA(cudaMemcpyAsync(w.off.p, offs.data(), 8 * na, cudaMemcpyHostToDevice, st));
     k_dec_unrle1_write<<<ugrid, 32 * kUnrleWarps, 0, st>>>(
-        didx, ddb, L, na, cap, w.lanes.get<LaneStart>(), w.lens.get<int64_t>(),
-        w.off.get<int64_t>(), w.out[slot].get<uint8_t>(), w.crc.get<uint32_t>());
+        didx, ddb, L, na, cap, w.lanes.get<LaneStart>(), w.off.get<int64_t>(),
+        w.out[slot].get<uint8_t>());
+    BZ_LAUNCH_CHECK();
+    k_dec_crc<<<na, 256, 0, st>>>(w.lens.get<int64_t>(), w.off.get<int64_t>(),
+                                  w.out[slot].get<uint8_t>(), w.crc.get<uint32_t>());
     BZ_LAUNCH_CHECK();
     BZ_CUDA(cudaMemcpyAsync(w.h_crc, w.crc.p, 4 * na, cudaMemcpyDeviceToHost, st));
     BZ_CUDA(cudaEventRecord(w.written[slot], st));

@@ -24,20 +24,6 @@ namespace bz2g {
 
 namespace {
 
-// c_klane.v[l] = x^(8 * 16 * (255 - l)) mod P: thread l's 16 bytes sit that
-// far before the end of a 4096-byte tile.
-struct LaneShift {
-  uint32_t v[256];
-  constexpr LaneShift() : v() {
-    uint32_t k = 1u;
-    const uint32_t step = xpow8_pow2(4);  // x^(8*16)
-    for (int l = 255; l >= 0; --l) {
-      v[l] = k;
-      k = gf_mul_c(k, step);
-    }
-  }
-};
-__constant__ LaneShift c_klane{};
 
 // Stage one raw tile into shared memory: sb[0..len) = bytes, *prev = byte
 // before the tile (or -1 at the block start).

@@ -109,32 +109,35 @@ __device__ __forceinline__ uint32_t load16(const uint8_t *in, int64_t n, int64_t
 
 // fa[t] / la[t]: first / last run start in tile t (INT64_MAX / -1 if none).
 __global__ void __launch_bounds__(kSplitThreads)
-    k_split_runs(const uint8_t *__restrict__ in, int64_t n, int64_t *fa, int64_t *la) {
-  __shared__ int64_t sh[2][8];
-  const int64_t p0 = (int64_t)blockIdx.x * kSplitTile + threadIdx.x * 16;
-  uint8_t c[16];
-  int nv;
-  const uint32_t s = load16(in, n, p0, c, nv);
-  int64_t f = s ? p0 + __ffs(s) - 1 : INT64_MAX;
-  int64_t l = s ? p0 + 31 - __clz(s) : -1;
-  for (int o = 16; o; o >>= 1) {
-    f = min(f, (int64_t)__shfl_xor_sync(0xffffffffu, (long long)f, o));
-    l = max(l, (int64_t)__shfl_xor_sync(0xffffffffu, (long long)l, o));
-  }
-  if (lane_id() == 0) {
-    sh[0][warp_id()] = f;
-    sh[1][warp_id()] = l;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int w = 1; w < kSplitThreads / 32; w++) {
-      f = min(f, sh[0][w]);
-      l = max(l, sh[1][w]);
+    k_split_runs(const uint8_t *__restrict__ in, int64_t n, int64_t T, int64_t *fa,
+                 int64_t *la) {
+  __shared__ int64_t sh[2][2][8];
+  for (int64_t t = blockIdx.x, it = 0; t < T; t += gridDim.x, it++) {
+    const int64_t p0 = t * kSplitTile + threadIdx.x * 16;
+    uint8_t c[16];
+    int nv;
+    const uint32_t s = load16(in, n, p0, c, nv);
+    int64_t f = s ? p0 + __ffs(s) - 1 : INT64_MAX;
+    int64_t l = s ? p0 + 31 - __clz(s) : -1;
+    for (int o = 16; o; o >>= 1) {
+      f = min(f, (int64_t)__shfl_xor_sync(0xffffffffu, (long long)f, o));
+      l = max(l, (int64_t)__shfl_xor_sync(0xffffffffu, (long long)l, o));
     }
-    f = min(f, sh[0][0]);
-    l = max(l, sh[1][0]);
-    fa[blockIdx.x] = f;
-    la[blockIdx.x] = l;
+    // double-buffered partials: one barrier per tile
+    int64_t(*buf)[8] = sh[it & 1];
+    if (lane_id() == 0) {
+      buf[0][warp_id()] = f;
+      buf[1][warp_id()] = l;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 0; w < kSplitThreads / 32; w++) {
+        f = min(f, buf[0][w]);
+        l = max(l, buf[1][w]);
+      }
+      fa[t] = f;
+      la[t] = l;
+    }
   }
 }
 
@@ -194,15 +197,21 @@ __global__ void __launch_bounds__(kScanThreads)
 }
 
 // Per position of the thread's 16 bytes: the run start before p0 is rs_in;
-// calls f(k, position, run start) for each byte inside the input.
+// calls f(position, run start, position in its chunk) for each byte inside
+// the input.
 template <typename F>
 __device__ __forceinline__ void walk16(int64_t p0, int nv, uint32_t s, int64_t rs_in, F f) {
   int64_t rs = rs_in;
+  int q = (int)((p0 - rs_in) % kCut);  // chunk position of p0 if it continues the run
 #pragma unroll
   for (int k = 0; k < 16; k++) {
     if (k < nv) {
-      if ((s >> k) & 1u) rs = p0 + k;
-      f(k, p0 + k, rs);
+      if ((s >> k) & 1u) {
+        rs = p0 + k;
+        q = 0;
+      }
+      f(p0 + k, rs, q);
+      q = q + 1 == kCut ? 0 : q + 1;
     }
   }
 }
@@ -221,18 +230,20 @@ __device__ __forceinline__ int64_t run_start_in(int64_t p0, uint32_t s, int64_t 
 
 // c[t] = sum of cnt over tile t.
 __global__ void __launch_bounds__(kSplitThreads)
-    k_split_count(const uint8_t *__restrict__ in, int64_t n, const int64_t *lb, int32_t *c) {
+    k_split_count(const uint8_t *__restrict__ in, int64_t n, int64_t T, const int64_t *lb,
+                  int32_t *c) {
   __shared__ int64_t sh[32];
-  const int64_t t = blockIdx.x;
-  const int64_t p0 = t * kSplitTile + threadIdx.x * 16;
-  uint8_t b[16];
-  int nv;
-  const uint32_t s = load16(in, n, p0, b, nv);
-  const int64_t rs0 = run_start_in(p0, s, lb[t], sh);
-  int64_t sum = 0;
-  walk16(p0, nv, s, rs0, [&](int, int64_t p, int64_t rs) { sum += cnt_of((int)((p - rs) % kCut)); });
-  const int64_t tot = block_scan(sum, sh, SumOp());
-  if (threadIdx.x == kSplitThreads - 1) c[t] = (int32_t)tot;
+  for (int64_t t = blockIdx.x; t < T; t += gridDim.x) {
+    const int64_t p0 = t * kSplitTile + threadIdx.x * 16;
+    uint8_t b[16];
+    int nv;
+    const uint32_t s = load16(in, n, p0, b, nv);
+    const int64_t rs0 = run_start_in(p0, s, lb[t], sh);
+    int64_t sum = 0;
+    walk16(p0, nv, s, rs0, [&](int64_t, int64_t, int q) { sum += cnt_of(q); });
+    const int64_t tot = block_scan(sum, sh, SumOp());
+    if (threadIdx.x == kSplitThreads - 1) c[t] = (int32_t)tot;
+  }
 }
 
 // P[t] = exclusive prefix of c, P[T] = total.  One thread block.
@@ -269,13 +280,14 @@ __global__ void __launch_bounds__(kSplitThreads)
                   const int64_t *lb, const int64_t *nf, int64_t maxw, int64_t *ends, int cap,
                   int *count, int *err) {
   __shared__ int64_t sh[32];
-  __shared__ int64_t s_start, s_G, s_x0, s_Gx0, s_rs0, s_re0, s_last_rs;
+  __shared__ int64_t s_start, s_G, s_x0, s_Gx0, s_rs0, s_re0, s_last_rs, s_span;
   __shared__ int s_nb;
   const int tid = threadIdx.x;
   if (tid == 0) {
     s_start = 0;
     s_G = 0;
     s_nb = 0;
+    s_span = 0;
   }
   __syncthreads();
   const int64_t PT = P[T];
@@ -290,7 +302,26 @@ __global__ void __launch_bounds__(kSplitThreads)
     int64_t xend = n, Gx = PT;
     if (PT >= target) {
       // t* = the last tile with P[t*] < target (P[s's tile] <= Gs < target)
-      int64_t lo = s / kSplitTile, hi = T;
+      const int64_t lo0 = s / kSplitTile;
+      int64_t lo = lo0, hi = T;
+      if (s_span > 0) {
+        // first probes: 256 consecutive tiles around the tile the previous
+        // block's span predicts (block sizes change slowly)
+        const int64_t fv = max(lo + 1, lo + s_span - kSplitThreads / 2);
+        const int64_t lv = min(hi - 1, fv + kSplitThreads - 1);
+        if (fv <= lv) {
+          const int64_t q = fv + tid;
+          const int k = __syncthreads_count(q <= lv && P[q] < target);
+          if (k == 0) {
+            hi = fv;
+          } else if (k == lv - fv + 1) {
+            lo = lv;
+          } else {
+            lo = fv + k - 1;
+            hi = fv + k;
+          }
+        }
+      }
       while (hi - lo > 1) {
         const int64_t step = (hi - lo + kSplitThreads - 1) / kSplitThreads;
         const int64_t q = lo + (int64_t)(tid + 1) * step;
@@ -306,17 +337,17 @@ __global__ void __launch_bounds__(kSplitThreads)
       const uint32_t sm = load16(in, n, p0, b, nv);
       const int64_t rs_in = run_start_in(p0, sm, lb[t], sh);
       int64_t sum = 0;
-      walk16(p0, nv, sm, rs_in, [&](int, int64_t p, int64_t rs) { sum += cnt_of((int)((p - rs) % kCut)); });
+      walk16(p0, nv, sm, rs_in, [&](int64_t, int64_t, int q) { sum += cnt_of(q); });
       const int64_t inc = block_scan(sum, sh, SumOp());
       // x0: the first position of the tile with G(x0) >= target
       int64_t g = P[t] + inc - sum, my_x0 = INT64_MAX, my_rs = -1, my_g = 0, last_rs = -1;
-      walk16(p0, nv, sm, rs_in, [&](int, int64_t p, int64_t rs) {
+      walk16(p0, nv, sm, rs_in, [&](int64_t p, int64_t rs, int q) {
         if (my_x0 == INT64_MAX && g >= target) {
           my_x0 = p;
           my_rs = rs;
           my_g = g;
         }
-        g += cnt_of((int)((p - rs) % kCut));
+        g += cnt_of(q);
         last_rs = rs;
       });
       const int64_t x0m = block_scan(my_x0, sh, MinOp());
@@ -382,6 +413,7 @@ __global__ void __launch_bounds__(kSplitThreads)
     if (tid == 0) {
       ends[s_nb] = xend;
       s_nb++;
+      s_span = xend / kSplitTile - s / kSplitTile;
       s_start = xend;
       s_G = Gx;
     }
@@ -421,11 +453,15 @@ std::vector<int64_t> bzip2_split(const uint8_t *d_in, int64_t n, int level, cuda
   int64_t *dends = P + (T + 1) + (T + 1) / 2 + 1;
   int *counters = reinterpret_cast<int *>(dends + cap);
   BZ_CUDA(cudaMemsetAsync(counters, 0, 8, st));
-  k_split_runs<<<(unsigned)T, kSplitThreads, 0, st>>>(d_in, n, fa, la);
+  int dev = 0, sms = 0;
+  BZ_CUDA(cudaGetDevice(&dev));
+  BZ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const unsigned grid = (unsigned)std::min<int64_t>(T, (int64_t)sms * 8);
+  k_split_runs<<<grid, kSplitThreads, 0, st>>>(d_in, n, T, fa, la);
   BZ_LAUNCH_CHECK();
   k_split_scan_runs<<<1, kScanThreads, 0, st>>>(T, n, la, fa, lb, nf);
   BZ_LAUNCH_CHECK();
-  k_split_count<<<(unsigned)T, kSplitThreads, 0, st>>>(d_in, n, lb, c);
+  k_split_count<<<grid, kSplitThreads, 0, st>>>(d_in, n, T, lb, c);
   BZ_LAUNCH_CHECK();
   k_split_prefix<<<1, kScanThreads, 0, st>>>(T, c, P);
   BZ_LAUNCH_CHECK();
