@@ -11,12 +11,11 @@
 //      broadcasts): header (CRC, origPtr, symbol map, tables, selectors),
 //      Huffman symbols via a 10-bit lookup table with the canonical slow path
 //      for longer codes, RUNA/RUNB zero runs, and the inverse move-to-front
-//      with the 256-entry list spread over the lanes (8 bytes each).  Out: the
-//      BWT last column L and, per position, the rank of L[i] among equal
-//      symbols before it.
-//   3. k_dec_lf: LF vector tt[C[L[i]] + rank[i]] = i << 8 | L[i] (parallel).
+//      32 MTF steps at a time across the warp.  Out: the BWT last column L.
+//   3. k_dec_lf_hist / _scan / _rank: LF vector
+//      tt[C[L[i]] + rank(i)] = i << 8 | L[i] by a stable counting sort.
 //   4. k_dec_split / k_dec_walk / k_dec_chain: per block, the chain from
-//      origPtr gives the RLE1 bytes, cut at up to 256 splitters that are
+//      origPtr gives the RLE1 bytes, cut at up to 2048 splitters that are
 //      walked in parallel.
 //   5. k_dec_unrle1_count / _write: per block, one warp expands the RLE1 runs
 //      (4 equal bytes then a count byte) from 32 segments at once; k_dec_crc
@@ -148,16 +147,27 @@ struct DecShared {
   uint16_t perm[kDecMaxGroups][kDecMaxAlpha];
   uint8_t minlen[kDecMaxGroups];
   uint8_t len[kDecMaxGroups][kDecMaxAlpha];
-  int32_t cnt[256];
   uint8_t seq2unseq[256];
-  int32_t flag;
+  uint8_t list[2][256];  // MTF list before / after a batch of steps
+  uint32_t used[8];      // list positions a batch read
 };
+
+// c copies of byte v at d (word stores between unaligned ends).
+__device__ __forceinline__ void fill_bytes(uint8_t *d, int c, uint8_t v) {
+  while (c > 0 && (reinterpret_cast<uintptr_t>(d) & 3u)) {
+    *d++ = v;
+    c--;
+  }
+  const uint32_t wv = 0x01010101u * v;
+  for (; c >= 4; c -= 4, d += 4) *reinterpret_cast<uint32_t *>(d) = wv;
+  while (c-- > 0) *d++ = v;
+}
 
 // One warp per candidate.  sel: per-candidate selector scratch (kDecMaxSel).
 __global__ void __launch_bounds__(32) k_dec_block(const uint32_t *words, int64_t nwords,
                                                   const int64_t *cand, int ncand,
                                                   DecBlock *out, uint8_t *Lbuf,
-                                                  int32_t *rank, uint8_t *selbuf, int cap) {
+                                                  uint8_t *selbuf, int cap) {
   __shared__ DecShared sh;
   const int bi = blockIdx.x;
   if (bi >= ncand) return;
@@ -170,7 +180,6 @@ __global__ void __launch_bounds__(32) k_dec_block(const uint32_t *words, int64_t
   r.crc = 0;
   r.status = kDecOk;
   uint8_t *L = Lbuf + (size_t)bi * cap;
-  int32_t *RK = rank + (size_t)bi * cap;
   uint8_t *sel = selbuf + (size_t)bi * kDecMaxSel;
   BitReader br;
   br.init(words, nwords, r.start + 48);
@@ -287,20 +296,101 @@ __global__ void __launch_bounds__(32) k_dec_block(const uint32_t *words, int64_t
       }
     }
   }
-  for (int c = ln; c < 256; c += 32) sh.cnt[c] = 0;
   __syncwarp();
-  // Huffman symbols -> RUNA/RUNB runs and inverse MTF.  The list: lane l
-  // holds positions 8l .. 8l+7, byte k of its word = position 8l + k.
-  uint64_t word = 0;
-  for (int k = 7; k >= 0; k--) {
-    const int p = 8 * ln + k;
-    word = (word << 8) | (uint64_t)(p < nuse ? p : 0);
-  }
-  int m = 0;
+  // Huffman symbols -> RUNA/RUNB runs -> MTF steps, batched: lane q holds
+  // step q of the batch (v = MTF index, 0 for a zero run; bytes = 1, or the
+  // run length).  A full batch is resolved across the warp at once:
+  //  * lane t walks its index back through the batch's earlier steps s: a
+  //    step moved the entry at v_s to the front, so position p after it was
+  //    p - 1 before it when 1 <= p <= v_s, and p == 0 is step s's own output;
+  //  * lanes that reach position 0 point at that step's lane, the others read
+  //    the list as it was before the batch; pointer jumping settles pointers;
+  //  * the new list: the batch's distinct outputs, most recent first, then
+  //    the untouched entries in their old order.
+  for (int p = ln; p < 256; p += 32) sh.list[0][p] = (uint8_t)p;
+  __syncwarp();
+  int cur = 0;
+  int my_v = 0, my_n = 0, nst = 0;
+  int m = 0;         // bytes written by resolved batches
+  int64_t pend = 0;  // bytes of the batch being filled
   int64_t zrun = 0;
   int zbit = 0;
   const int eob = nuse + 1;
   int gsel = 0, gleft = 0, tsel = 0;
+  auto resolve_batch = [&]() {
+    const unsigned full = 0xffffffffu;
+    const bool act = ln < nst;
+    int p = my_v, ptr = -1;
+#pragma unroll
+    for (int s = 30; s >= 0; --s) {
+      const int vs = __shfl_sync(full, my_v, s);
+      if (ln > s && ptr < 0) {
+        if (p == 0) ptr = s;
+        else if (p <= vs) p--;
+      }
+    }
+    const uint8_t *lst = sh.list[cur];
+    const bool from_list = act && ptr < 0;
+    int val = from_list ? (int)lst[p] : -1;
+#pragma unroll
+    for (int r2 = 0; r2 < 5; r2++) {
+      const int src = ptr >= 0 ? ptr : ln;
+      const int tv = __shfl_sync(full, val, src);
+      const int tp = __shfl_sync(full, ptr, src);
+      if (val < 0 && ptr >= 0) {
+        if (tv >= 0) val = tv;
+        else ptr = tp;
+      }
+    }
+    const unsigned peers = __match_any_sync(full, act ? val : 256 + ln);
+    const unsigned above = ~((2u << ln) - 1u);  // lanes after this one
+    const bool last = act && (peers & above) == 0u;
+    const unsigned lastm = __ballot_sync(full, last);
+    const int D = __popc(lastm);
+    if (ln < 8) sh.used[ln] = 0u;
+    __syncwarp();
+    if (from_list) atomicOr(&sh.used[p >> 5], 1u << (p & 31));
+    __syncwarp();
+    uint8_t *nx = sh.list[cur ^ 1];
+    if (last) nx[__popc(lastm & above)] = (uint8_t)val;
+    {
+      const int q0 = 8 * ln;
+      int below = 0;
+      for (int x = 0; x < (q0 >> 5); x++) below += __popc(sh.used[x]);
+      const uint32_t uw = sh.used[q0 >> 5];
+      for (int j = 0; j < 8; j++) {
+        const int q = q0 + j;
+        if (q >= nuse) break;
+        const uint32_t bit = 1u << (q & 31);
+        if (!(uw & bit)) nx[D + q - below - __popc(uw & (bit - 1u))] = lst[q];
+      }
+    }
+    // bytes: step t at m + (bytes of the earlier steps)
+    const int nb = act ? my_n : 0;
+    const int incl = warp_incl_sum(nb);
+    if (act) {
+      const uint8_t c = sh.seq2unseq[val];
+      if (nb == 1) L[m + incl - 1] = c;
+      else fill_bytes(L + m + incl - nb, nb, c);
+    }
+    m += __shfl_sync(full, incl, 31);
+    cur ^= 1;
+    nst = 0;
+    pend = 0;
+    __syncwarp();
+  };
+  // queue one step; false when the block would pass its capacity
+  auto push_step = [&](int v, int64_t bytes) -> bool {
+    if (bytes > (int64_t)cap - m - pend) return false;
+    if (ln == nst) {
+      my_v = v;
+      my_n = (int)bytes;
+    }
+    nst++;
+    pend += bytes;
+    if (nst == 32) resolve_batch();
+    return true;
+  };
   if (r.status == kDecOk) {
     for (int guard = 0;; guard++) {
       if (guard > cap + 64) {
@@ -346,55 +436,28 @@ __global__ void __launch_bounds__(32) k_dec_block(const uint32_t *words, int64_t
         zbit++;
         continue;
       }
-      // flush a pending zero run: copies of the list's front symbol
+      // a pending zero run: copies of the list's front entry (no move)
       if (zrun > 0) {
-        if (zrun > cap - m) {
+        if (!push_step(0, zrun)) {
           r.status = kDecTooLong;
           break;
         }
-        const int front = (int)__shfl_sync(0xffffffffu, (uint32_t)(word & 0xFFu), 0);
-        const uint8_t c = sh.seq2unseq[front];
-        const int base_cnt = sh.cnt[c];
-        for (int64_t o = ln; o < zrun; o += 32) {
-          L[m + o] = c;
-          RK[m + o] = base_cnt + (int)o;
-        }
-        __syncwarp();
-        if (ln == 0) sh.cnt[c] = base_cnt + (int)zrun;
-        __syncwarp();
-        m += (int)zrun;
         zrun = 0;
         zbit = 0;
       }
       if (sym == eob) break;
-      // value v = sym - 1 >= 1: symbol at list position v moves to the front
+      // value v = sym - 1 >= 1: the entry at list position v moves to the front
       const int v = sym - 1;
       if (v >= nuse) {
         r.status = kDecBadSymbol;
         break;
       }
-      if (m >= cap) {
+      if (!push_step(v, 1)) {
         r.status = kDecTooLong;
         break;
       }
-      const int owner = v >> 3, jb = v & 7;
-      const uint32_t pos = (uint32_t)((__shfl_sync(0xffffffffu, word, owner) >> (8 * jb)) & 0xFFu);
-      const uint64_t top = __shfl_up_sync(0xffffffffu, word >> 56, 1);
-      const uint64_t carry = ln == 0 ? (uint64_t)pos : top;
-      if (ln < owner) {
-        word = (word << 8) | carry;
-      } else if (ln == owner) {
-        const uint64_t lowm = jb == 7 ? ~0ull : ((1ull << (8 * (jb + 1))) - 1);
-        word = (word & ~lowm) | (((word << 8) | carry) & lowm);
-      }
-      const uint8_t c = sh.seq2unseq[pos];
-      if (ln == 0) {
-        L[m] = c;
-        RK[m] = sh.cnt[c]++;
-      }
-      __syncwarp();
-      m++;
     }
+    if (r.status == kDecOk && nst > 0) resolve_batch();
   }
   if (r.status == kDecOk && (r.orig_ptr < 0 || r.orig_ptr >= m)) r.status = kDecBadOrigPtr;
   r.m = m;
@@ -402,44 +465,84 @@ __global__ void __launch_bounds__(32) k_dec_block(const uint32_t *words, int64_t
   if (ln == 0) out[bi] = r;
 }
 
-// Cumulative symbol counts of each accepted block: C[b][c] = symbols < c.
-__global__ void k_dec_counts(const int32_t *idx, const DecBlock *db, const uint8_t *Lbuf,
-                             int32_t *C, int cap) {
+// LF vector without serial ranks: T[C[L[i]] + rank(i)] = i << 8 | L[i], with
+// rank(i) = #{j < i : L[j] == L[i]} (then for j = LF(i), psi(j) = i and
+// F[j] = L[i]).  A stable counting sort by the byte: per 4096-entry chunk a
+// histogram, per block a scan over chunks (each chunk's start per byte value,
+// C included), then per chunk the ranks of 256 entries at a time: equal bytes
+// in a warp by match_any, earlier warps by shared counts.
+constexpr int kLfChunk = 4096;
+constexpr int kLfChunks = (kDecCap + kLfChunk - 1) / kLfChunk;
+
+__global__ void __launch_bounds__(256) k_dec_lf_hist(const int32_t *idx, const DecBlock *db,
+                                                     const uint8_t *Lbuf, int32_t *H, int cap) {
   __shared__ int cnt[256];
-  const int k = blockIdx.x;
+  const int k = blockIdx.y, ch = blockIdx.x;
   const int bi = idx[k];
   const int m = db[bi].m;
+  const int c0 = ch * kLfChunk;
+  if (c0 >= m) return;
+  const uint8_t *L = Lbuf + (size_t)bi * cap;
   cnt[threadIdx.x] = 0;
   __syncthreads();
-  const uint8_t *L = Lbuf + (size_t)bi * cap;
-  for (int i = threadIdx.x; i < m; i += blockDim.x) atomicAdd(&cnt[L[i]], 1);
+  const int c1 = min(m, c0 + kLfChunk);
+  for (int i = c0 + threadIdx.x; i < c1; i += 256) atomicAdd(&cnt[L[i]], 1);
   __syncthreads();
-  if (threadIdx.x == 0) {
-    int run = 0;
-    for (int c = 0; c < 256; c++) {
-      const int v = cnt[c];
-      cnt[c] = run;
-      run += v;
-    }
-  }
-  __syncthreads();
-  C[(size_t)k * 256 + threadIdx.x] = cnt[threadIdx.x];
+  H[((size_t)k * kLfChunks + ch) * 256 + threadIdx.x] = cnt[threadIdx.x];
 }
 
-// tt[C[L[i]] + rank[i]] = i << 8 | L[i]: for j = LF(i), psi(j) = i and
-// F[j] = L[i]   (grid.y = accepted block)
-__global__ void k_dec_lf(const int32_t *idx, const DecBlock *db, const uint8_t *Lbuf,
-                         const int32_t *rank, const int32_t *C, uint32_t *tt, int cap) {
-  const int k = blockIdx.y;
+// Per block (thread = byte value): H[chunk][c] becomes the position of the
+// chunk's first c in F order.
+__global__ void __launch_bounds__(256) k_dec_lf_scan(const int32_t *idx, const DecBlock *db,
+                                                     int32_t *H) {
+  __shared__ int scratch[40];
+  const int k = blockIdx.x;
+  const int m = db[idx[k]].m;
+  const int nch = (m + kLfChunk - 1) / kLfChunk;
+  int32_t *h = H + (size_t)k * kLfChunks * 256 + threadIdx.x;
+  int tot = 0;
+  for (int ch = 0; ch < nch; ch++) tot += h[(size_t)ch * 256];
+  int all;
+  int run = block_excl_sum(tot, scratch, &all);  // C[c]
+  for (int ch = 0; ch < nch; ch++) {
+    const int v = h[(size_t)ch * 256];
+    h[(size_t)ch * 256] = run;
+    run += v;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_dec_lf_rank(const int32_t *idx, const DecBlock *db,
+                                                     const uint8_t *Lbuf, const int32_t *H,
+                                                     uint32_t *tt, int cap) {
+  __shared__ int run[256];
+  __shared__ int wc[8][256];
+  const int k = blockIdx.y, ch = blockIdx.x;
   const int bi = idx[k];
   const int m = db[bi].m;
+  const int c0 = ch * kLfChunk;
+  if (c0 >= m) return;
   const uint8_t *L = Lbuf + (size_t)bi * cap;
-  const int32_t *RK = rank + (size_t)bi * cap;
   uint32_t *T = tt + (size_t)k * cap;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-    const int c = L[i];
-    const int j = C[(size_t)k * 256 + c] + RK[i];
-    if (j >= 0 && j < m) T[j] = ((uint32_t)i << 8) | (uint32_t)c;
+  const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
+  run[threadIdx.x] = H[((size_t)k * kLfChunks + ch) * 256 + threadIdx.x];
+  for (int sub = 0; sub < kLfChunk / 256; sub++) {
+    const int i = c0 + sub * 256 + threadIdx.x;
+    if (c0 + sub * 256 >= m) break;  // uniform
+    const bool valid = i < m;
+    const int c = valid ? (int)L[i] : 256 + ln;
+    for (int q = threadIdx.x; q < 8 * 256; q += 256) (&wc[0][0])[q] = 0;
+    __syncthreads();
+    const unsigned peers = __match_any_sync(0xffffffffu, c);
+    const int wr = __popc(peers & ((1u << ln) - 1u));
+    if (valid && wr == 0) wc[w][c] = __popc(peers);
+    __syncthreads();
+    if (valid) {
+      int j = run[c] + wr;
+      for (int q = 0; q < w; q++) j += wc[q][c];
+      if (j >= 0 && j < m) T[j] = ((uint32_t)i << 8) | (uint32_t)c;
+    }
+    __syncthreads();
+    if (valid && wr == 0) atomicAdd(&run[c], __popc(peers));
   }
 }
 
@@ -675,17 +778,6 @@ __global__ void __launch_bounds__(32 * kUnrleWarps)
   if (ln == 0) lens[k] = off;
 }
 
-// c copies of byte v at d (word stores between unaligned ends).
-__device__ __forceinline__ void fill_bytes(uint8_t *d, int c, uint8_t v) {
-  while (c > 0 && (reinterpret_cast<uintptr_t>(d) & 3u)) {
-    *d++ = v;
-    c--;
-  }
-  const uint32_t wv = 0x01010101u * v;
-  for (; c >= 4; c -= 4, d += 4) *reinterpret_cast<uint32_t *>(d) = wv;
-  while (c-- > 0) *d++ = v;
-}
-
 __global__ void __launch_bounds__(32 * kUnrleWarps)
     k_dec_unrle1_write(const int32_t *idx, const DecBlock *db, const uint8_t *rle, int nacc,
                        int cap, const LaneStart *lanes, const int64_t *off, uint8_t *out) {
@@ -830,7 +922,7 @@ struct MallocSink : DecSink {
 // (stream st).
 struct DecWork {
   std::mutex mu;
-  DevBuf words, blk, eos, cnt, cand, db, L, rank, sel, idx, C, tt, lens, off, crc, ctl, bad,
+  DevBuf words, blk, eos, cnt, cand, db, L, hist, sel, idx, tt, lens, off, crc, ctl, bad,
       lanes;
   DevBuf out[2];
   cudaStream_t st = nullptr, cs = nullptr;
@@ -856,7 +948,7 @@ struct DecWork {
   }
   size_t held() const {
     size_t s = 0;
-    for (const DevBuf *b : {&L, &rank, &tt, &sel, &ctl, &out[0], &out[1]}) s += b->cap;
+    for (const DevBuf *b : {&L, &hist, &tt, &sel, &ctl, &out[0], &out[1]}) s += b->cap;
     return s;
   }
 };
@@ -872,10 +964,10 @@ DecWork &dec_work() {
   return *per_device[dev];
 }
 
-// Device bytes of one candidate slot: last column (later the RLE1 bytes),
-// ranks, LF vector, selectors, visited marks.
-constexpr size_t kSlotBytes = (size_t)kDecCap * 9 + kDecMaxSel + sizeof(WalkCtl) +
-                              sizeof(DecBlock) + 256 * 4 + 32 * 8 + 64;
+// Device bytes of one candidate slot: last column (later the RLE1 bytes), LF
+// vector, chunk histograms, selectors, walk control.
+constexpr size_t kSlotBytes = (size_t)kDecCap * 5 + (size_t)kLfChunks * 256 * 4 + kDecMaxSel +
+                              sizeof(WalkCtl) + sizeof(DecBlock) + 32 * 8 + 64;
 constexpr int kMaxBatch = 4096;
 
 bool is_header(const uint8_t *h) {
@@ -940,10 +1032,9 @@ void decode_words(DecWork &w, size_t n, DecSink &sink) {
   w.cand.reserve(8 * (size_t)batch);
   w.db.reserve(sizeof(DecBlock) * (size_t)batch);
   w.L.reserve((size_t)batch * cap);
-  w.rank.reserve((size_t)batch * cap * 4);
+  w.hist.reserve((size_t)batch * kLfChunks * 256 * 4);
   w.sel.reserve((size_t)batch * kDecMaxSel);
   w.idx.reserve(4 * (size_t)batch);
-  w.C.reserve((size_t)batch * 256 * 4);
   w.tt.reserve((size_t)batch * cap * 4);
   w.lens.reserve(8 * (size_t)batch);
   w.off.reserve(8 * (size_t)batch);
@@ -1014,8 +1105,7 @@ void decode_words(DecWork &w, size_t n, DecSink &sink) {
     const int nc = (int)std::min<size_t>(batch, cands.size() - ci);
     BZ_CUDA(cudaMemcpyAsync(w.cand.p, cands.data() + ci, 8 * nc, cudaMemcpyHostToDevice, st));
     k_dec_block<<<nc, 32, 0, st>>>(w.words.get<uint32_t>(), nwords, w.cand.get<int64_t>(), nc,
-                                   w.db.get<DecBlock>(), L, w.rank.get<int32_t>(),
-                                   w.sel.get<uint8_t>(), cap);
+                                   w.db.get<DecBlock>(), L, w.sel.get<uint8_t>(), cap);
     BZ_LAUNCH_CHECK();
     BZ_CUDA(cudaMemcpyAsync(hdb.data(), w.db.p, sizeof(DecBlock) * nc, cudaMemcpyDeviceToHost,
                             st));
@@ -1039,10 +1129,13 @@ void decode_words(DecWork &w, size_t n, DecSink &sink) {
     const int32_t *didx = w.idx.get<int32_t>();
     const DecBlock *ddb = w.db.get<DecBlock>();
     BZ_CUDA(cudaMemcpyAsync(w.idx.p, acc.data(), 4 * na, cudaMemcpyHostToDevice, st));
-    k_dec_counts<<<na, 256, 0, st>>>(didx, ddb, L, w.C.get<int32_t>(), cap);
+    const dim3 lgrid(kLfChunks, na);
+    k_dec_lf_hist<<<lgrid, 256, 0, st>>>(didx, ddb, L, w.hist.get<int32_t>(), cap);
     BZ_LAUNCH_CHECK();
-    k_dec_lf<<<dim3(64, na), 256, 0, st>>>(didx, ddb, L, w.rank.get<int32_t>(),
-                                           w.C.get<int32_t>(), w.tt.get<uint32_t>(), cap);
+    k_dec_lf_scan<<<na, 256, 0, st>>>(didx, ddb, w.hist.get<int32_t>());
+    BZ_LAUNCH_CHECK();
+    k_dec_lf_rank<<<lgrid, 256, 0, st>>>(didx, ddb, L, w.hist.get<int32_t>(),
+                                         w.tt.get<uint32_t>(), cap);
     BZ_LAUNCH_CHECK();
     k_dec_split<<<na, 256, 0, st>>>(didx, ddb, w.ctl.get<WalkCtl>(), w.tt.get<uint32_t>(), cap);
     BZ_LAUNCH_CHECK();
