@@ -67,37 +67,39 @@ enum DecStatus {
 __device__ __forceinline__ uint32_t bswap32(uint32_t x) { return __byte_perm(x, 0, 0x0123); }
 
 // Sequential big-endian bit reader over the stream's words (reads past the end
-// return zeros).
+// return zeros).  A three-word window w0:w1:w2 (already byte-swapped) and the
+// bit offset in w0: peek32 is one funnel shift, and the word after the
+// window is loaded when the offset passes a word, well before it is needed.
 struct BitReader {
   const uint32_t *w;
-  int64_t nwords, wpos;
-  uint64_t buf;  // next bits, left-aligned
-  int have;
+  int64_t nwords, wnext;  // wnext: index of the word after the window
+  uint32_t w0, w1, w2;
+  int bo;
+  __device__ __forceinline__ uint32_t ld(int64_t i) const {
+    return i < nwords ? bswap32(w[i]) : 0u;
+  }
   __device__ void init(const uint32_t *words, int64_t nw, int64_t bitpos) {
     w = words;
     nwords = nw;
-    wpos = bitpos >> 5;
-    buf = 0;
-    have = 0;
-    refill();
-    const int skip = (int)(bitpos & 31);
-    buf <<= skip;
-    have -= skip;
-    refill();
+    const int64_t i = bitpos >> 5;
+    w0 = ld(i);
+    w1 = ld(i + 1);
+    w2 = ld(i + 2);
+    wnext = i + 3;
+    bo = (int)(bitpos & 31);
   }
-  __device__ __forceinline__ void refill() {
-    while (have <= 32) {
-      const uint32_t v = wpos < nwords ? bswap32(w[wpos]) : 0u;
-      wpos++;
-      buf |= (uint64_t)v << (32 - have);
-      have += 32;
-    }
-  }
-  __device__ __forceinline__ uint32_t peek(int n) { return (uint32_t)(buf >> (64 - n)); }
+  // the 32 bits from the current position
+  __device__ __forceinline__ uint32_t peek32() const { return __funnelshift_l(w1, w0, bo); }
+  __device__ __forceinline__ uint32_t peek(int n) const { return peek32() >> (32 - n); }
+  // n <= 32
   __device__ __forceinline__ void skip(int n) {
-    buf <<= n;
-    have -= n;
-    refill();
+    bo += n;
+    if (bo >= 32) {
+      bo -= 32;
+      w0 = w1;
+      w1 = w2;
+      w2 = ld(wnext++);
+    }
   }
   __device__ __forceinline__ uint32_t get(int n) {
     if (n == 0) return 0;
@@ -105,7 +107,7 @@ struct BitReader {
     skip(n);
     return v;
   }
-  __device__ __forceinline__ int64_t pos() const { return wpos * 32 - have; }
+  __device__ __forceinline__ int64_t pos() const { return (wnext - 3) * 32 + bo; }
 };
 
 __global__ void k_dec_magic(const uint32_t *words, int64_t nwords, int64_t nbits,
@@ -311,8 +313,8 @@ __global__ void __launch_bounds__(32) k_dec_block(const uint32_t *words, int64_t
   __syncwarp();
   int cur = 0;
   int my_v = 0, my_n = 0, nst = 0;
-  int m = 0;         // bytes written by resolved batches
-  int64_t pend = 0;  // bytes of the batch being filled
+  int m = 0;     // bytes written by resolved batches
+  int pend = 0;  // bytes of the batch being filled
   int64_t zrun = 0;
   int zbit = 0;
   const int eob = nuse + 1;
@@ -379,52 +381,55 @@ __global__ void __launch_bounds__(32) k_dec_block(const uint32_t *words, int64_t
     pend = 0;
     __syncwarp();
   };
-  // queue one step; false when the block would pass its capacity
-  auto push_step = [&](int v, int64_t bytes) -> bool {
-    if (bytes > (int64_t)cap - m - pend) return false;
+  // queue one step (the caller has checked the capacity)
+  auto push_step = [&](int v, int bytes) {
     if (ln == nst) {
       my_v = v;
-      my_n = (int)bytes;
+      my_n = bytes;
     }
     nst++;
     pend += bytes;
     if (nst == 32) resolve_batch();
-    return true;
   };
+  // Every iteration takes one symbol of a 50-symbol group and the groups are
+  // bounded by nsel, so the loop ends.
   if (r.status == kDecOk) {
-    for (int guard = 0;; guard++) {
-      if (guard > cap + 64) {
-        r.status = kDecTooLong;
-        break;
-      }
+    int tsel_next = sel[0];
+    const uint16_t *lut = sh.lut[0];
+    for (;;) {
       if (gleft == 0) {
         if (gsel >= nsel) {
           r.status = kDecBadSymbol;
           break;
         }
-        tsel = sel[gsel++];
+        tsel = tsel_next;
+        lut = sh.lut[tsel];
+        gsel++;
+        tsel_next = gsel < nsel ? sel[gsel] : 0;  // next group's table, loaded early
         gleft = 50;
-        __syncwarp();
       }
       gleft--;
       // one symbol with table tsel
       int sym;
-      const uint32_t e = sh.lut[tsel][br.peek(kLutBits)];
+      const uint32_t win = br.peek32();
+      const uint32_t e = lut[win >> (32 - kLutBits)];
       if (e) {
         br.skip((int)(e >> 9));
         sym = (int)(e & 511u);
       } else {
-        int n = sh.minlen[tsel];
-        int code = (int)br.get(n);
+        // longer than the table: the canonical limits from kLutBits + 1 bits
+        int n = max((int)sh.minlen[tsel], kLutBits + 1);
+        int code = (int)(win >> (32 - n));
         while (n <= kDecMaxCode && code > sh.limit[tsel][n]) {
           n++;
-          code = (code << 1) | (int)br.get(1);
+          code = (int)(win >> (32 - n));
         }
-        const int idx = code - sh.base[tsel][n];
-        if (n > kDecMaxCode || idx < 0 || idx >= alpha) {
+        const int idx = n <= kDecMaxCode ? code - sh.base[tsel][n] : -1;
+        if (idx < 0 || idx >= alpha) {
           r.status = kDecBadSymbol;
           break;
         }
+        br.skip(n);
         sym = sh.perm[tsel][idx];
       }
       if (sym <= 1) {  // RUNA / RUNB: bijective base-2 digits, least significant first
@@ -438,24 +443,22 @@ __global__ void __launch_bounds__(32) k_dec_block(const uint32_t *words, int64_t
       }
       // a pending zero run: copies of the list's front entry (no move)
       if (zrun > 0) {
-        if (!push_step(0, zrun)) {
+        if (zrun > (int64_t)(cap - m - pend)) {
           r.status = kDecTooLong;
           break;
         }
+        push_step(0, (int)zrun);
         zrun = 0;
         zbit = 0;
       }
       if (sym == eob) break;
       // value v = sym - 1 >= 1: the entry at list position v moves to the front
       const int v = sym - 1;
-      if (v >= nuse) {
-        r.status = kDecBadSymbol;
+      if (v >= nuse || m + pend >= cap) {
+        r.status = v >= nuse ? kDecBadSymbol : kDecTooLong;
         break;
       }
-      if (!push_step(v, 1)) {
-        r.status = kDecTooLong;
-        break;
-      }
+      push_step(v, 1);
     }
     if (r.status == kDecOk && nst > 0) resolve_batch();
   }
