@@ -327,6 +327,18 @@ def main():
                    "ratio": round(len(lbytes) / n, 5),
                    "size_vs_plain": round(len(lbytes) / len(out), 6),
                    "decoded_prefix_bytes": len(dec), "decoded_prefix_ok": dec == head}
+    # bzip2 1.0.8's block format (block split by RLE1 length, 255-byte runs;
+    # byte-identical to libbz2), split included; checked by decoding a prefix
+    for _ in range(args.warmup):
+        B.compress_device_into(d_in, h_out, 9, B.BZIP2_BLOCKS)
+    zt, zlen = timed(lambda: B.compress_device_into(d_in, h_out, 9, B.BZIP2_BLOCKS))
+    zbytes = bytes(h_out[: min(zlen, 4 << 20)].numpy())
+    zt = max_over_ranks(zt, world)
+    import bz2
+    zdec = bz2.BZ2Decompressor().decompress(zbytes, max_length=8 << 20)
+    bzip2_form = {"MB/s": round(n * world * args.steps / zt / 1e6, 2),
+                  "ratio": round(zlen / n, 5), "size_vs_plain": round(zlen / len(out), 6),
+                  "decoded_prefix_ok": zdec == d_in[: len(zdec)].cpu().numpy().tobytes()}
     dt = max_over_ranks(dt, world)
     value = n * world * args.steps / dt / 1e6
 
@@ -421,7 +433,7 @@ def main():
                        "blocks": int(stats["blocks"]), "ratio": round(ratio, 4)},
             "e2e": e2e, "roofline": roof, "pipeline_roofline": pipeline, "cpu_baseline": cpu,
             "forms": {"plain": round(value, 2), "batched": round(batched_value, 2),
-                      "learned": learned},
+                      "learned": learned, "bzip2_format": bzip2_form},
             "decode": decode,
             "clocks": clk.summary(), "gpu_launches": int(launches),
             "stats": {k: stats[k] for k in ("n", "m", "A", "s", "g", "bits")},

@@ -99,7 +99,7 @@ struct EngineKey {
 };
 std::mutex g_eng_mu;
 std::map<EngineKey, std::unique_ptr<Compressor>> g_engines;
-int g_slab = 128, g_workers = 3;
+int g_slab = 128, g_workers = 5;
 bool g_timing = false;
 thread_local StageTimes g_last_stats;
 

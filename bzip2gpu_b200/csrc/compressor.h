@@ -34,7 +34,7 @@ struct StageTimes {
 
 struct CompressorConfig {
   int slab_blocks = 128;
-  int workers = 3;
+  int workers = 5;
   int64_t max_block_bytes = 900000;
   bool time_stages = false;
   // Learned table selector: packed weights on this engine's device

@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -438,15 +439,34 @@ std::vector<int64_t> bzip2_split(const uint8_t *d_in, int64_t n, int level, cuda
   const int64_t cap = bzip2_split_max_blocks(n, level);
   BZ_REQUIRE(cap < (int64_t)1 << 30, kErrTooLarge, "input too large for the bzip2 split");
   BZ_REQUIRE(T < (int64_t)1 << 31, kErrTooLarge, "input too large for the bzip2 split");
-  // one allocation: fa, la, lb, nf, P (T + 1 each), c, ends, counters
+  // one scratch region per device, kept between calls (grown when too small):
+  // fa, la, lb, nf, P (T + 1 each), c, ends, counters
   const size_t words = 5 * (size_t)(T + 1) + (size_t)(T + 1) / 2 + 1 + (size_t)cap + 2;
-  int64_t *buf = nullptr;
-  BZ_CUDA(cudaMallocAsync((void **)&buf, words * 8, st));
-  struct Free {
-    int64_t *p;
-    cudaStream_t st;
-    ~Free() { cudaFreeAsync(p, st); }
-  } release{buf, st};
+  struct Scratch {
+    std::mutex mu;
+    int64_t *p = nullptr;
+    size_t words = 0;
+  };
+  static std::mutex table_mu;
+  static std::vector<Scratch *> per_device;  // kept for the process lifetime
+  int dev0 = 0;
+  BZ_CUDA(cudaGetDevice(&dev0));
+  Scratch *sc;
+  {
+    std::lock_guard<std::mutex> g(table_mu);
+    if ((int)per_device.size() <= dev0) per_device.resize(dev0 + 1, nullptr);
+    if (!per_device[dev0]) per_device[dev0] = new Scratch();
+    sc = per_device[dev0];
+  }
+  std::lock_guard<std::mutex> hold(sc->mu);  // calls on one device take turns
+  if (sc->words < words) {
+    if (sc->p) BZ_CUDA(cudaFree(sc->p));
+    sc->p = nullptr;
+    sc->words = 0;
+    BZ_CUDA(cudaMalloc((void **)&sc->p, words * 8));
+    sc->words = words;
+  }
+  int64_t *buf = sc->p;
   int64_t *fa = buf, *la = fa + (T + 1), *lb = la + (T + 1), *nf = lb + (T + 1),
           *P = nf + (T + 1);
   int32_t *c = reinterpret_cast<int32_t *>(P + (T + 1));
