@@ -75,13 +75,17 @@ __global__ void __launch_bounds__(256) k_mtf_block_scan(SlabDev d) {
 constexpr int kSub = kTile / 32;      // symbols per lane
 constexpr int kListStride = 264;      // bytes per lane list (8-aligned, bank spread)
 constexpr int kPartStride = kSub + 4;
+// The tile in shared memory: lane l's kSub bytes at l * (kSub + 4), so the 32
+// lanes walking their own slices hit 32 different banks.
+constexpr int kSLaneStride = kSub + 4;
+__device__ __forceinline__ int sl_at(int i) { return i + (i / kSub) * 4; }
 
 __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d) {
   __shared__ __align__(16) int key[256];
-  __shared__ __align__(16) uint8_t sL[kTile];
+  __shared__ __align__(16) uint8_t sL[32 * kSLaneStride];
   __shared__ __align__(16) uint8_t lists[32 * kListStride];
   __shared__ __align__(4) uint8_t part[32 * kPartStride];
-  __shared__ uint32_t pmask[32][8];
+  __shared__ uint32_t pmask[32][9];  // padded row: no bank conflicts across lanes
   __shared__ int pcount[32];
   const int t = blockIdx.x;
   const int b = d.tile_block[t];
@@ -105,7 +109,14 @@ __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d) {
     key[c] = !use ? INT32_MIN : (lp >= 0 ? lp : -1 - c);
   }
   const uint4 *src = reinterpret_cast<const uint4 *>(d.last + off + lt);
-  for (int w = ln; w < (valid + 15) / 16; w += 32) reinterpret_cast<uint4 *>(sL)[w] = src[w];
+  for (int w = ln; w < (valid + 15) / 16; w += 32) {
+    const uint4 v = src[w];
+    uint32_t *d4 = reinterpret_cast<uint32_t *>(sL + sl_at(16 * w));
+    d4[0] = v.x;
+    d4[1] = v.y;
+    d4[2] = v.z;
+    d4[3] = v.w;
+  }
 #pragma unroll
   for (int w = 0; w < 8; w++) pmask[ln][w] = 0;
   __syncwarp();
@@ -132,11 +143,12 @@ __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d) {
   // partial lists
   const int a0 = ln * kSub;
   const int a1 = min(valid, a0 + kSub);
+  uint8_t *mySL = sL + 4 * ln;  // this lane's slice: mySL[i] for i in [a0, a1)
   {
     int cnt = 0;
     uint8_t *pp = part + ln * kPartStride;
     for (int i = a1 - 1; i >= a0; i--) {
-      const int c = sL[i];
+      const int c = mySL[i];
       const uint32_t bit = 1u << (c & 31);
       const uint32_t mw = pmask[ln][c >> 5];
       if (!(mw & bit)) {
@@ -189,7 +201,7 @@ __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d) {
     uint64_t *lw = reinterpret_cast<uint64_t *>(lists + ln * kListStride);
     const uint64_t ones = 0x0101010101010101ull, highs = 0x8080808080808080ull;
     for (int i = a0; i < a1; i++) {
-      const uint32_t c = sL[i];
+      const uint32_t c = mySL[i];
       const uint64_t bc = ones * c;
       uint64_t carry = c;
       int q = 0;
@@ -207,14 +219,17 @@ __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d) {
         lw[wi] = (wv << 8) | carry;
         carry = wv >> 56;
       }
-      sL[i] = (uint8_t)q;
+      mySL[i] = (uint8_t)q;
     }
   }
   __syncwarp();
   uint4 *dst = reinterpret_cast<uint4 *>(d.mtf + off + lt);
   const int full = valid / 16;
-  for (int w = ln; w < full; w += 32) dst[w] = reinterpret_cast<const uint4 *>(sL)[w];
-  for (int i = full * 16 + ln; i < valid; i += 32) d.mtf[off + lt + i] = sL[i];
+  for (int w = ln; w < full; w += 32) {
+    const uint32_t *s4 = reinterpret_cast<const uint32_t *>(sL + sl_at(16 * w));
+    dst[w] = make_uint4(s4[0], s4[1], s4[2], s4[3]);
+  }
+  for (int i = full * 16 + ln; i < valid; i += 32) d.mtf[off + lt + i] = sL[sl_at(i)];
 }
 
 }  // namespace
