@@ -108,34 +108,34 @@ __device__ __forceinline__ uint32_t load16(const uint8_t *in, int64_t n, int64_t
   return s;
 }
 
+// Per-tile kernels: one warp per 4096-byte tile, lane l on bytes
+// 128 l .. 128 l + 127 (eight 16-byte pieces), warp shuffles only.
+constexpr int kLaneBytes = kSplitTile / 32;
+
 // fa[t] / la[t]: first / last run start in tile t (INT64_MAX / -1 if none).
 __global__ void __launch_bounds__(kSplitThreads)
     k_split_runs(const uint8_t *__restrict__ in, int64_t n, int64_t T, int64_t *fa,
                  int64_t *la) {
-  __shared__ int64_t sh[2][2][8];
-  for (int64_t t = blockIdx.x, it = 0; t < T; t += gridDim.x, it++) {
-    const int64_t p0 = t * kSplitTile + threadIdx.x * 16;
-    uint8_t c[16];
-    int nv;
-    const uint32_t s = load16(in, n, p0, c, nv);
-    int64_t f = s ? p0 + __ffs(s) - 1 : INT64_MAX;
-    int64_t l = s ? p0 + 31 - __clz(s) : -1;
+  const int64_t nwarps = (int64_t)gridDim.x * (kSplitThreads / 32);
+  for (int64_t t = (int64_t)blockIdx.x * (kSplitThreads / 32) + warp_id(); t < T; t += nwarps) {
+    const int64_t base = t * kSplitTile + (int64_t)lane_id() * kLaneBytes;
+    int64_t f = INT64_MAX, l = -1;
+#pragma unroll
+    for (int piece = 0; piece < kLaneBytes / 16; piece++) {
+      const int64_t p0 = base + piece * 16;
+      uint8_t c[16];
+      int nv;
+      const uint32_t sm = load16(in, n, p0, c, nv);
+      if (sm) {
+        f = min(f, p0 + __ffs(sm) - 1);
+        l = max(l, p0 + 31 - __clz(sm));
+      }
+    }
     for (int o = 16; o; o >>= 1) {
       f = min(f, (int64_t)__shfl_xor_sync(0xffffffffu, (long long)f, o));
       l = max(l, (int64_t)__shfl_xor_sync(0xffffffffu, (long long)l, o));
     }
-    // double-buffered partials: one barrier per tile
-    int64_t(*buf)[8] = sh[it & 1];
     if (lane_id() == 0) {
-      buf[0][warp_id()] = f;
-      buf[1][warp_id()] = l;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      for (int w = 0; w < kSplitThreads / 32; w++) {
-        f = min(f, buf[0][w]);
-        l = max(l, buf[1][w]);
-      }
       fa[t] = f;
       la[t] = l;
     }
@@ -233,17 +233,36 @@ __device__ __forceinline__ int64_t run_start_in(int64_t p0, uint32_t s, int64_t 
 __global__ void __launch_bounds__(kSplitThreads)
     k_split_count(const uint8_t *__restrict__ in, int64_t n, int64_t T, const int64_t *lb,
                   int32_t *c) {
-  __shared__ int64_t sh[32];
-  for (int64_t t = blockIdx.x; t < T; t += gridDim.x) {
-    const int64_t p0 = t * kSplitTile + threadIdx.x * 16;
-    uint8_t b[16];
-    int nv;
-    const uint32_t s = load16(in, n, p0, b, nv);
-    const int64_t rs0 = run_start_in(p0, s, lb[t], sh);
-    int64_t sum = 0;
-    walk16(p0, nv, s, rs0, [&](int64_t, int64_t, int q) { sum += cnt_of(q); });
-    const int64_t tot = block_scan(sum, sh, SumOp());
-    if (threadIdx.x == kSplitThreads - 1) c[t] = (int32_t)tot;
+  const int64_t nwarps = (int64_t)gridDim.x * (kSplitThreads / 32);
+  for (int64_t t = (int64_t)blockIdx.x * (kSplitThreads / 32) + warp_id(); t < T; t += nwarps) {
+    const int64_t base = t * kSplitTile + (int64_t)lane_id() * kLaneBytes;
+    uint8_t b[kLaneBytes / 16][16];
+    uint32_t sm[kLaneBytes / 16];
+    int nv[kLaneBytes / 16];
+    int64_t last = -1;
+#pragma unroll
+    for (int piece = 0; piece < kLaneBytes / 16; piece++) {
+      sm[piece] = load16(in, n, base + piece * 16, b[piece], nv[piece]);
+      if (sm[piece]) last = base + piece * 16 + 31 - __clz(sm[piece]);
+    }
+    // the run start before this lane's bytes: exclusive max over earlier lanes
+    int64_t inc = last;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t v = __shfl_up_sync(0xffffffffu, (long long)inc, o);
+      if ((int)lane_id() >= o) inc = max(inc, v);
+    }
+    int64_t rs = __shfl_up_sync(0xffffffffu, (long long)inc, 1);
+    if (lane_id() == 0) rs = -1;
+    rs = max(rs, lb[t]);
+    int sum = 0;
+#pragma unroll
+    for (int piece = 0; piece < kLaneBytes / 16; piece++) {
+      const int64_t p0 = base + piece * 16;
+      walk16(p0, nv[piece], sm[piece], rs, [&](int64_t, int64_t, int q) { sum += cnt_of(q); });
+      if (sm[piece]) rs = p0 + 31 - __clz(sm[piece]);
+    }
+    for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (lane_id() == 0) c[t] = sum;
   }
 }
 
@@ -476,7 +495,8 @@ std::vector<int64_t> bzip2_split(const uint8_t *d_in, int64_t n, int level, cuda
   int dev = 0, sms = 0;
   BZ_CUDA(cudaGetDevice(&dev));
   BZ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  const unsigned grid = (unsigned)std::min<int64_t>(T, (int64_t)sms * 8);
+  const unsigned grid =
+      (unsigned)std::min<int64_t>((T + kSplitThreads / 32 - 1) / (kSplitThreads / 32), (int64_t)sms * 8);
   k_split_runs<<<grid, kSplitThreads, 0, st>>>(d_in, n, T, fa, la);
   BZ_LAUNCH_CHECK();
   k_split_scan_runs<<<1, kScanThreads, 0, st>>>(T, n, la, fa, lb, nf);
