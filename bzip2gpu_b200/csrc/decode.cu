@@ -169,10 +169,11 @@ __device__ __forceinline__ void fill_bytes(uint8_t *d, int c, uint8_t v) {
 __global__ void __launch_bounds__(32) k_dec_block(const uint32_t *words, int64_t nwords,
                                                   const int64_t *cand, int ncand,
                                                   DecBlock *out, uint8_t *Lbuf,
-                                                  uint8_t *selbuf, int cap) {
+                                                  uint8_t *selbuf, int cap,
+                                                  const int32_t *order) {
   __shared__ DecShared sh;
-  const int bi = blockIdx.x;
-  if (bi >= ncand) return;
+  if ((int)blockIdx.x >= ncand) return;
+  const int bi = order[blockIdx.x];  // largest compressed blocks first
   const int ln = threadIdx.x;
   DecBlock r;
   r.start = cand[bi];
@@ -925,7 +926,7 @@ struct MallocSink : DecSink {
 // (stream st).
 struct DecWork {
   std::mutex mu;
-  DevBuf words, blk, eos, cnt, cand, db, L, hist, sel, idx, tt, lens, off, crc, ctl, bad,
+  DevBuf words, blk, eos, cnt, cand, order, db, L, hist, sel, idx, tt, lens, off, crc, ctl, bad,
       lanes;
   DevBuf out[2];
   cudaStream_t st = nullptr, cs = nullptr;
@@ -1033,6 +1034,7 @@ void decode_words(DecWork &w, size_t n, DecSink &sink) {
   const int batch = (int)std::min<size_t>(bmax, std::max<size_t>(cands.size(), 1));
   const int cap = kDecCap;
   w.cand.reserve(8 * (size_t)batch);
+  w.order.reserve(4 * (size_t)batch);
   w.db.reserve(sizeof(DecBlock) * (size_t)batch);
   w.L.reserve((size_t)batch * cap);
   w.hist.reserve((size_t)batch * kLfChunks * 256 * 4);
@@ -1059,6 +1061,7 @@ void decode_words(DecWork &w, size_t n, DecSink &sink) {
   size_t ci = 0;
   int nbatch = 0;
   std::vector<DecBlock> hdb(batch);
+  std::vector<int32_t> order;
   // block CRCs of the last batch, checked once st has caught up
   std::vector<uint32_t> want;
   auto settle = [&]() {
@@ -1107,8 +1110,20 @@ void decode_words(DecWork &w, size_t n, DecSink &sink) {
                "bzip2 stream: no block or end-of-stream marker where one must start");
     const int nc = (int)std::min<size_t>(batch, cands.size() - ci);
     BZ_CUDA(cudaMemcpyAsync(w.cand.p, cands.data() + ci, 8 * nc, cudaMemcpyHostToDevice, st));
+    // A launch lasts as long as its slowest blocks: start the largest ones
+    // first (compressed size = distance to the next candidate).
+    order.resize(nc);
+    for (int q = 0; q < nc; q++) order[q] = q;
+    auto csize = [&](int q) {
+      const size_t k = ci + (size_t)q;
+      return (k + 1 < cands.size() ? cands[k + 1] : nbits) - cands[k];
+    };
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return csize(a) > csize(b); });
+    BZ_CUDA(cudaMemcpyAsync(w.order.p, order.data(), 4 * nc, cudaMemcpyHostToDevice, st));
     k_dec_block<<<nc, 32, 0, st>>>(w.words.get<uint32_t>(), nwords, w.cand.get<int64_t>(), nc,
-                                   w.db.get<DecBlock>(), L, w.sel.get<uint8_t>(), cap);
+                                   w.db.get<DecBlock>(), L, w.sel.get<uint8_t>(), cap,
+                                   w.order.get<int32_t>());
     BZ_LAUNCH_CHECK();
     BZ_CUDA(cudaMemcpyAsync(hdb.data(), w.db.p, sizeof(DecBlock) * nc, cudaMemcpyDeviceToHost,
                             st));
