@@ -175,17 +175,23 @@ __global__ void __launch_bounds__(256, kVals ? 2 : 3)
   }
   __syncthreads();
   {
-    // prefix over warps for each digit, then exclusive scan over digits
+    // per digit: its local base (exclusive scan over digits of the tile's
+    // counts); each warp's count becomes that warp's local start for the
+    // digit, and the digit's global base becomes (global - local) base, so
+    // the placement and the write below read one table entry each
     const int dg = threadIdx.x;
     uint32_t run = 0;
-    for (int ww = 0; ww < kSortWarps; ww++) {
-      uint32_t c = wcnt[ww * kRadix + dg];
-      wcnt[ww * kRadix + dg] = run;
-      run += c;
-    }
+    for (int ww = 0; ww < kSortWarps; ww++) run += wcnt[ww * kRadix + dg];
     __shared__ uint32_t scratch[40];
     uint32_t tot;
-    lbase[dg] = block_excl_sum(run, scratch, &tot);
+    const uint32_t lb = block_excl_sum(run, scratch, &tot);
+    uint32_t at = lb;
+    for (int ww = 0; ww < kSortWarps; ww++) {
+      const uint32_t c = wcnt[ww * kRadix + dg];
+      wcnt[ww * kRadix + dg] = at;
+      at += c;
+    }
+    goff[dg] -= lb;
   }
   __syncthreads();
 #pragma unroll
@@ -194,7 +200,7 @@ __global__ void __launch_bounds__(256, kVals ? 2 : 3)
     if (e < valid) {
       const int dg = (int)((key[i] >> shift) & (kRadix - 1));
       const uint32_t r = (i & 1) ? rank2[i >> 1] >> 16 : rank2[i >> 1] & 0xffffu;
-      const uint32_t pos = lbase[dg] + wcnt[w * kRadix + dg] + r;
+      const uint32_t pos = wcnt[w * kRadix + dg] + r;
       sk[pos] = key[i];
       if (kVals) sv[pos] = val[i];
     }
@@ -205,7 +211,7 @@ __global__ void __launch_bounds__(256, kVals ? 2 : 3)
   for (int k = threadIdx.x; k < valid; k += blockDim.x) {
     const uint64_t kk = sk[k];
     const int dg = (int)((kk >> shift) & (kRadix - 1));
-    const uint32_t g = goff[dg] + (uint32_t)k - lbase[dg];
+    const uint32_t g = goff[dg] + (uint32_t)k;
     KO[g] = kk;
     if (kVals) VO[g] = sv[k];
   }
