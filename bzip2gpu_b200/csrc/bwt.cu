@@ -161,8 +161,15 @@ __global__ void __launch_bounds__(256, kVals ? 2 : 3)
   for (int i = 0; i < kTileItems; i++) {
     const int e = w * kWarpSpan + i * 32 + ln;
     const bool ok = e < valid;
-    const int dg = ok ? (int)((key[i] >> shift) & (kRadix - 1)) : kRadix + 1;
-    const unsigned peers = __match_any_sync(0xffffffffu, dg);
+    const int dg = ok ? (int)((key[i] >> shift) & (kRadix - 1)) : 0;
+    // lanes with the same digit: one ballot per digit bit, valid lanes only
+    unsigned peers = __ballot_sync(0xffffffffu, ok);
+#pragma unroll
+    for (int bit = 0; bit < 8; bit++) {
+      const bool on = (dg >> bit) & 1;
+      const unsigned bb = __ballot_sync(0xffffffffu, on);
+      peers &= on ? bb : ~bb;
+    }
     const uint32_t before = ok ? wcnt[w * kRadix + dg] : 0;
     const uint32_t r = before + __popc(peers & lt_mask);
     if (i & 1)
