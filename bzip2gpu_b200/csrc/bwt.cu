@@ -64,6 +64,19 @@ __device__ __forceinline__ int tile_valid(const SlabDev &d, int t, const int32_t
   return v < 0 ? 0 : (v > kTile ? kTile : v);
 }
 
+// The valid lanes of the warp whose 8-bit digit equals this lane's: one
+// ballot per digit bit (cheaper here than __match_any_sync).
+__device__ __forceinline__ unsigned digit_peers(int dg, bool ok) {
+  unsigned peers = __ballot_sync(0xffffffffu, ok);
+#pragma unroll
+  for (int bit = 0; bit < kRadixBits; bit++) {
+    const bool on = (dg >> bit) & 1;
+    const unsigned bb = __ballot_sync(0xffffffffu, on);
+    peers &= on ? bb : ~bb;
+  }
+  return peers;
+}
+
 __global__ void __launch_bounds__(256) k_radix_hist(SlabDev d, int shift, const int32_t *list) {
   __shared__ uint32_t cnt[kRadix];
   const int t = tile_id(list);
@@ -119,7 +132,7 @@ __global__ void __launch_bounds__(256) k_radix_scan(SlabDev d) {
 
 // Stable scatter of one tile by one 8-bit digit.  Elements are warp-striped
 // (lane l, item i <-> element w*512 + i*32 + l) so that ranking item by item
-// with __match_any_sync keeps the original order; the tile is sorted locally
+// over the lanes with equal digits keeps the original order; the tile is sorted locally
 // in shared memory, then written so that equal digits go out contiguously.
 // All of a thread's loads are issued before the ranking starts.
 template <bool kVals>
@@ -162,14 +175,7 @@ __global__ void __launch_bounds__(256, kVals ? 2 : 3)
     const int e = w * kWarpSpan + i * 32 + ln;
     const bool ok = e < valid;
     const int dg = ok ? (int)((key[i] >> shift) & (kRadix - 1)) : 0;
-    // lanes with the same digit: one ballot per digit bit, valid lanes only
-    unsigned peers = __ballot_sync(0xffffffffu, ok);
-#pragma unroll
-    for (int bit = 0; bit < 8; bit++) {
-      const bool on = (dg >> bit) & 1;
-      const unsigned bb = __ballot_sync(0xffffffffu, on);
-      peers &= on ? bb : ~bb;
-    }
+    const unsigned peers = digit_peers(dg, ok);
     const uint32_t before = ok ? wcnt[w * kRadix + dg] : 0;
     const uint32_t r = before + __popc(peers & lt_mask);
     if (i & 1)

@@ -474,7 +474,7 @@ __global__ void __launch_bounds__(32) k_dec_block(const uint32_t *words, int64_t
 // F[j] = L[i]).  A stable counting sort by the byte: per 4096-entry chunk a
 // histogram, per block a scan over chunks (each chunk's start per byte value,
 // C included), then per chunk the ranks of 256 entries at a time: equal bytes
-// in a warp by match_any, earlier warps by shared counts.
+// in a warp by ballots, earlier warps by shared counts.
 constexpr int kLfChunk = 4096;
 constexpr int kLfChunks = (kDecCap + kLfChunk - 1) / kLfChunk;
 
@@ -536,7 +536,14 @@ __global__ void __launch_bounds__(256) k_dec_lf_rank(const int32_t *idx, const D
     const int c = valid ? (int)L[i] : 256 + ln;
     for (int q = threadIdx.x; q < 8 * 256; q += 256) (&wc[0][0])[q] = 0;
     __syncthreads();
-    const unsigned peers = __match_any_sync(0xffffffffu, c);
+    // lanes with the same byte: one ballot per bit (cheaper than match_any)
+    unsigned peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+    for (int bit = 0; bit < 8; bit++) {
+      const bool on = (c >> bit) & 1;
+      const unsigned bb = __ballot_sync(0xffffffffu, on);
+      peers &= on ? bb : ~bb;
+    }
     const int wr = __popc(peers & ((1u << ln) - 1u));
     if (valid && wr == 0) wc[w][c] = __popc(peers);
     __syncthreads();
