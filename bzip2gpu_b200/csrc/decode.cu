@@ -309,7 +309,8 @@ __global__ void __launch_bounds__(32) k_dec_block(const uint32_t *words, int64_t
   //  * lanes that reach position 0 point at that step's lane, the others read
   //    the list as it was before the batch; pointer jumping settles pointers;
   //  * the new list: the batch's distinct outputs, most recent first, then
-  //    the untouched entries in their old order.
+  //    the untouched entries in their old order (equal outputs found by
+  //    ballots).
   for (int p = ln; p < 256; p += 32) sh.list[0][p] = (uint8_t)p;
   __syncwarp();
   int cur = 0;
@@ -345,7 +346,14 @@ __global__ void __launch_bounds__(32) k_dec_block(const uint32_t *words, int64_t
         else ptr = tp;
       }
     }
-    const unsigned peers = __match_any_sync(full, act ? val : 256 + ln);
+    // active lanes with the same output: one ballot per bit of it
+    unsigned peers = __ballot_sync(full, act);
+#pragma unroll
+    for (int bit = 0; bit < 8; bit++) {
+      const bool on = act && ((val >> bit) & 1);
+      const unsigned bb = __ballot_sync(full, on);
+      peers &= on ? bb : ~bb;
+    }
     const unsigned above = ~((2u << ln) - 1u);  // lanes after this one
     const bool last = act && (peers & above) == 0u;
     const unsigned lastm = __ballot_sync(full, last);

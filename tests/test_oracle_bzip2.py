@@ -61,3 +61,19 @@ def test_run_cut_255_differs_from_259_only_on_long_runs():
     assert r255.size == 10 * (5 + 5) and r259.size == 10 * (5 + 5)
     assert list(r255[:10]) == [0, 0, 0, 0, 251, 0, 0, 0, 0, 41]
     assert list(r259[:10]) == [0, 0, 0, 0, 255, 0, 0, 0, 0, 37]
+
+
+@pytest.mark.parametrize("level", [1, 9])
+def test_bzip2_format_bounds_hold(level):
+    # the library's host-side bounds for BZ2G_BZIP2_BLOCKS (no GPU needed):
+    # the stream bound covers the oracle's stream, and the split bound its
+    # block count, on inputs that make many blocks or expand under RLE1
+    import bzip2gpu_b200 as B
+    rng = np.random.default_rng(205)
+    cases = [np.repeat(rng.integers(0, 256, 250000).astype(np.uint8), 4),  # RLE1 expands 5/4
+             rng.integers(0, 256, 600000).astype(np.uint8),
+             np.zeros(3_000_000, np.uint8)]
+    for a in cases:
+        s = O.compress(a, level, O.BZIP2_BLOCKS, threads=4)
+        assert len(s) <= B.compress_bound(a.size, B.BZIP2_BLOCKS)
+        assert O.bzip2_split(a, level).size <= B.lib().bz2g_bzip2_split_bound(a.size, level)
