@@ -42,7 +42,10 @@ int bz2g_version(void);
  * output reaches 100000 * level - 19 bytes, as libbz2 cuts them.  The stream
  * is then byte-identical to libbz2's at the same level, except that a block
  * whose RLE1 output is periodic (equal rotations) may carry another origPtr
- * among the equal rotations, which decodes the same.  No counterpart in the
+ * among the equal rotations, which decodes the same.  The split walks the
+ * whole input, so in this mode a host input is first copied to device memory
+ * whole (it must fit there; the reference format streams slab by slab).
+ * No counterpart in the
  * reference, whose TODO.md:38-40 lists the split as missing and which cuts
  * 900000 raw bytes for every level, src/main.cpp:26,36. */
 #define BZ2G_BZIP2_BLOCKS (-1)
