@@ -9,7 +9,7 @@
 //   2. k_dec_block: one warp per candidate block.  All 32 lanes walk the bit
 //      stream in lockstep (the same reads, so shared-memory tables are read as
 //      broadcasts): header (CRC, origPtr, symbol map, tables, selectors),
-//      Huffman symbols via a 9-bit lookup table with the canonical slow path
+//      Huffman symbols via an 8-bit lookup table with the canonical slow path
 //      for longer codes, RUNA/RUNB zero runs, and the inverse move-to-front
 //      32 MTF steps at a time across the warp.  Out: the BWT last column L.
 //   3. k_dec_lf_hist / _scan / _rank: LF vector
@@ -49,7 +49,7 @@ constexpr int kDecMaxGroups = 6;
 constexpr int kDecMaxAlpha = 258;
 constexpr int kDecMaxCode = 20;
 constexpr int kDecMaxSel = 18002;
-constexpr int kLutBits = 9;
+constexpr int kLutBits = 8;
 // Per-block capacity of the last column (the reference's 900,000-byte raw
 // blocks can exceed 900,000 RLE1 bytes by up to a quarter).
 constexpr int kDecCap = 1200000;
