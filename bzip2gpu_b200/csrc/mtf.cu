@@ -81,12 +81,14 @@ constexpr int kSLaneStride = kSub + 4;
 __device__ __forceinline__ int sl_at(int i) { return i + (i / kSub) * 4; }
 
 __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d) {
-  __shared__ __align__(16) int key[256];
+  // The start keys are read before the partial lists are written, so they
+  // share storage (17.6 KB in all: 12 single-warp blocks per SM).
+  __shared__ __align__(16) uint8_t part_key[32 * kPartStride];
+  int *key = reinterpret_cast<int *>(part_key);  // [256]
+  uint8_t *part = part_key;
   __shared__ __align__(16) uint8_t sL[32 * kSLaneStride];
   __shared__ __align__(16) uint8_t lists[32 * kListStride];
-  __shared__ __align__(4) uint8_t part[32 * kPartStride];
   __shared__ uint32_t pmask[32][9];  // padded row: no bank conflicts across lanes
-  __shared__ int pcount[32];
   const int t = blockIdx.x;
   const int b = d.tile_block[t];
   const int64_t off = d.off[b];
@@ -144,8 +146,9 @@ __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d) {
   const int a0 = ln * kSub;
   const int a1 = min(valid, a0 + kSub);
   uint8_t *mySL = sL + 4 * ln;  // this lane's slice: mySL[i] for i in [a0, a1)
+  __syncwarp();  // every lane has read the start keys
+  int cnt = 0;  // this lane's partial-list length
   {
-    int cnt = 0;
     uint8_t *pp = part + ln * kPartStride;
     for (int i = a1 - 1; i >= a0; i--) {
       const int c = mySL[i];
@@ -156,14 +159,13 @@ __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d) {
         pp[cnt++] = (uint8_t)c;
       }
     }
-    pcount[ln] = cnt;
   }
   __syncwarp();
   // lane lists, in turn: list k = partial(k-1) ++ (list k-1 minus partial(k-1))
   for (int k = 1; k < 32; k++) {
     const uint8_t *prevl = lists + (k - 1) * kListStride;
     uint8_t *cur = lists + k * kListStride;
-    const int pc = pcount[k - 1];
+    const int pc = __shfl_sync(0xffffffffu, cnt, k - 1);
     const uint8_t *pp = part + (k - 1) * kPartStride;
     for (int q = ln; q < pc; q += 32) cur[q] = pp[q];
     uint8_t keepv[8];
