@@ -53,3 +53,24 @@ def test_cli_file_stdout_and_stdin(torch_cuda, tmp_path):
     assert r.returncode == 0 and r.stdout == B.compress(data, 9)
     r = subprocess.run([str(CLI), str(tmp_path / "missing.dat")], capture_output=True, timeout=60)
     assert r.returncode != 0
+
+
+def test_cli_bzip2_format_equals_libbz2(torch_cuda, tmp_path):
+    # BZ2G_BZIP2_FORMAT=1: bzip2 1.0.8's block format, so every level gives
+    # libbz2's own stream (levels 1..8 included)
+    import bz2
+    import os
+    data = np.concatenate([W.small_markov(1500000, seed=74),
+                           np.repeat(np.arange(40, dtype=np.uint8), 700)])
+    src = tmp_path / "g.dat"
+    src.write_bytes(data.tobytes())
+    env = dict(os.environ, BZ2G_BZIP2_FORMAT="1")
+    r = subprocess.run([str(CLI), "-z", "-1", str(src)], capture_output=True, timeout=300, env=env)
+    assert r.returncode == 0, r.stderr
+    assert (tmp_path / "g.dat.bz2").read_bytes() == bz2.compress(data.tobytes(), 1)
+    r = subprocess.run([str(CLI), "-9"], input=data.tobytes(), capture_output=True, timeout=300,
+                       env=env)
+    assert r.returncode == 0 and r.stdout == bz2.compress(data.tobytes(), 9)
+    r = subprocess.run([str(CLI), str(tmp_path / "missing.dat")], capture_output=True, timeout=60,
+                       env=env)
+    assert r.returncode != 0
