@@ -221,7 +221,11 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
   int64_t ntot = 0;
   for (int b = 0; b < nblocks; b++) {
     BZ_REQUIRE(lens[b] > 0 && lens[b] <= raw_max, kErrArg,
-               "block length outside (0, max_block_bytes]");
+               cfg_.m_cap > 0
+                   ? "block of " + std::to_string(lens[b]) +
+                         " raw bytes exceeds a slab's raw capacity of " +
+                         std::to_string(raw_max) + " bytes (raise slab_blocks)"
+                   : std::string("block length outside (0, max_block_bytes]"));
     ntot += lens[b];
   }
   if (level < 1) level = 1;
