@@ -22,7 +22,8 @@
 //      computes each block's CRC over its output (4096-byte chunks combined
 //      over GF(2)), checked against the header.
 // Batches of blocks go through steps 2-5 while the previous batch's bytes are
-// copied out on a second stream.
+// copied out on a second stream; within a batch the largest compressed blocks
+// start first, since a launch lasts as long as its slowest blocks.
 // Every field read from the stream is range-checked and every loop is bounded,
 // so a malformed stream gives an error status, not a fault.
 #include <cuda_runtime.h>
@@ -283,7 +284,8 @@ __global__ void __launch_bounds__(32) k_dec_block(const uint32_t *words, int64_t
   }
   __syncwarp();
   if (r.status == kDecOk) {
-    // lookup tables: every 10-bit prefix that starts a code of length <= 10
+    // lookup tables: every kLutBits-bit prefix that starts a code of at most
+    // kLutBits bits
     for (int t = 0; t < ng; t++) {
       for (int p = ln; p < (1 << kLutBits); p += 32) {
         uint16_t e = 0;
