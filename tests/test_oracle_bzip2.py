@@ -77,3 +77,17 @@ def test_bzip2_format_bounds_hold(level):
         s = O.compress(a, level, O.BZIP2_BLOCKS, threads=4)
         assert len(s) <= B.compress_bound(a.size, B.BZIP2_BLOCKS)
         assert O.bzip2_split(a, level).size <= B.lib().bz2g_bzip2_split_bound(a.size, level)
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_oracle_bzip2_mode_random_runs_equal_libbz2(seed):
+    # run lengths around the 4-byte threshold and the 255-byte cut, mixed
+    # with literals, so block cuts land inside and next to long runs
+    rng = np.random.default_rng(300 + seed)
+    n_runs = int(rng.integers(20000, 60000))
+    lens = rng.choice([1, 2, 3, 4, 5, 254, 255, 256, 259, 300, 510, 511, 1000],
+                      size=n_runs, p=[.3, .15, .1, .1, .05, .04, .04, .04, .04, .04, .04, .03, .03])
+    vals = rng.integers(0, int(rng.integers(2, 256)), n_runs).astype(np.uint8)
+    a = np.repeat(vals, lens)
+    level = int(rng.integers(1, 4))
+    assert O.compress(a, level, O.BZIP2_BLOCKS, threads=4) == bz2.compress(a.tobytes(), level)
