@@ -103,3 +103,19 @@ def test_large_markov_stream(torch_cuda):
     a = d.cpu().numpy()
     s = B.compress_device(d, 9, B.BZIP2_BLOCKS)
     assert s == bz2.compress(a.tobytes(), 9)
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_random_runs_equal_libbz2(torch_cuda, seed):
+    # run lengths around the 4-byte threshold and the 255-byte cut, so block
+    # cuts land inside and next to long runs (small blocks: levels 1-3)
+    rng = np.random.default_rng(300 + seed)
+    n_runs = int(rng.integers(20000, 60000))
+    lens = rng.choice([1, 2, 3, 4, 5, 254, 255, 256, 259, 300, 510, 511, 1000],
+                      size=n_runs, p=[.3, .15, .1, .1, .05, .04, .04, .04, .04, .04, .04, .03, .03])
+    vals = rng.integers(0, int(rng.integers(2, 256)), n_runs).astype(np.uint8)
+    a = np.repeat(vals, lens)
+    level = int(rng.integers(1, 4))
+    d = torch_cuda.from_numpy(a.copy()).cuda()
+    assert np.array_equal(B.bzip2_split(d, level), O.bzip2_split(a, level))
+    assert B.compress(a, level, B.BZIP2_BLOCKS) == bz2.compress(a.tobytes(), level)
