@@ -135,3 +135,18 @@ def test_rle1_segments_with_ambiguous_states(torch_cuda, seed):
     b = np.concatenate([np.full(L, L % 251, np.uint8) for L in range(1, 600)])
     assert B.decompress(B.compress(b, 9)) == b.tobytes()
     assert B.decompress(bz2.compress(b.tobytes(), 1)) == b.tobytes()
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_libbz2_run_heavy_streams(torch_cuda, seed):
+    # run lengths around 4, 255 and 259 mixed with literals: long RUNA/RUNB
+    # zero runs, MTF batches of repeats, RLE1 count bytes near 255
+    rng = np.random.default_rng(400 + seed)
+    n_runs = int(rng.integers(20000, 60000))
+    lens = rng.choice([1, 2, 3, 4, 5, 254, 255, 256, 259, 300, 510, 1000],
+                      size=n_runs, p=[.3, .15, .1, .1, .05, .05, .05, .04, .04, .04, .04, .04])
+    vals = rng.integers(0, int(rng.integers(2, 256)), n_runs).astype(np.uint8)
+    a = np.repeat(vals, lens)
+    for level in (1, 9):
+        assert B.decompress(bz2.compress(a.tobytes(), level)) == a.tobytes()
+        assert B.decompress(B.compress(a, level)) == a.tobytes()
