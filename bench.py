@@ -12,6 +12,10 @@ compresses the whole stream to a complete .bz2 stream.
   e2e    MB/s through bz2g_compress_into with input and output in page-locked
          host memory: the host->device copy of every input byte and the
          device->host copy of the stream are inside the timed region.
+After the timed regions (unless --no-check): the whole plain stream is
+compared byte for byte with the oracle's stream of the same input, and the
+whole learned-form and bzip2-format streams are decoded by libbz2 (every
+block) and compared with the input ("checks" in the JSON line).
 Under torchrun each rank compresses its own stream (weak scaling, no
 collective on the data path); times are the max over ranks.
 --impl reference times the reference path's CPU implementation (the oracle
@@ -130,28 +134,35 @@ def barrier(world: int):
         dist.barrier()
 
 
-def cpu_sample_time(host, nbytes: int, threads: int):
+def cpu_sample_time(host, threads: int):
     import oracle
     t = time.perf_counter()
-    out = oracle.compress(host[:nbytes], 9, 900000, threads=threads)
+    out = oracle.compress(host, 9, 900000, threads=threads)
     return time.perf_counter() - t, len(out)
 
 
+CPU_SAMPLE_NOTE = ("the first 1,800,000 bytes (two blocks) of each of the stream's 64 MiB "
+                   "segments, so every parameter redraw is in the sample")
+
+
 def run_reference(args):
-    """The reference path on the host cores (oracle port), bounded sample."""
+    """The reference path on the host cores (the oracle port of its
+    semantics), on a bounded sample of the same stream.  Nothing of the
+    product library is loaded: the sample comes from the oracle's generator,
+    whose bytes a CPU test pins to the product generator's."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import bzip2gpu_b200.workloads as W
+    import oracle
     threads = os.cpu_count() or 1
-    sample = min(args.size, args.cpu_sample)
-    host = W.large_stream(sample, device=False)
+    host = oracle.large_stream_sample(args.size)
+    sample = host.size
     for _ in range(args.warmup):
-        cpu_sample_time(host, min(sample, 8 << 20), threads)
+        cpu_sample_time(host[: 8 << 20], threads)
     times = []
     for _ in range(args.steps):
-        dt, _ = cpu_sample_time(host, sample, threads)
+        dt, _ = cpu_sample_time(host, threads)
         times.append(dt)
     tot = sum(times)
     mbps = sample * len(times) / tot / 1e6
@@ -160,12 +171,12 @@ def run_reference(args):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(tot / len(times) * 1e3, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample_bytes": sample, "block_bytes": 900000,
-                   "level": 9},
+        "config": {"workload": WORKLOAD, "bytes_per_rank": args.size, "sample_bytes": sample,
+                   "block_bytes": 900000, "level": 9},
         "cpu_baseline": {"value": round(mbps, 2), "unit": "MB/s", "cores": threads,
                          "kind": "port",
-                         "sample": f"first {sample} bytes of the large Markov stream, "
-                                   f"{threads} threads, one block per thread"},
+                         "sample": f"{sample} bytes: {CPU_SAMPLE_NOTE}; {threads} threads, "
+                                   f"one block per thread"},
         "e2e": {"value": round(mbps, 2), "unit": "MB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -247,8 +258,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--size", type=int, default=10 << 30)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-sample", type=int, default=256 << 20)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-check", action="store_true",
+                    help="skip the whole-stream parity and round-trip checks")
     ap.add_argument("--slab", type=int, default=0)
     ap.add_argument("--workers", type=int, default=0)
     ap.add_argument("--workload", default="large", choices=["large", "batch"])
@@ -325,25 +337,18 @@ def main():
         finally:
             B.set_selector("plain")
         lt = max_over_ranks(lt, world)
-        import bz2
-        dec = bz2.BZ2Decompressor().decompress(lbytes[: 4 << 20], max_length=8 << 20)
-        head = d_in[: len(dec)].cpu().numpy().tobytes()
         learned = {"MB/s": round(n * world * args.steps / lt / 1e6, 2),
                    "ratio": round(len(lbytes) / n, 5),
-                   "size_vs_plain": round(len(lbytes) / len(out), 6),
-                   "decoded_prefix_bytes": len(dec), "decoded_prefix_ok": dec == head}
+                   "size_vs_plain": round(len(lbytes) / len(out), 6)}
     # bzip2 1.0.8's block format (block split by RLE1 length, 255-byte runs;
     # byte-identical to libbz2), split included; checked by decoding a prefix
     for _ in range(args.warmup):
         B.compress_device_into(d_in, h_out, 9, B.BZIP2_BLOCKS)
     zt, zlen = timed(lambda: B.compress_device_into(d_in, h_out, 9, B.BZIP2_BLOCKS))
-    zbytes = bytes(h_out[: min(zlen, 4 << 20)].numpy())
+    zbytes = bytes(h_out[:zlen].numpy())
     zt = max_over_ranks(zt, world)
-    import bz2
-    zdec = bz2.BZ2Decompressor().decompress(zbytes, max_length=8 << 20)
     bzip2_form = {"MB/s": round(n * world * args.steps / zt / 1e6, 2),
-                  "ratio": round(zlen / n, 5), "size_vs_plain": round(zlen / len(out), 6),
-                  "decoded_prefix_ok": zdec == d_in[: len(zdec)].cpu().numpy().tobytes()}
+                  "ratio": round(zlen / n, 5), "size_vs_plain": round(zlen / len(out), 6)}
     dt = max_over_ranks(dt, world)
     value = n * world * args.steps / dt / 1e6
 
@@ -356,7 +361,7 @@ def main():
         torch.cuda.synchronize()
         B.compress_into(h_in, h_out, 9)  # warm the host path
         dte, oute = timed(lambda: B.compress_into(h_in, h_out, 9))
-        assert bytes(h_out[:64].numpy()) == out[:64]
+        assert oute == len(out) and bytes(h_out[:oute].numpy()) == out
         # the GPU decoder on the same stream (every block CRC and the stream
         # CRC are checked by the decoder): device-resident (stream and output
         # in HBM) and end to end (pinned host stream in, pinned host bytes out)
@@ -389,9 +394,36 @@ def main():
         e2e = {"value": round(n * world * args.steps / dte / 1e6, 2), "unit": "MB/s",
                "h2d_bytes_per_step": n, "d2h_bytes_per_step": int(oute),
                "api": "bz2g_compress_into (pinned host input and output)"}
-        host_sample = h_in[: min(n, args.cpu_sample)].numpy()
+        host = h_in.numpy()
     else:
-        host_sample = d_in[: min(n, args.cpu_sample)].cpu().numpy()
+        host = d_in.cpu().numpy()
+
+    # Whole-stream checks (outside the timed regions): the plain stream equals
+    # the oracle's stream of the same input byte for byte, and the learned and
+    # bzip2-format streams decode to the input through libbz2, every block
+    # (each re-wrapped as a stream of its own, decoded on all host threads);
+    # the learned stream also through this library's GPU decoder.
+    checks = None
+    if not args.no_check:
+        import oracle
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        identical = oracle.compress(host, 9, 900000, threads=threads) == out
+        checks = {"parity": {"bytes": n, "stream_bytes": len(out), "identical": bool(identical),
+                             "against": f"oracle port of the reference path, {threads} threads",
+                             "seconds": round(time.perf_counter() - t0, 1)}}
+        if learned is not None:
+            rt = oracle.libbz2_matches(lbytes, host, threads)
+            dec = memoryview(B.decompress(lbytes))
+            rt["gpu_decoder_identical"] = len(dec) == n and all(
+                dec[i:i + (1 << 28)] == host[i:i + (1 << 28)].tobytes()
+                for i in range(0, n, 1 << 28))
+            del dec
+            learned["round_trip"] = bool(rt["identical"] and rt["gpu_decoder_identical"])
+            checks["learned_round_trip"] = rt
+        rt = oracle.libbz2_matches(zbytes, host, threads)
+        bzip2_form["round_trip"] = bool(rt["identical"])
+        checks["bzip2_format_round_trip"] = rt
 
     peak, peak_kind = peaks()
     mb = B.model_bytes(stats)
@@ -424,12 +456,13 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1:
+        import oracle
         threads = os.cpu_count() or 1
-        sample = host_sample.size
-        cpu_dt, _ = cpu_sample_time(host_sample, sample, threads)
-        cpu = {"value": round(sample / cpu_dt / 1e6, 2), "unit": "MB/s", "cores": threads,
+        sample = oracle.large_stream_sample(n, seed=seed)
+        cpu_dt, _ = cpu_sample_time(sample, threads)
+        cpu = {"value": round(sample.size / cpu_dt / 1e6, 2), "unit": "MB/s", "cores": threads,
                "kind": "port",
-               "sample": f"first {sample} bytes of the same stream, oracle port of the "
+               "sample": f"{sample.size} bytes: {CPU_SAMPLE_NOTE}; oracle port of the "
                          f"reference path, {threads} threads"}
 
     if rank == 0:
@@ -447,7 +480,7 @@ def main():
             "e2e": e2e, "roofline": roof, "pipeline_roofline": pipeline, "cpu_baseline": cpu,
             "forms": {"plain": round(value, 2), "batched": round(batched_value, 2),
                       "learned": learned, "bzip2_format": bzip2_form},
-            "decode": decode,
+            "decode": decode, "checks": checks,
             "clocks": clk.summary(), "gpu_launches": int(launches),
             "stats": {k: stats[k] for k in ("n", "m", "A", "s", "g", "bits")},
             "stage_ms_sum_over_slabs_last_step": stage_ms,

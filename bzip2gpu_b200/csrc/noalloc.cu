@@ -10,6 +10,7 @@
 // the same ones bz2g_rle1 runs.
 #include <cstring>
 #include <map>
+#include <utility>
 #include <mutex>
 #include <string>
 
@@ -40,29 +41,61 @@ constexpr size_t kNoAllocBytes = kOffScalars + 256;
 
 static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocBytes];
 
-// Set-up, once per device with that device current: the device address of
-// the scratch (the host-side symbol is only a stand-in and must not be
-// passed to a kernel).
-std::mutex g_mu;
-std::map<int, uint8_t *> g_addr;
+// Set-up, once per device context with that device current: the device
+// address of the scratch (the host-side symbol is only a stand-in and must
+// not be passed to a kernel).  The address is kept per (device, context), so
+// a context that was torn down and created again (cudaDeviceReset) gets a
+// fresh lookup instead of a stale address.  The current context comes from
+// the driver's cuCtxGetCurrent, reached through the runtime's entry-point
+// query so that the library needs no link to the driver library.
+using CtxGetCurrentFn = int (*)(void **);
 
-uint8_t *scratch_address() {
-  int dev = 0;
-  BZ_CUDA(cudaGetDevice(&dev));
-  std::lock_guard<std::mutex> g(g_mu);
-  auto it = g_addr.find(dev);
-  if (it != g_addr.end()) return it->second;
+void *current_context() {
+  static CtxGetCurrentFn fn = [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      f = nullptr;
+    }
+    return reinterpret_cast<CtxGetCurrentFn>(f);
+  }();
+  void *ctx = nullptr;
+  if (fn && fn(&ctx) != 0) ctx = nullptr;
+  return ctx;
+}
+
+std::mutex g_mu;
+std::map<std::pair<int, void *>, uint8_t *> g_addr;
+
+uint8_t *lookup_scratch() {
   void *p = nullptr;
   cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
   if (e != cudaSuccess)
     throw Error(kErrCuda, std::string("cudaGetSymbolAddress(g_noalloc_scratch) failed: ") +
                               cudaGetErrorString(e));
-  g_addr[dev] = static_cast<uint8_t *>(p);
   return static_cast<uint8_t *>(p);
 }
 
+uint8_t *scratch_address() {
+  int dev = 0;
+  BZ_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(g_mu);
+  void *ctx = current_context();
+  if (ctx) {
+    auto it = g_addr.find({dev, ctx});
+    if (it != g_addr.end()) return it->second;
+  }
+  // the lookup itself makes the device's context current if it was not yet
+  uint8_t *p = lookup_scratch();
+  ctx = current_context();
+  if (ctx) g_addr[{dev, ctx}] = p;
+  return p;
+}
+
 // One-block plan for n input bytes, written into the scratch.
-__global__ void k_noalloc_plan(uint8_t *base, int n, int64_t cap) {
+__global__ void k_noalloc_plan(uint8_t *base, int n) {
   int64_t *p64 = reinterpret_cast<int64_t *>(base + kOffPlan64);
   int32_t *p32 = reinterpret_cast<int32_t *>(base + kOffPlan32);
   int32_t *rt_block = reinterpret_cast<int32_t *>(base + kOffRtBlock);
@@ -75,7 +108,7 @@ __global__ void k_noalloc_plan(uint8_t *base, int n, int64_t cap) {
   if (threadIdx.x == 0) {
     p64[0] = 0;                                     // raw_off
     p64[1] = 0;                                     // off
-    p64[2] = cap;                                   // cap
+    p64[2] = 0;                                     // cap (unused by RLE1)
     p32[0] = n;                                     // raw_len
     p32[1] = 0;                                     // rt_first[0]
     p32[2] = nt;                                    // rt_first[1]
@@ -126,7 +159,7 @@ extern "C" int bz2g_rle1_noalloc(const uint8_t *d_in, int n, uint8_t *d_out, int
     d.crc_acc = reinterpret_cast<uint32_t *>(base + kOffScalars + 8);
     d.rle1 = d_out;  // written in place: off[0] == 0
     BZ_CUDA(cudaMemcpyAsync(d.raw, d_in, (size_t)n, cudaMemcpyDeviceToDevice, st));
-    k_noalloc_plan<<<1, 256, 0, st>>>(base, n, align_up(rle1_bound(n), kTile));
+    k_noalloc_plan<<<1, 256, 0, st>>>(base, n);
     BZ_LAUNCH_CHECK();
     stage_rle1_crc(d, st);
     int h_m = 0;

@@ -137,10 +137,12 @@ int bz2g_rle1(const uint8_t *d_in, int n, uint8_t *d_out, int *m, void *stream);
  * every GPU that loads the library until the process exits), so n is at
  * most 1048576 bytes (BZ2G_ERR_TOO_LARGE beyond, with a message in
  * bz2g_last_error).  d_out holds bz2g_rle1_bound(n) bytes.  The first call on
- * a device looks up the array's device address (cudaGetSymbolAddress); make
- * that first call before any stream capture.  Calls share the array: calls
- * that overlap on the GPU (for example on two streams) race, so serialise
- * them. */
+ * a device (or on a device context created anew) looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture begins.  Each call waits for its stream to finish the work before
+ * it returns, since *m is read back to the host.  Calls share the array:
+ * calls that overlap on the GPU (for example from two host threads on two
+ * streams) race, so serialise them. */
 int bz2g_rle1_noalloc(const uint8_t *d_in, int n, uint8_t *d_out, int *m, void *stream);
 
 /* bzip2 block CRC of n device bytes.

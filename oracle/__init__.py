@@ -35,7 +35,8 @@ class BlockInfo(ctypes.Structure):
 
 def build() -> Path:
     if not LIB.exists() or LIB.stat().st_mtime < max(
-            (HERE / f).stat().st_mtime for f in ("bz2_oracle.c", "bz2_oracle.h")):
+            (HERE / f).stat().st_mtime
+            for f in ("bz2_oracle.c", "bz2_oracle.h", "gen_oracle.c", "blocks.c")):
         subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
     return LIB
 
@@ -79,6 +80,14 @@ def lib():
         L.orc_bzip2_split.argtypes = [_vp, ctypes.c_int64, _i, _vp, ctypes.c_int64]
         L.orc_compress_bound.restype = ctypes.c_int64
         L.orc_compress_bound.argtypes = [ctypes.c_int64, _i]
+        L.orc_gen_markov.argtypes = [ctypes.c_uint64, _vp, _i, ctypes.c_double, ctypes.c_double,
+                                     _i, _i, _vp, ctypes.c_int64, _i]
+        L.orc_gen_uniform.argtypes = [ctypes.c_uint64, _vp, ctypes.c_int64, _i]
+        L.orc_scan_magic.restype = ctypes.c_int64
+        L.orc_scan_magic.argtypes = [_vp, ctypes.c_int64, _i, _vp, ctypes.c_int64, _i]
+        L.orc_rewrap_block.restype = ctypes.c_int64
+        L.orc_rewrap_block.argtypes = [_vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, _i,
+                                       _vp]
         _lib = L
     return _lib
 
@@ -309,3 +318,131 @@ def assemble(parts, bits, folds, nblocks, level: int = 9) -> bytes:
                            out.ctypes.data, cap)
     return out[:n].tobytes()
 
+
+
+# ------------------------------------------------------------ workload bytes
+def _threads(threads):
+    import os
+    return threads if threads else (os.cpu_count() or 1)
+
+
+def gen_markov(n: int, seed: int, alphabet, alpha: float, p_run: float, run_min: int,
+               run_max: int, threads: int = 0) -> np.ndarray:
+    """Order-1 Markov bytes with run starts (definition in gen_oracle.c)."""
+    alph = np.ascontiguousarray(alphabet, dtype=np.uint8)
+    out = np.empty(n, np.uint8)
+    if lib().orc_gen_markov(seed & (2**64 - 1), alph.ctypes.data, alph.size, alpha, p_run,
+                            run_min, run_max, out.ctypes.data, n, _threads(threads)) != 0:
+        raise ValueError("gen_markov: bad arguments")
+    return out
+
+
+def gen_uniform(n: int, seed: int, threads: int = 0) -> np.ndarray:
+    out = np.empty(n, np.uint8)
+    if lib().orc_gen_uniform(seed & (2**64 - 1), out.ctypes.data, n, _threads(threads)) != 0:
+        raise ValueError("gen_uniform: bad arguments")
+    return out
+
+
+SEGMENT = 64 << 20
+
+
+def large_stream_segments(n: int, seed: int = 0xB2C4):
+    """Parameters of the large Markov stream's 64 MiB segments: (seed,
+    alphabet, alpha) per segment, drawn from numpy's PCG64 with `seed`: an
+    alphabet size uniform in 2..256 (a random subset of the byte values,
+    ascending) and alpha log-uniform in 0.05..5."""
+    import math
+    rng = np.random.default_rng(seed)
+    res = []
+    for k in range((n + SEGMENT - 1) // SEGMENT):
+        a = int(rng.integers(2, 257))
+        alph = np.sort(rng.choice(256, a, replace=False)).astype(np.uint8)
+        alpha = float(math.exp(rng.uniform(math.log(0.05), math.log(5.0))))
+        res.append((seed * 1000003 + k, alph, alpha))
+    return res
+
+
+def large_stream(n: int, seed: int = 0xB2C4, threads: int = 0) -> np.ndarray:
+    """The first n bytes of the large Markov stream (2 % run starts of length
+    4..300, parameters redrawn every 64 MiB)."""
+    out = np.empty(n, np.uint8)
+    for k, (sseed, alph, alpha) in enumerate(large_stream_segments(n, seed)):
+        a, b = k * SEGMENT, min(n, (k + 1) * SEGMENT)
+        out[a:b] = gen_markov(b - a, sseed, alph, alpha, 0.02, 4, 300, threads)
+    return out
+
+
+def large_stream_sample(n: int, per_segment: int = 1_800_000, seed: int = 0xB2C4,
+                        threads: int = 0) -> np.ndarray:
+    """A bounded sample of the n-byte large Markov stream that covers every
+    one of its parameter redraws: the first `per_segment` bytes of each 64 MiB
+    segment (two 900,000-byte blocks by default), back to back.  These are
+    the stream's own bytes: a segment's chains do not depend on its length."""
+    parts = []
+    for k, (sseed, alph, alpha) in enumerate(large_stream_segments(n, seed)):
+        seg = min(n, (k + 1) * SEGMENT) - k * SEGMENT
+        parts.append(gen_markov(min(per_segment, seg), sseed, alph, alpha, 0.02, 4, 300, threads))
+    return np.concatenate(parts) if parts else np.zeros(0, np.uint8)
+
+
+# ------------------------------------------------- libbz2 decode, in parallel
+def _scan(s: np.ndarray, kind: int, threads: int) -> np.ndarray:
+    n = lib().orc_scan_magic(s.ctypes.data, s.size, kind, None, 0, threads)
+    out = np.zeros(max(n, 1), np.int64)
+    lib().orc_scan_magic(s.ctypes.data, s.size, kind, out.ctypes.data, n, threads)
+    return out[:n]
+
+
+def block_bounds(stream, threads: int = 0):
+    """(start bit, end bit) of every block of a single .bz2 stream: from each
+    block magic to the next one, the last to the end-of-stream magic."""
+    s = _u8(stream)
+    t = _threads(threads)
+    starts = _scan(s, 0, t)
+    eos = _scan(s, 1, t)
+    if eos.size == 0:
+        raise ValueError("no end-of-stream marker")
+    end = int(eos[-1])
+    starts = starts[starts < end]
+    ends = np.append(starts[1:], end)
+    return list(zip(starts.tolist(), ends.tolist()))
+
+
+def rewrap_block(stream, b0: int, b1: int, level: int) -> bytes:
+    s = _u8(stream)
+    out = np.zeros((b1 - b0) // 8 + 32, np.uint8)
+    k = lib().orc_rewrap_block(s.ctypes.data, s.size, b0, b1, level, out.ctypes.data)
+    return out[:k].tobytes()
+
+
+def libbz2_matches(stream, expect, threads: int = 0) -> dict:
+    """Decode every block of `stream` with libbz2 (each block re-wrapped as a
+    stream of its own, blocks on `threads` threads) and compare the
+    concatenated output with `expect` (a host array).  A block magic that is
+    really payload bits makes two blocks fail to decode, so the result also
+    reports a mismatch then."""
+    import bz2
+    from concurrent.futures import ThreadPoolExecutor
+
+    s = _u8(stream)
+    e = _u8(expect)
+    level = int(s[3]) - 48
+    bounds = block_bounds(s, threads)
+
+    def dec(bb):
+        try:
+            return bz2.decompress(rewrap_block(s, bb[0], bb[1], level))
+        except (OSError, ValueError):
+            return None
+
+    at, ok = 0, True
+    with ThreadPoolExecutor(_threads(threads)) as ex:
+        for d in ex.map(dec, bounds):
+            if d is None or not ok:
+                ok = False
+                continue
+            if d != e[at:at + len(d)].tobytes():
+                ok = False
+            at += len(d)
+    return {"blocks": len(bounds), "bytes": at, "identical": bool(ok and at == e.size)}

@@ -234,3 +234,22 @@ def test_config1_stress_stream_bit_exact(torch_cuda):
     long_blocks = sum(oracle.rle1(a[i:i + 900000]).size > 900000 for i in range(0, a.size, 900000))
     print(f"config 1: {len(got)} bytes, {long_blocks} blocks with RLE1 output > 900,000 bytes")
     assert long_blocks > 0
+
+
+def test_config4_large_stream_slice_bit_exact(torch_cuda):
+    # config 4 (the large Markov stream): its first 600 MiB span ten of the
+    # 64 MiB parameter redraws, among them segment 1 (66 symbols, alpha
+    # 0.061: deep, low-entropy blocks) and block borders that straddle the
+    # redraws.  The device stream must equal the oracle's byte for byte, and
+    # the input here comes from the oracle's own generator, pinned to the
+    # device generator's bytes.
+    import os
+    n = 600 << 20
+    segs = oracle.large_stream_segments(n)
+    assert len(segs) == 10 and min(al for _, _, al in segs) < 0.1
+    host = oracle.large_stream(n)
+    d = W.large_stream(n, device=True)
+    assert torch_cuda.equal(d[-(1 << 20):].cpu(), torch_cuda.from_numpy(host[-(1 << 20):]))
+    got = B.compress_device(d, 9)
+    ref = oracle.compress(host, 9, threads=os.cpu_count() or 8)
+    assert got == ref

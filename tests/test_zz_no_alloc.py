@@ -31,18 +31,34 @@ def _noalloc(torch, d_in):
     return rc, out[: max(m.value, 0)], m.value
 
 
+def _call(torch, d_in, out):
+    m = ctypes.c_int(-1)
+    rc = _fn()(d_in.data_ptr(), d_in.numel(), out.data_ptr(), ctypes.byref(m),
+               torch.cuda.current_stream().cuda_stream)
+    return rc, m.value
+
+
 def test_noalloc_matches_allocating_entry_point_twice(torch_cuda):
     torch = torch_cuda
     inputs = [W.small_markov(1 << 20, seed=41),                       # at the size limit
               np.concatenate([np.full(300000, 7), np.arange(777) % 3,
                               np.full(1037, 9)]).astype(np.uint8)]     # long runs, smaller
-    for a in inputs:  # two calls in a row share (and must clear) the scratch
-        d_in = torch.from_numpy(a).cuda()
-        rc, got, m = _noalloc(torch, d_in)
+    d_ins = [torch.from_numpy(a).cuda() for a in inputs]
+    refs = [B.rle1(d) for d in d_ins]
+    outs = [torch.full((B.lib().bz2g_rle1_bound(d.numel()),), 0xAA, dtype=torch.uint8,
+                       device="cuda") for d in d_ins]
+    # set-up call (the scratch's address; the library's kernels loaded)
+    assert _call(torch, d_ins[1], outs[1])[0] == 0, B.lib().bz2g_last_error()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    res = [_call(torch, d, o) for d, o in zip(d_ins, outs)]  # two calls in a row
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 >= free0, f"device memory taken during the calls: {free0 - free1} bytes"
+    for (rc, m), ref, o in zip(res, refs, outs):
         assert rc == 0, B.lib().bz2g_last_error()
-        ref = B.rle1(d_in)
         assert m == ref.numel()
-        assert torch.equal(got, ref)
+        assert torch.equal(o[:m], ref)
 
 
 def test_noalloc_rejects_inputs_over_the_limit(torch_cuda):
