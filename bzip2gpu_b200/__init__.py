@@ -83,6 +83,7 @@ _SIGS = {
     "bz2g_set_selector": (_i, [_i]),
     "bz2g_get_selector": (_i, []),
     "bz2g_selector_logits": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
+    "bz2g_selector_wait_check": (_i, [_vp, _i, _vp, _c.c_uint64, _i, _vp]),
     "bz2g_huffman_build_learned": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _c.POINTER(_i),
                                         _c.POINTER(_i), _vp]),
     "bz2g_selector_dataset": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _c.c_int64,
@@ -503,6 +504,19 @@ def selector_logits(d_syms, d_params, stream=None):
     _check(lib().bz2g_selector_logits(_ptr(d_syms), s, _ptr(d_params), _ptr(lg), _ptr(sel),
                                       _stream(stream)))
     return lg, sel
+
+
+ERR_TIMEOUT = 6
+
+
+def selector_wait_check(d_syms, d_params, wait_limit_ns: int, withhold_weights: bool,
+                        stream=None) -> None:
+    """Failure-path check of the tensor-core selector kernel: every wait in
+    it bounded by wait_limit_ns; withhold_weights makes the waits for the
+    weights run out.  Raises Bz2gError (code ERR_TIMEOUT) when a wait ran out."""
+    _check(lib().bz2g_selector_wait_check(_ptr(d_syms), d_syms.numel(), _ptr(d_params),
+                                          int(wait_limit_ns), int(bool(withhold_weights)),
+                                          _stream(stream)))
 
 
 def huffman_build_learned(d_syms, n_in_use: int, d_params, stream=None):

@@ -710,6 +710,34 @@ int bz2g_selector_logits(const uint16_t *d_syms, int s, const float *d_params, f
   });
 }
 
+int bz2g_selector_wait_check(const uint16_t *d_syms, int s, const float *d_params,
+                             uint64_t wait_limit_ns, int withhold_weights, void *stream) {
+  return guard([&] {
+    BZ_REQUIRE(s > 0 && d_syms && d_params, kErrArg, "bad arguments");
+    BZ_REQUIRE(wait_limit_ns > 0, kErrArg, "wait limit must be positive");
+    cudaStream_t st = S(stream);
+    OneBlock ob(s, st);
+    const SlabDev &d = ob.d();
+    const int nsel = (s + kGroupSize - 1) / kGroupSize;
+    BZ_CUDA(cudaMemcpyAsync(d.rle2, d_syms, sizeof(uint16_t) * s, cudaMemcpyDeviceToDevice, st));
+    set_int(d.s, s, st);
+    set_int(d.n_sel, nsel, st);
+    set_int(d.n_groups, kMaxGroups, st);
+    set_int(d.learned, 1, st);
+    BZ_CUDA(cudaMemsetAsync(d.rfreq, 0, sizeof(int32_t) * kMaxGroups * kMaxAlpha, st));
+    BZ_CUDA(cudaMemsetAsync(d.err, 0, sizeof(int32_t), st));
+    uint8_t *packed = pack_params(d_params, st);
+    mlp::launch_select(d, packed, nullptr, nullptr, nullptr, st, wait_limit_ns,
+                       withhold_weights ? 1 : 0);
+    BZ_CUDA(cudaMemcpyAsync(d.h_flags, d.err, 4, cudaMemcpyDeviceToHost, st));
+    BZ_CUDA(cudaFreeAsync(packed, st));
+    BZ_CUDA(cudaStreamSynchronize(st));
+    BZ_REQUIRE(d.h_flags[0] == 0, kErrTimeout,
+               "selector kernel: a bounded wait ran out (error word " +
+                   std::to_string(d.h_flags[0]) + ")");
+  });
+}
+
 int bz2g_huffman_build_learned(const uint16_t *d_syms, int s, int n_in_use, const float *d_params,
                                uint8_t *len, int32_t *code, uint8_t *selectors,
                                uint8_t *mlp_selectors, int *n_selectors, int *n_groups,

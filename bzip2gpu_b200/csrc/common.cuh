@@ -44,6 +44,7 @@ enum Status {
   kErrAlloc = 3,
   kErrInternal = 4,
   kErrTooLarge = 5,
+  kErrTimeout = 6,  // a bounded wait inside a kernel ran out
 };
 
 [[noreturn]] void throw_cuda(cudaError_t e, const char *expr, const char *file, int line);

@@ -152,9 +152,12 @@ __device__ __forceinline__ void epilogue_chunk(const uint32_t (&r)[32], float sc
   }
 }
 
+// wait_ns bounds every wait of the kernel.  withhold != 0 (the failure-path
+// check, never the pipeline) makes the weight producer issue no copy and
+// signal nothing, so the waits for the weights run out.
 __global__ void __launch_bounds__(kSelThreads, 1)
     k_mlp_select(SlabDev d, const uint8_t *__restrict__ packed, float *logits,
-                 int32_t *rfreq_out) {
+                 int32_t *rfreq_out, uint64_t wait_ns, int withhold) {
   extern __shared__ __align__(1024) uint8_t sm[];
   uint8_t *act = sm + kSAct;
   uint8_t *ring = sm + kSRing;
@@ -197,7 +200,7 @@ __global__ void __launch_bounds__(kSelThreads, 1)
 
   if (warp == 5) {
     // ---------------------------------------------------- weight producer
-    if (lane == 0) {
+    if (lane == 0 && !withhold) {
       mbar_expect_tx(wbar, kW3Bytes + kBiasBytes);
       bulk_g2s(w3, packed + kPW3, kW3Bytes, wbar);
       bulk_g2s(sm + kSBias, packed + kPBias, kBiasBytes, wbar);
@@ -208,7 +211,7 @@ __global__ void __launch_bounds__(kSelThreads, 1)
         if (!tile_active(d, gt, &b, &g0, &nh)) continue;
         for (int c = 0; c < kChunksPerTile; c++, q++) {
           const uint32_t s = q % kStages, n = q / kStages;
-          if (n > 0 && !mbar_wait(&empty[s], (n - 1) & 1, abort_s, err, 1)) {
+          if (n > 0 && !mbar_wait(&empty[s], (n - 1) & 1, abort_s, err, 1, wait_ns)) {
             ok = false;
             break;
           }
@@ -229,35 +232,35 @@ __global__ void __launch_bounds__(kSelThreads, 1)
     if (lane == 0) {
       const uint32_t id_h = idesc_bf16_f32(128, kHid), id_o = idesc_bf16_f32(128, kOutPad);
       const uint32_t a0 = smem_u32(act), r0 = smem_u32(ring), w30 = smem_u32(w3);
-      bool ok = mbar_wait(wbar, 0, abort_s, err, 2);
+      bool ok = mbar_wait(wbar, 0, abort_s, err, 2, wait_ns);
       uint32_t q = 0, it = 0;
       for (int gt = blockIdx.x; gt < d.n_group_tiles && ok; gt += gridDim.x) {
         int b, g0, nh;
         if (!tile_active(d, gt, &b, &g0, &nh)) continue;
         const uint32_t ph = it & 1;
-        if (!(ok = mbar_wait(xbar, ph, abort_s, err, 2))) break;
+        if (!(ok = mbar_wait(xbar, ph, abort_s, err, 2, wait_ns))) break;
         fence_after_sync();
         for (int j = 0; j < kL1Steps && ok; j++, q++) {
           const uint32_t s = q % kStages;
-          if (!(ok = mbar_wait(&full[s], (q / kStages) & 1, abort_s, err, 2))) break;
+          if (!(ok = mbar_wait(&full[s], (q / kStages) & 1, abort_s, err, 2, wait_ns))) break;
           mma_bf16(tbase, desc_noswizzle(a0 + j * 256, 128, kInPad * 16),
                    desc_noswizzle(r0 + s * kChunkBytes, 128, 256), id_h, j > 0);
           mma_commit(&empty[s]);
         }
         if (!ok) break;
         mma_commit(d1bar);
-        if (!(ok = mbar_wait(h1bar, ph, abort_s, err, 2))) break;
+        if (!(ok = mbar_wait(h1bar, ph, abort_s, err, 2, wait_ns))) break;
         fence_after_sync();
         for (int j = 0; j < kL2Steps && ok; j++, q++) {
           const uint32_t s = q % kStages;
-          if (!(ok = mbar_wait(&full[s], (q / kStages) & 1, abort_s, err, 2))) break;
+          if (!(ok = mbar_wait(&full[s], (q / kStages) & 1, abort_s, err, 2, wait_ns))) break;
           mma_bf16(tbase + kHid, desc_noswizzle(a0 + j * 256, 128, kHid * 16),
                    desc_noswizzle(r0 + s * kChunkBytes, 128, 256), id_h, j > 0);
           mma_commit(&empty[s]);
         }
         if (!ok) break;
         mma_commit(d2bar);
-        if (!(ok = mbar_wait(h2bar, ph, abort_s, err, 2))) break;
+        if (!(ok = mbar_wait(h2bar, ph, abort_s, err, 2, wait_ns))) break;
         fence_after_sync();
         for (int j = 0; j < kL2Steps; j++)
           mma_bf16(tbase, desc_noswizzle(a0 + j * 256, 128, kHid * 16),
@@ -273,7 +276,7 @@ __global__ void __launch_bounds__(kSelThreads, 1)
   } else {
     // ------------------------------------------------------ compute warps
     const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
-    bool stop = compute_any(!mbar_wait(wbar, 0, abort_s, err, 4));
+    bool stop = compute_any(!mbar_wait(wbar, 0, abort_s, err, 4, wait_ns));
     uint32_t it = 0;
     for (int gt = blockIdx.x; gt < d.n_group_tiles && !stop; gt += gridDim.x) {
       int b, g0, nh;
@@ -304,7 +307,7 @@ __global__ void __launch_bounds__(kSelThreads, 1)
       fence_async_smem();
       mbar_arrive(xbar);
       // layer 1: scale by 1/size, bias, ReLU -> H1 (kt = 256) over the counts
-      if ((stop = compute_any(!mbar_wait(d1bar, ph, abort_s, err, 4)))) break;
+      if ((stop = compute_any(!mbar_wait(d1bar, ph, abort_s, err, 4, wait_ns)))) break;
       fence_after_sync();
 #pragma unroll 1
       for (int c = 0; c < kHid / 32; c++) {
@@ -317,7 +320,7 @@ __global__ void __launch_bounds__(kSelThreads, 1)
       fence_before_sync();
       mbar_arrive(h1bar);
       // layer 2: bias, ReLU -> H2
-      if ((stop = compute_any(!mbar_wait(d2bar, ph, abort_s, err, 4)))) break;
+      if ((stop = compute_any(!mbar_wait(d2bar, ph, abort_s, err, 4, wait_ns)))) break;
       fence_after_sync();
 #pragma unroll 1
       for (int c = 0; c < kHid / 32; c++) {
@@ -330,7 +333,7 @@ __global__ void __launch_bounds__(kSelThreads, 1)
       fence_before_sync();
       mbar_arrive(h2bar);
       // layer 3: logits, first maximum over the six tables
-      if ((stop = compute_any(!mbar_wait(d3bar, ph, abort_s, err, 4)))) break;
+      if ((stop = compute_any(!mbar_wait(d3bar, ph, abort_s, err, 4, wait_ns)))) break;
       fence_after_sync();
       uint32_t r[16];
       BZ_TMEM_LD16(tbase + lane_base, r);
@@ -725,13 +728,14 @@ void to_bf16(const float *params, bf16 *out, cudaStream_t st) {
 }
 
 void launch_select(const SlabDev &d, const uint8_t *packed, float *logits, int *err,
-                   int32_t *rfreq, cudaStream_t st) {
+                   int32_t *rfreq, cudaStream_t st, uint64_t wait_ns, int withhold) {
   smem_attr(k_mlp_select, kSelSmem, g_select_attr);
   if (d.n_group_tiles <= 0) return;
   SlabDev dd = d;
   if (err) dd.err = err;
   const int grid = std::min(d.n_group_tiles, num_sms());
-  k_mlp_select<<<grid, kSelThreads, kSelSmem, st>>>(dd, packed, logits, rfreq ? rfreq : d.rfreq);
+  k_mlp_select<<<grid, kSelThreads, kSelSmem, st>>>(dd, packed, logits, rfreq ? rfreq : d.rfreq,
+                                                    wait_ns, withhold);
   BZ_LAUNCH_CHECK();
 }
 

@@ -123,24 +123,52 @@ __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d) {
   for (int w = 0; w < 8; w++) pmask[ln][w] = 0;
   __syncwarp();
   {
-    // rank of each of this lane's 8 symbols among all keys (list of lane 0);
-    // the keys are read four at a time and compared against all eight
-    int kc[8], r[8];
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
-      kc[q] = key[ln + 32 * q];
-      r[q] = 0;
-    }
-    const int4 *k4 = reinterpret_cast<const int4 *>(key);
-    for (int c2 = 0; c2 < 64; c2++) {
-      const int4 v = k4[c2];
+    // Lane 0's list: the in-use symbols by key, largest first.  A bitonic
+    // sort of the 256 keys across the warp (symbol 8k+q in register q of lane
+    // k; partners 8 or more apart sit in other lanes and come by shuffle),
+    // each key packed with its symbol as (key + 257) << 8 | symbol, 0 for
+    // symbols not in use.  Keys are distinct and above -258, so the packing
+    // keeps their order.
+    uint32_t v[8];
+    {
+      const int4 *k4 = reinterpret_cast<const int4 *>(key) + 2 * ln;
+      const int4 lo = k4[0], hi = k4[1];
+      const int kk[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
 #pragma unroll
       for (int q = 0; q < 8; q++)
-        r[q] += (v.x > kc[q]) + (v.y > kc[q]) + (v.z > kc[q]) + (v.w > kc[q]);
+        v[q] = kk[q] == INT32_MIN ? 0u : ((uint32_t)(kk[q] + 257) << 8) | (uint32_t)(8 * ln + q);
+    }
+#pragma unroll
+    for (int k = 2; k <= 256; k <<= 1) {
+#pragma unroll
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        if (j >= 8) {
+          const int lj = j >> 3;
+          const bool lower = (ln & lj) == 0;
+#pragma unroll
+          for (int q = 0; q < 8; q++) {
+            const uint32_t o = __shfl_xor_sync(0xffffffffu, v[q], lj);
+            const bool asc = ((8 * ln + q) & k) != 0;  // descending overall
+            const bool keep_max = lower != asc;
+            v[q] = keep_max ? max(v[q], o) : min(v[q], o);
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < 8; q++) {
+            if (q & j) continue;
+            const int p = q | j;
+            const bool asc = ((8 * ln + q) & k) != 0;
+            const uint32_t a = v[q], b = v[p];
+            const uint32_t mn = min(a, b), mx = max(a, b);
+            v[q] = asc ? mn : mx;
+            v[p] = asc ? mx : mn;
+          }
+        }
+      }
     }
 #pragma unroll
     for (int q = 0; q < 8; q++)
-      if (kc[q] != INT32_MIN) lists[r[q]] = (uint8_t)(ln + 32 * q);
+      if (8 * ln + q < nuse) lists[8 * ln + q] = (uint8_t)(v[q] & 0xffu);
   }
   // partial lists
   const int a0 = ln * kSub;

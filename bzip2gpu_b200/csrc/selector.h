@@ -59,9 +59,12 @@ void to_bf16(const float *params, __nv_bfloat16 *out, cudaStream_t st);
 // d.sel and adds the chosen tables' symbol counts into rfreq (nullptr:
 // d.rfreq; same layout).  logits (optional, debugging and tests): per group
 // tile, 128 rows x 8 floats.  err: device word (nullptr: d.err), nonzero if a
-// wait inside the kernel timed out.
+// wait inside the kernel timed out.  wait_ns bounds each wait; withhold != 0
+// (failure-path check only) keeps the weight producer from issuing anything,
+// so the waits for the weights run out and the kernel returns with err set.
 void launch_select(const SlabDev &d, const uint8_t *packed, float *logits, int *err,
-                   int32_t *rfreq, cudaStream_t st);
+                   int32_t *rfreq, cudaStream_t st, uint64_t wait_ns = 2000000000ull,
+                   int withhold = 0);
 
 // ---------------------------------------------------------------- training
 // Training-set tap of the compression pipeline: for every block with six

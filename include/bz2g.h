@@ -28,6 +28,7 @@ extern "C" {
 #define BZ2G_ERR_ALLOC 3
 #define BZ2G_ERR_INTERNAL 4
 #define BZ2G_ERR_TOO_LARGE 5
+#define BZ2G_ERR_TIMEOUT 6 /* a bounded wait inside a kernel ran out */
 
 #define BZ2G_MAX_GROUPS 6  /* include/compression.h:65 max_n_groups */
 #define BZ2G_MAX_ALPHA 258 /* include/compression.h:66 max_alphabet_size */
@@ -285,6 +286,20 @@ int bz2g_get_selector(void);
  * ceil(s/50) bytes); d_params: device fp32 parameters. */
 int bz2g_selector_logits(const uint16_t *d_syms, int s, const float *d_params, float *d_logits,
                          uint8_t *d_sel, void *stream);
+
+/* Failure-path check of the tensor-core selector kernel (no counterpart in
+ * the reference, which has no error path: include/utils.h:3-12).  Every wait
+ * inside that kernel is bounded; a wait that runs out sets a device error
+ * word, the kernel's threads leave their loops, free their tensor memory and
+ * return, and the host turns the word into an error.  This runs the kernel
+ * over s symbols as one six-table block with each wait limited to
+ * wait_limit_ns.  withhold_weights != 0 keeps the kernel's weight producer
+ * from issuing any copy, so the waits for the weights run out: the call then
+ * returns BZ2G_ERR_TIMEOUT (the error word in bz2g_last_error) and the
+ * device stays usable.  With withhold_weights == 0 it returns BZ2G_OK once
+ * the kernel met all its waits. */
+int bz2g_selector_wait_check(const uint16_t *d_syms, int s, const float *d_params,
+                             uint64_t wait_limit_ns, int withhold_weights, void *stream);
 
 /* bz2g_huffman_build with the learned selector (d_params: device fp32
  * parameters).  mlp_selectors (host, ceil(s/50) bytes, may be NULL) gets the
