@@ -246,6 +246,57 @@ def run_batch(args):
                           "bit_exact": True}))
 
 
+def run_stress(args):
+    """The BWT stress stream (zeros | periodic-17 | uniform | Markov, 64 MiB
+    each, 900,000-byte blocks): MB/s, the stream checked against the oracle,
+    and the BWT's HBM GB/s per doubling round by the byte model (28 bytes per
+    rotation still in a group of two or more, over the round's device time).
+    One worker stream by default, so each round's time is its own."""
+    world, rank, local = dist_setup(args.gpus)
+    import torch
+
+    import bzip2gpu_b200 as B
+    import bzip2gpu_b200.workloads as W
+    import oracle
+
+    host = W.stress()
+    d_in = torch.from_numpy(host).cuda()
+    B.set_engine(args.slab or 128, args.workers or 1)
+    B.set_timing(True)
+    out = B.compress_device(d_in, 9)
+    for _ in range(max(args.warmup - 1, 0)):
+        B.compress_device(d_in, 9)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        got = B.compress_device(d_in, 9)
+    e1.record()
+    torch.cuda.synchronize()
+    dt = e0.elapsed_time(e1) / 1e3
+    rounds = B.last_round_stats()
+    stats = B.last_stats()
+    peak, peak_kind = peaks()
+    rows = []
+    for r in rounds:
+        shift = None if r["round"] == 0 else 4 << (r["round"] - 1)
+        gbs = 28 * r["active"] / (r["ms"] / 1e3) / 1e9 if r["ms"] > 0 else 0.0
+        rows.append({"round": r["round"], "shift": shift, "active": r["active"],
+                     "ms": round(r["ms"], 3), "model_GBps": round(gbs, 1),
+                     "frac_of_hbm": round(gbs / peak, 4)})
+    identical = got == out and out == oracle.compress(host, 9, threads=os.cpu_count() or 8)
+    if rank == 0:
+        print(json.dumps({"workload": "BWT stress: zeros | periodic-17 | uniform | Markov, "
+                                      "64 MiB each, 900k blocks", "bytes": int(host.size),
+                          "MB/s": round(host.size * args.steps / dt / 1e6, 2),
+                          "identical_to_oracle": bool(identical), "workers": args.workers or 1,
+                          "peak_GBps": peak, "peak_kind": peak_kind,
+                          "stage_ms": {k[3:]: round(v, 2) for k, v in stats.items()
+                                       if k.startswith("ms_")},
+                          "bwt_rounds": rows}))
+
+
 # DRAM bytes per algorithmic byte of k_radix_scatter: (127.4 + 76.6) MB / 256 MB
 # in an ncu capture of its first-sort pass over a 64-block slab
 TRAFFIC_PER_ALGO_BYTE = 204.0 / 256.0
@@ -263,13 +314,15 @@ def main():
                     help="skip the whole-stream parity and round-trip checks")
     ap.add_argument("--slab", type=int, default=0)
     ap.add_argument("--workers", type=int, default=0)
-    ap.add_argument("--workload", default="large", choices=["large", "batch"])
+    ap.add_argument("--workload", default="large", choices=["large", "batch", "stress"])
     ap.add_argument("--batch-count", type=int, default=2048)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "stress":
+        return run_stress(args)
 
     world, rank, local = dist_setup(args.gpus)
     import torch

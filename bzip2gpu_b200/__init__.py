@@ -55,6 +55,7 @@ _SIGS = {
     "bz2g_set_timing": (_i, [_i]),
     "bz2g_last_stats": (_i, [_c.POINTER(_c.c_double), _i]),
     "bz2g_launch_count": (_c.c_int64, []),
+    "bz2g_last_round_stats": (_i, [_c.POINTER(_c.c_double), _i]),
     "bz2g_rle1_bound": (_sz, [_sz]),
     "bz2g_rle1": (_i, [_vp, _i, _vp, _c.POINTER(_i), _vp]),
     "bz2g_crc32": (_i, [_vp, _sz, _c.POINTER(_c.c_uint32), _vp]),
@@ -329,6 +330,17 @@ def last_stats() -> dict:
     buf = (ctypes.c_double * len(STAT_FIELDS))()
     lib().bz2g_last_stats(buf, len(STAT_FIELDS))
     return dict(zip(STAT_FIELDS, list(buf)))
+
+
+def last_round_stats() -> list[dict]:
+    """BWT rounds of the last whole-stream call with timing on: per round its
+    index (0: the first sort by 4-byte prefixes, standing for the doubling
+    rounds with shift 1 and 2), the rotations the byte model charges to it
+    (28 bytes each) and its device milliseconds summed over slabs."""
+    buf = (ctypes.c_double * 96)()
+    n = lib().bz2g_last_round_stats(buf, 96)
+    return [{"round": int(buf[3 * r]), "active": int(buf[3 * r + 1]), "ms": buf[3 * r + 2]}
+            for r in range(n)]
 
 
 def launch_count() -> int:

@@ -23,6 +23,7 @@
 // (item = prefix << 32 | i), rounds use item = head << 2kb | rank << kb | i.
 // Larger m keeps separate 64-bit keys and 32-bit rotations, with P = 8.
 #include <algorithm>
+#include <cstring>
 
 #include "engine.h"
 
@@ -264,15 +265,186 @@ void radix_sort(const SlabDev &d, int lo, int hi, int has_vals, cudaStream_t st,
   }
 }
 
+// --------------------------------------------------- first sort, by text
+// The first sort orders every rotation by its first 4 bytes with four LSD
+// passes of 8 bits, moving 4-byte rotation indices only: pass p's digit is
+// byte q = 3 - p of the rotation, read from the block's text (a few hundred
+// KB per block, served from L2), so each pass reads and writes 4 bytes per
+// rotation instead of an 8-byte (key, index) item.  Pass 0 starts from index
+// order and reads no input array; the last pass writes the packed item
+// (prefix << 32 | index) that the ranking kernels read.  Indices are below
+// 2^21 here (the packed layout), so a digit and an index share one 32-bit
+// word in shared memory.
+constexpr size_t kTextSmem =
+    (size_t)kTile * 4 + (size_t)kSortWarps * kRadix * 4 + 2 * kRadix * 4;
+
+__device__ __forceinline__ int wrap_add(int i, int q, int m) {
+  int j = i + q;
+  while (j >= m) j -= m;
+  return j;
+}
+
+// The first 4 bytes of rotation i, big-endian.
+__device__ __forceinline__ uint32_t text_prefix4(const uint8_t *T, int m, int i) {
+  uint32_t k = 0;
+#pragma unroll
+  for (int q = 0; q < 4; q++) k = (k << 8) | T[wrap_add(i, q, m)];
+  return k;
+}
+
+__global__ void __launch_bounds__(256) k_text_hist(SlabDev d, int q, int first) {
+  __shared__ uint32_t cnt[kRadix];
+  const int t = blockIdx.x;
+  int b, lt;
+  const int valid = tile_valid(d, t, d.sort_len, &b, &lt);
+  if (valid == 0) return;
+  cnt[threadIdx.x] = 0;
+  __syncthreads();
+  const int m = d.m[b];
+  const uint8_t *T = d.rle1 + d.off[b];
+  const uint32_t *V = d.vals[d.sort_ctl[0]] + d.off[b] + lt;
+  for (int e = threadIdx.x; e < valid; e += blockDim.x) {
+    const int i = first ? lt + e : (int)V[e];
+    atomicAdd(&cnt[T[wrap_add(i, q, m)]], 1u);
+  }
+  __syncthreads();
+  d.tile_hist[(size_t)t * kRadix + threadIdx.x] = cnt[threadIdx.x];
+}
+
+// One stable pass of the first sort (same tile scheme as k_radix_scatter:
+// warp-striped ranking by ballots, local order in shared memory, runs of
+// equal digits written out contiguously).
+__global__ void __launch_bounds__(256, 4)
+    k_text_scatter(SlabDev d, int q, int first, int last, int timed) {
+  const int t = blockIdx.x;
+  int b, lt;
+  const int valid = tile_valid(d, t, d.sort_len, &b, &lt);
+  if (valid == 0) return;
+  if (timed >= 0 && threadIdx.x == 0)
+    atomicAdd((unsigned long long *)&d.kt_elems[timed], (unsigned long long)valid);
+  extern __shared__ __align__(16) uint8_t smem[];
+  uint32_t *sv = reinterpret_cast<uint32_t *>(smem);        // digit << 24 | index
+  uint32_t *wcnt = sv + kTile;                               // [warp][digit]
+  uint32_t *lbase = wcnt + kSortWarps * kRadix;
+  uint32_t *goff = lbase + kRadix;
+  const int cur = d.sort_ctl[0];
+  const int64_t off = d.off[b];
+  const int m = d.m[b];
+  const uint8_t *T = d.rle1 + off;
+  const uint32_t *V = d.vals[cur] + off + lt;
+  const int w = warp_id(), ln = lane_id();
+
+  uint32_t idx[kTileItems];
+#pragma unroll
+  for (int i = 0; i < kTileItems; i++) {
+    const int e = w * kWarpSpan + i * 32 + ln;
+    idx[i] = e < valid ? (first ? (uint32_t)(lt + e) : V[e]) : 0u;
+  }
+  uint32_t dgt[kTileItems];
+#pragma unroll
+  for (int i = 0; i < kTileItems; i++) {
+    const int e = w * kWarpSpan + i * 32 + ln;
+    dgt[i] = e < valid ? T[wrap_add((int)idx[i], q, m)] : 0u;
+  }
+  for (int i = threadIdx.x; i < kSortWarps * kRadix; i += blockDim.x) wcnt[i] = 0;
+  goff[threadIdx.x] = d.tile_hist[(size_t)t * kRadix + threadIdx.x];
+  __syncthreads();
+
+  uint32_t rank2[kTileItems / 2];
+  const unsigned lt_mask = (1u << ln) - 1u;
+#pragma unroll
+  for (int i = 0; i < kTileItems; i++) {
+    const int e = w * kWarpSpan + i * 32 + ln;
+    const bool ok = e < valid;
+    const int dg = (int)dgt[i];
+    const unsigned peers = digit_peers(dg, ok);
+    const uint32_t before = ok ? wcnt[w * kRadix + dg] : 0;
+    const uint32_t r = before + __popc(peers & lt_mask);
+    if (i & 1)
+      rank2[i >> 1] |= r << 16;
+    else
+      rank2[i >> 1] = r;
+    __syncwarp();
+    if (ok && (peers & lt_mask) == 0) wcnt[w * kRadix + dg] = before + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  {
+    const int dg = threadIdx.x;
+    uint32_t run = 0;
+    for (int ww = 0; ww < kSortWarps; ww++) run += wcnt[ww * kRadix + dg];
+    __shared__ uint32_t scratch[40];
+    uint32_t tot;
+    const uint32_t lb = block_excl_sum(run, scratch, &tot);
+    uint32_t at = lb;
+    for (int ww = 0; ww < kSortWarps; ww++) {
+      const uint32_t c = wcnt[ww * kRadix + dg];
+      wcnt[ww * kRadix + dg] = at;
+      at += c;
+    }
+    goff[dg] -= lb;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < kTileItems; i++) {
+    const int e = w * kWarpSpan + i * 32 + ln;
+    if (e < valid) {
+      const uint32_t r = (i & 1) ? rank2[i >> 1] >> 16 : rank2[i >> 1] & 0xffffu;
+      sv[wcnt[w * kRadix + dgt[i]] + r] = (dgt[i] << 24) | idx[i];
+    }
+  }
+  __syncthreads();
+  if (!last) {
+    uint32_t *VO = d.vals[cur ^ 1];
+    for (int k = threadIdx.x; k < valid; k += blockDim.x) {
+      const uint32_t v = sv[k];
+      VO[goff[v >> 24] + (uint32_t)k] = v & 0xffffffu;
+    }
+  } else {
+    uint64_t *KO = d.keys[cur ^ 1];
+    for (int k = threadIdx.x; k < valid; k += blockDim.x) {
+      const uint32_t v = sv[k];
+      const uint32_t i = v & 0xffffffu;
+      KO[goff[v >> 24] + (uint32_t)k] = ((uint64_t)text_prefix4(T, m, (int)i) << 32) | i;
+    }
+  }
+}
+
+__global__ void k_text_flip(SlabDev d) {
+  d.sort_ctl[0] ^= 1;
+  d.sort_ctl[1] = 0;
+}
+
+// The first sort of the packed layout: four passes over rotation indices,
+// ending with packed items in keys[sort_ctl[0]].  Every pass runs (no
+// trivial-pass skip): pass 0 has no input array and the last one writes the
+// packed items.
+void text_sort(const SlabDev &d, cudaStream_t st) {
+  for (int p = 0; p < 4; p++) {
+    const int q = 3 - p;
+    k_text_hist<<<d.ntiles, 256, 0, st>>>(d, q, p == 0);
+    BZ_LAUNCH_CHECK();
+    k_radix_scan<<<d.nblocks, 256, 0, st>>>(d);
+    BZ_LAUNCH_CHECK();
+    int timed = -1;
+    if (d.kt_on && *d.kt_n < kMaxTimedLaunches) {
+      timed = (*d.kt_n)++;
+      d.kt_bpe[timed] = p == 3 ? 12 : 8;  // index read, index (or packed item) written
+      BZ_CUDA(cudaEventRecord(d.kt_ev[2 * timed], st));
+    }
+    k_text_scatter<<<d.ntiles, 256, kTextSmem, st>>>(d, q, p == 0, p == 3, timed);
+    BZ_LAUNCH_CHECK();
+    if (timed >= 0) BZ_CUDA(cudaEventRecord(d.kt_ev[2 * timed + 1], st));
+    k_text_flip<<<1, 1, 0, st>>>(d);
+    BZ_LAUNCH_CHECK();
+  }
+}
+
 // ------------------------------------------------------------------- BWT
 __global__ void k_bwt_init(SlabDev d) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b == 0) {
-    d.sort_ctl[0] = 0;
-    d.sort_ctl[1] = 0;
-    d.sort_ctl[2] = 0;
-    d.sort_ctl[3] = 0;
-  }
+  if (b == 0)
+    for (int k = 0; k < 10; k++) d.sort_ctl[k] = 0;
   if (b >= d.nblocks) return;
   int m = d.m[b];
   d.sort_len[b] = m > 1 ? m : 0;
@@ -282,42 +454,6 @@ __global__ void k_bwt_init(SlabDev d) {
   d.active_sum[b] = 0;
   for (int k = 0; k < 8; k++) d.pstat[b * 8 + k] = 0;
   if (m == 1) d.sa[d.off[b]] = 0;
-}
-
-// Group heads and singletons of the prefix-1, -2, -4 (and -8) partitions,
-// read off the first sort's keys (key_bits = 32 packed, 64 otherwise):
-// pstat[b*8 + q] heads, pstat[b*8 + 4 + q] singletons of prefix 2^q bytes.
-__global__ void __launch_bounds__(256) k_bwt_prefix_stats(SlabDev d, Layout L, int key_bits,
-                                                          int nq) {
-  int b, lt;
-  int valid = tile_valid(d, blockIdx.x, d.sort_len, &b, &lt);
-  if (valid == 0) return;
-  const int m = d.m[b];
-  const uint64_t *K = d.keys[d.sort_ctl[0]] + d.off[b];
-  int cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  for (int e = threadIdx.x; e < valid; e += blockDim.x) {
-    const int j = lt + e;
-    const uint64_t k = key_of(L, K[j]);
-    const uint64_t kp = j > 0 ? key_of(L, K[j - 1]) : 0;
-    const uint64_t kn = j + 1 < m ? key_of(L, K[j + 1]) : 0;
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      if (q < nq) {
-        const int sh = key_bits - 8 * (1 << q);
-        const uint64_t a = sh > 0 ? k >> sh : k;
-        const bool hd = j == 0 || a != (sh > 0 ? kp >> sh : kp);
-        const bool tl = j + 1 == m || a != (sh > 0 ? kn >> sh : kn);
-        cnt[q] += hd;
-        cnt[4 + q] += hd && tl;
-      }
-    }
-  }
-#pragma unroll
-  for (int q = 0; q < 8; q++) {
-    int v = cnt[q];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane_id() == 0 && v) atomicAdd(&d.pstat[b * 8 + q], v);
-  }
 }
 
 // The oracle's accounting of the rounds h = 1, 2, (4) that the first sort
@@ -341,6 +477,7 @@ __global__ void k_bwt_prefix_account(SlabDev d, int nq) {
   }
   d.active_sum[b] = A;
   d.ngroups[b] = ps[nq - 2];
+  if (A) atomicAdd(reinterpret_cast<unsigned long long *>(d.sort_ctl + 8), (unsigned long long)A);
 }
 
 // First keys: the first 4 (packed) or 8 bytes of each rotation.
@@ -384,9 +521,12 @@ __global__ void __launch_bounds__(256) k_bwt_keys0(SlabDev d, int packed) {
 __device__ __forceinline__ uint64_t key_at(const uint64_t *K, int k) { return K[k]; }
 
 // Per tile: last head (SA position), head count, singleton count, active
-// (non-singleton) count.
+// (non-singleton) count.  After the first sort (nq > 0) it also counts, from
+// the same reads, the group heads and singletons of the prefix-1, -2 (-4, -8)
+// byte partitions (key_bits = 32 packed, 64 otherwise): pstat[b*8 + q] heads
+// and pstat[b*8 + 4 + q] singletons of prefix 2^q bytes.
 __global__ void __launch_bounds__(256) k_bwt_flags(SlabDev d, Layout L, int initial,
-                                                   const int32_t *list) {
+                                                   const int32_t *list, int key_bits, int nq) {
   __shared__ int red[4][kSortWarps];
   const int t = tile_id(list);
   int b, lt;
@@ -398,19 +538,41 @@ __global__ void __launch_bounds__(256) k_bwt_flags(SlabDev d, Layout L, int init
   const int32_t *P = d.kpos[d.sort_ctl[3]] + off;
   const int w = warp_id(), ln = lane_id();
   int last = -1, heads = 0, sing = 0;
+  int pc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll 4
   for (int i = 0; i < kTileItems; i++) {
     const int e = w * kWarpSpan + i * 32 + ln;
     if (e < valid) {
       const int k = lt + e;
       const uint64_t key = key_of(L, K[k]);
-      const bool hd = k == 0 || key != key_of(L, K[k - 1]);
+      const uint64_t kp = k > 0 ? key_of(L, K[k - 1]) : 0;
+      const uint64_t kn = k + 1 < len ? key_of(L, K[k + 1]) : 0;
+      const bool hd = k == 0 || key != kp;
       if (hd) {
-        const bool tl = k + 1 == len || key_of(L, K[k + 1]) != key;
+        const bool tl = k + 1 == len || kn != key;
         last = max(last, initial ? k : P[k]);
         heads++;
         sing += tl;
       }
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        if (q < nq) {
+          const int sh = key_bits - 8 * (1 << q);
+          const uint64_t a = sh > 0 ? key >> sh : key;
+          const bool h2 = k == 0 || a != (sh > 0 ? kp >> sh : kp);
+          const bool t2 = k + 1 == len || a != (sh > 0 ? kn >> sh : kn);
+          pc[q] += h2;
+          pc[4 + q] += h2 && t2;
+        }
+      }
+    }
+  }
+  if (nq > 0) {
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      int v = pc[q];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (ln == 0 && v) atomicAdd(&d.pstat[b * 8 + q], v);
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
@@ -483,6 +645,7 @@ __global__ void __launch_bounds__(256) k_bwt_rank_block(SlabDev d, int64_t prefi
     } else {
       d.act_len[b] = active;
       atomicAdd(&d.sort_ctl[2], 1);
+      atomicAdd(&d.sort_ctl[6], active);
       atomicAdd(&d.sort_ctl[4], (active + kTile - 1) / kTile);
       d.active_sum[b] += active;  // rotations entering the next round
     }
@@ -641,6 +804,8 @@ void stage_bwt(const SlabDev &d, int max_m, cudaStream_t st) {
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScatterSmem));
     BZ_CUDA(cudaFuncSetAttribute(k_radix_scatter<false>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScatterSmem));
+    BZ_CUDA(cudaFuncSetAttribute(k_text_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kTextSmem));
     smem_configured = true;
   }
   int kb = 1;
@@ -649,44 +814,63 @@ void stage_bwt(const SlabDev &d, int max_m, cudaStream_t st) {
   k_bwt_init<<<(d.nblocks + 127) / 128, 128, 0, st>>>(d);
   BZ_LAUNCH_CHECK();
   if (max_m <= 1) return;
-  k_bwt_keys0<<<d.ntiles, 256, 0, st>>>(d, packed);
-  BZ_LAUNCH_CHECK();
+  bool rounds_timed = d.kt_on && d.rt_ev != nullptr;
+  if (rounds_timed) {
+    d.rt_act[0] = 0;
+    BZ_CUDA(cudaEventRecord(d.rt_ev[0], st));
+  }
   // first sort: 4-byte prefixes in the high half of packed items, or 8-byte keys
   const Layout first = {packed, packed ? 32 : 0};
   const Layout round = {packed, packed ? kb : 0};
-  if (packed)
-    radix_sort(d, 32, 64, 0, st, d.ntiles, nullptr);
-  else
+  if (packed) {
+    text_sort(d, st);
+  } else {
+    k_bwt_keys0<<<d.ntiles, 256, 0, st>>>(d, packed);
+    BZ_LAUNCH_CHECK();
     radix_sort(d, 0, 64, 1, st, d.ntiles, nullptr);
+  }
   const int nq = packed ? 3 : 4;  // prefixes 1,2,4 (,8) bytes
-  k_bwt_prefix_stats<<<d.ntiles, 256, 0, st>>>(d, first, packed ? 32 : 64, nq);
-  BZ_LAUNCH_CHECK();
-  k_bwt_prefix_account<<<(d.nblocks + 127) / 128, 128, 0, st>>>(d, nq);
-  BZ_LAUNCH_CHECK();
   int64_t prefix = packed ? 4 : 8;
   int grid = d.ntiles;
   const int32_t *list = nullptr;
+  int r = 0;  // round being run (0: the first sort)
   for (int initial = 1;; initial = 0) {
     const Layout L = initial ? first : round;
     BZ_CUDA(cudaMemsetAsync(d.sort_ctl + 2, 0, sizeof(int32_t), st));
-    BZ_CUDA(cudaMemsetAsync(d.sort_ctl + 4, 0, 2 * sizeof(int32_t), st));
-    k_bwt_flags<<<grid, 256, 0, st>>>(d, L, initial, list);
+    BZ_CUDA(cudaMemsetAsync(d.sort_ctl + 4, 0, 3 * sizeof(int32_t), st));
+    k_bwt_flags<<<grid, 256, 0, st>>>(d, L, initial, list, packed ? 32 : 64, initial ? nq : 0);
     BZ_LAUNCH_CHECK();
+    if (initial) {
+      k_bwt_prefix_account<<<(d.nblocks + 127) / 128, 128, 0, st>>>(d, nq);
+      BZ_LAUNCH_CHECK();
+    }
     k_bwt_rank_block<<<d.nblocks, 256, 0, st>>>(d, prefix);
     BZ_LAUNCH_CHECK();
     k_bwt_apply<<<grid, 256, 0, st>>>(d, L, initial, kb, list);
     BZ_LAUNCH_CHECK();
     k_bwt_flip<<<1, 1, 0, st>>>(d);
     BZ_LAUNCH_CHECK();
+    if (rounds_timed) {
+      BZ_CUDA(cudaEventRecord(d.rt_ev[2 * r + 1], st));
+      *d.rt_n = r + 1;
+    }
     if (prefix >= max_m) break;
     k_bwt_tile_list<<<(d.nblocks + 127) / 128, 128, 0, st>>>(d);
     BZ_LAUNCH_CHECK();
-    BZ_CUDA(cudaMemcpyAsync(d.h_flags, d.sort_ctl + 2, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost,
+    BZ_CUDA(cudaMemcpyAsync(d.h_flags, d.sort_ctl + 2, 8 * sizeof(int32_t), cudaMemcpyDeviceToHost,
                             st));
     BZ_CUDA(cudaStreamSynchronize(st));
+    if (rounds_timed && initial)
+      std::memcpy(&d.rt_act[0], d.h_flags + 6, sizeof(int64_t));  // sort_ctl[8..9]
     if (d.h_flags[0] == 0) break;
     grid = d.h_flags[2];  // tiles holding active rotations
     list = d.tile_list;
+    r++;
+    if (rounds_timed && r >= kMaxRounds) rounds_timed = false;
+    if (rounds_timed) {
+      d.rt_act[r] = d.h_flags[4];  // rotations entering this round
+      BZ_CUDA(cudaEventRecord(d.rt_ev[2 * r], st));
+    }
     k_bwt_round_keys<<<grid, 256, 0, st>>>(d, (int)prefix, packed, kb, list);
     BZ_LAUNCH_CHECK();
     if (packed)

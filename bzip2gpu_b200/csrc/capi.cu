@@ -388,6 +388,19 @@ int bz2g_last_stats(double *out, int n) {
   return k;
 }
 
+int bz2g_last_round_stats(double *out, int n) {
+  const StageTimes &t = g_last_stats;
+  int rounds = 0;
+  for (int r = 0; r < kMaxRounds; r++)
+    if (t.round_ms[r] > 0 || t.round_active[r] > 0) rounds = r + 1;
+  for (int r = 0; r < rounds && 3 * r + 2 < n; r++) {
+    out[3 * r] = r;
+    out[3 * r + 1] = (double)t.round_active[r];
+    out[3 * r + 2] = t.round_ms[r];
+  }
+  return rounds;
+}
+
 int64_t bz2g_launch_count(void) { return launch_count(); }
 
 int bz2g_rle1(const uint8_t *d_in, int n, uint8_t *d_out, int *m, void *stream) {

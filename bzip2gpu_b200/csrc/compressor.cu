@@ -21,6 +21,9 @@
 
 namespace bz2g {
 
+static_assert(kMaxRounds == sizeof(StageTimes::round_ms) / sizeof(double),
+              "per-round statistics size");
+
 struct Compressor::Worker {
   Workspace *ws = nullptr;
   cudaStream_t st = nullptr;
@@ -33,6 +36,9 @@ struct Compressor::Worker {
   int32_t *h_err = nullptr;    // the workspace's device error word
   cudaEvent_t ev[8] = {};
   cudaEvent_t kt_ev[2 * kMaxTimedLaunches] = {};
+  cudaEvent_t rt_ev[2 * kMaxRounds] = {};
+  int rt_n = 0;
+  int64_t rt_act[kMaxRounds] = {};
   int kt_n = 0;
   int kt_bpe[kMaxTimedLaunches] = {};
   uint64_t *h_kt = nullptr;
@@ -41,6 +47,8 @@ struct Compressor::Worker {
     for (auto &e : ev)
       if (e) cudaEventDestroy(e);
     for (auto &e : kt_ev)
+      if (e) cudaEventDestroy(e);
+    for (auto &e : rt_ev)
       if (e) cudaEventDestroy(e);
     if (h_kt) cudaFreeHost(h_kt);
     delete ws;
@@ -71,6 +79,10 @@ Compressor::Compressor(const CompressorConfig &cfg) : cfg_(cfg) {
     BZ_CUDA(cudaMallocHost((void **)&w->h_err, sizeof(int32_t)));
     for (auto &e : w->ev) BZ_CUDA(cudaEventCreate(&e));
     for (auto &e : w->kt_ev) BZ_CUDA(cudaEventCreate(&e));
+    for (auto &e : w->rt_ev) BZ_CUDA(cudaEventCreate(&e));
+    w->ws->dev.rt_ev = w->rt_ev;
+    w->ws->dev.rt_n = &w->rt_n;
+    w->ws->dev.rt_act = w->rt_act;
     BZ_CUDA(cudaMallocHost((void **)&w->h_kt, 8 * kMaxTimedLaunches));
     w->ws->dev.kt_ev = w->kt_ev;
     w->ws->dev.kt_n = &w->kt_n;
@@ -311,6 +323,7 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
       const bool tm = times != nullptr && cfg_.time_stages;
       w.ws->dev.kt_on = tm;
       w.kt_n = 0;
+      w.rt_n = 0;
       if (tm) BZ_CUDA(cudaMemsetAsync(d.kt_elems, 0, 8 * kMaxTimedLaunches, w.st));
       if (tm) BZ_CUDA(cudaEventRecord(w.ev[0], w.st));
       stage_rle1_crc(d, w.st);
@@ -414,6 +427,12 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
         tsum.huffman += ms[4];
         tsum.sizes += ms[5];
         tsum.place += ms[6];
+        for (int r = 0; r < w.rt_n; r++) {
+          float t = 0;
+          BZ_CUDA(cudaEventElapsedTime(&t, w.rt_ev[2 * r], w.rt_ev[2 * r + 1]));
+          tsum.round_ms[r] += t;
+          tsum.round_active[r] += w.rt_act[r];
+        }
         for (int q = 0; q < w.kt_n; q++) {
           if (w.h_kt[q] == 0) continue;  // skipped pass (one digit value only)
           float t = 0;

@@ -27,6 +27,12 @@ struct StageTimes {
   // ms, and algorithmic bytes (each element's item read and written once)
   int64_t scatter_launches = 0;
   double scatter_ms = 0, scatter_bytes = 0;
+  // BWT rounds (when timing is enabled), summed over slabs by round index:
+  // r = 0 the first sort (standing for the oracle's rounds h = 1, 2), r >= 1
+  // the doubling round with shift 4 * 2^(r-1).  round_active: rotations the
+  // byte model charges to the round; round_ms: device time.
+  double round_ms[24] = {};
+  int64_t round_active[24] = {};
   // blocks whose tables came from the learned selector, and blocks with six
   // tables (the learned selector's domain; the rest fell back to plain)
   int64_t learned_blocks = 0, six_table_blocks = 0;

@@ -94,7 +94,9 @@ struct SlabDev {
   // radix sort control
   int32_t *sort_ctl;                   // [0]=cur key buffer, [1]=nontrivial flag,
                                        // [2]=blocks still sorting, [3]=cur kpos buffer,
-                                       // [4]=tiles of the next round, [5]=tile list fill
+                                       // [4]=tiles of the next round, [5]=tile list fill,
+                                       // [6]=rotations entering the next round,
+                                       // [8..9]=u64 rotations the first sort's model charges
   int32_t *h_flags;                    // pinned host mirror of small counters
   // stream state: [0] = bit offset (u64), [1] = stream crc, [2] = slab first word,
   // [3] = slab word count
@@ -107,9 +109,19 @@ struct SlabDev {
   int *kt_n;                // launches recorded in this slab
   int *kt_bpe;              // [kMaxTimedLaunches]
   uint64_t *kt_elems;       // device [kMaxTimedLaunches]
+  // optional per-round timing of the BWT (host-side fields, with kt_on):
+  // events around round r (r = 0: the first sort and its ranking; r >= 1:
+  // the doubling round with shift 4 * 2^(r-1)), rounds recorded, and the
+  // rotations the round's model charges (r = 0: those the first sort stands
+  // for, the oracle's rounds h = 1 and 2; r >= 1: active rotations entering
+  // the round)
+  cudaEvent_t *rt_ev;       // [2 * kMaxRounds]
+  int *rt_n;
+  int64_t *rt_act;          // [kMaxRounds]
 };
 
 constexpr int kMaxTimedLaunches = 96;
+constexpr int kMaxRounds = 24;
 
 // Owns the device buffers of a slab context (sized for a maximum slab).
 class Workspace {

@@ -117,6 +117,14 @@ int bz2g_set_engine(int slab_blocks, int workers);
  * bz2g_launch_count: kernels launched by this library since it was loaded. */
 int bz2g_set_timing(int on);
 int bz2g_last_stats(double *out, int n);
+/* Per BWT round of the last whole-stream call with timing on, summed over its
+ * slabs: out[3r] = r, out[3r+1] = rotations the HBM byte model charges to the
+ * round, out[3r+2] = device milliseconds.  Round 0 is the first sort by 4-byte
+ * prefixes (it stands for the reference's doubling rounds with shift 1 and 2,
+ * src/compression/fbwt.cu:66-95); round r >= 1 is the doubling round with
+ * shift 4 * 2^(r-1), charged with the rotations still in groups of two or
+ * more when it starts.  Returns the number of rounds. */
+int bz2g_last_round_stats(double *out, int n);
 int64_t bz2g_launch_count(void);
 
 /* ------------------------------------------------------------- per stage */
