@@ -5,6 +5,10 @@
 Products (all sm_100a, written under bzip2gpu_b200/_lib):
   libbz2gpu_b200.so      C-ABI (include/bz2g.h) and the C++ drop-in API
                          (include/compression.h, io.h, cli.h, crc32.h)
+  libbz2gpu_b200.a       the same objects as a static archive, for programs
+                         linked the way the reference links its core library
+                         (one CUDA runtime in the program, so client code can
+                         launch the exported count_frequencies kernel itself)
   bzip2gpu               the command line tool (same flags as the reference)
 Objects go to bzip2gpu_b200/_build.  A source is recompiled when it or any
 header in csrc/ or include/ is newer than its object.
@@ -78,6 +82,16 @@ def build(verbose: bool = False) -> Path:
         if r.returncode != 0:
             raise RuntimeError(f"link failed\n{r.stdout}\n{r.stderr}")
         os.replace(tmp, lib)
+    arch = LIB / "libbz2gpu_b200.a"
+    if not arch.exists() or arch.stat().st_mtime < max(o.stat().st_mtime for o in lib_objs):
+        tmp = arch.with_suffix(".a.tmp")
+        if tmp.exists():
+            tmp.unlink()
+        r = subprocess.run(["ar", "rcs", str(tmp), *map(str, lib_objs)], capture_output=True,
+                           text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"archive failed\n{r.stdout}\n{r.stderr}")
+        os.replace(tmp, arch)
     cli = LIB / "bzip2gpu"
     cli_obj = objs[CSRC / "cli_main.cpp"]
     if not cli.exists() or cli.stat().st_mtime < max(lib.stat().st_mtime, cli_obj.stat().st_mtime):

@@ -3,7 +3,8 @@ C++ API driven the way the reference's main() drives it.
 
 1. oracle/_ref/ref_unit_tests: the reference's tests/compression/*.cu and
    tests/io.cpp compiled unchanged against this project's include/ and linked
-   to libbz2gpu_b200.so (`make -C oracle ref-tests REF=<reference tree>`,
+   to this library (its static archive, one CUDA runtime in the program as in
+   the reference's own build; `make -C oracle ref-tests REF=<reference tree>`,
    with a small runner in place of GoogleTest).  They call rle1_compress,
    rle2_compress, fbwt, fmtf, make_symbols_table, huffman_build_trees,
    huffman_encode, count_frequencies (launched directly from the test) and
