@@ -52,6 +52,7 @@ _SIGS = {
     "bz2g_compress_batch_bound": (_sz, [_i, _vp, _vp, _vp]),
     "bz2g_free": (None, [_vp]),
     "bz2g_set_engine": (_i, [_i, _i]),
+    "bz2g_set_batch_tuning": (_i, [_i, _vp, _vp, _vp]),
     "bz2g_set_timing": (_i, [_i]),
     "bz2g_last_stats": (_i, [_c.POINTER(_c.c_double), _i]),
     "bz2g_launch_count": (_c.c_int64, []),
@@ -216,10 +217,40 @@ def compress_device(d_in, level: int = 9, block_bytes: int = 900000) -> bytes:
     return _take(out, ln.value)
 
 
+TUNING_FILE = Path(__file__).resolve().parent / "batch_tuning.json"
+_tuning_applied = False
+
+
+def set_batch_tuning(table) -> None:
+    """Batched-form slab shapes by block length: entries {"max_block_len",
+    "slab_blocks", "workers"} (bz2g_set_batch_tuning); an empty list restores
+    the engine's own shape."""
+    global _tuning_applied
+    n = len(table)
+    arr = [(ctypes.c_int * max(n, 1))(*[int(e[k]) for e in table])
+           for k in ("max_block_len", "slab_blocks", "workers")]
+    _check(lib().bz2g_set_batch_tuning(n, *arr))
+    _tuning_applied = True
+
+
+def _apply_committed_tuning() -> None:
+    """The measured table (bzip2gpu_b200/batch_tuning.json, written by
+    bzip2gpu_b200.autotune), applied once before the first batched call."""
+    if _tuning_applied:
+        return
+    if TUNING_FILE.exists():
+        import json
+        set_batch_tuning(json.loads(TUNING_FILE.read_text())["table"])
+    else:
+        set_batch_tuning([])
+
+
 def compress_batch(inputs, levels, block_bytes=None, out=None, on_device=False):
     """Batched form: a list of inputs (host arrays/bytes, or CUDA tensors with
     on_device=True) -> list of .bz2 streams (memoryviews into one buffer).
-    Block size per input: block_bytes[i], or levels[i] * 100000."""
+    Block size per input: block_bytes[i], or levels[i] * 100000.  Slab shapes
+    follow the committed tuning table unless set_batch_tuning() chose one."""
+    _apply_committed_tuning()
     count = len(inputs)
     keep = []
     ptrs = (ctypes.c_void_p * max(count, 1))()

@@ -78,7 +78,24 @@ __device__ __forceinline__ unsigned digit_peers(int dg, bool ok) {
   return peers;
 }
 
-__global__ void __launch_bounds__(256) k_radix_hist(SlabDev d, int shift, const int32_t *list) {
+// The first sort of the packed layout starts from index order, so its first
+// pass builds each tile's items itself from the block's text (read in order:
+// the item at element e of a tile is rotation lt + e) instead of reading
+// them: item = (first 4 bytes of the rotation, big-endian) << 32 | rotation.
+__device__ __forceinline__ uint64_t text_item(const uint8_t *T, int m, int i) {
+  uint32_t k = 0;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    int j = i + q;
+    while (j >= m) j -= m;
+    k = (k << 8) | T[j];
+  }
+  return ((uint64_t)k << 32) | (uint32_t)i;
+}
+
+// gen != 0: the generating first pass (items from the text, see text_item).
+__global__ void __launch_bounds__(256) k_radix_hist(SlabDev d, int shift, const int32_t *list,
+                                                    int gen) {
   __shared__ uint32_t cnt[kRadix];
   const int t = tile_id(list);
   int b, lt;
@@ -87,14 +104,20 @@ __global__ void __launch_bounds__(256) k_radix_hist(SlabDev d, int shift, const 
   cnt[threadIdx.x] = 0;
   __syncthreads();
   const uint64_t *K = d.keys[d.sort_ctl[0]] + d.off[b] + lt;
-  for (int e = threadIdx.x; e < valid; e += blockDim.x)
-    atomicAdd(&cnt[(uint32_t)(K[e] >> shift) & (kRadix - 1)], 1u);
+  const uint8_t *T = d.rle1 + d.off[b];
+  const int m = d.m[b];
+  for (int e = threadIdx.x; e < valid; e += blockDim.x) {
+    const uint64_t it = gen ? text_item(T, m, lt + e) : K[e];
+    atomicAdd(&cnt[(uint32_t)(it >> shift) & (kRadix - 1)], 1u);
+  }
   __syncthreads();
   d.tile_hist[(size_t)t * kRadix + threadIdx.x] = cnt[threadIdx.x];
 }
 
 // Per block: turn tile digit counts into global scatter bases.
-__global__ void __launch_bounds__(256) k_radix_scan(SlabDev d) {
+// force != 0 (the generating pass): the pass runs even if every tile holds one
+// digit only, since it writes the items the later passes read.
+__global__ void __launch_bounds__(256) k_radix_scan(SlabDev d, int force) {
   __shared__ uint32_t scratch[40];
   const int b = blockIdx.x;
   const int len = d.sort_len[b];
@@ -119,7 +142,7 @@ __global__ void __launch_bounds__(256) k_radix_scan(SlabDev d) {
   uint32_t tot;
   uint32_t base = block_excl_sum(run, scratch, &tot);
   int trivial = __syncthreads_or(run == (uint32_t)len);
-  if (!trivial && threadIdx.x == 0) atomicOr(&d.sort_ctl[1], 1);
+  if ((!trivial || force) && threadIdx.x == 0) atomicOr(&d.sort_ctl[1], 1);
   const uint32_t add = (uint32_t)d.off[b] + base;
   for (int k0 = 0; k0 < nt; k0 += kU) {
     uint32_t h[kU];
@@ -138,7 +161,7 @@ __global__ void __launch_bounds__(256) k_radix_scan(SlabDev d) {
 // All of a thread's loads are issued before the ranking starts.
 template <bool kVals>
 __global__ void __launch_bounds__(256, kVals ? 2 : 3)
-    k_radix_scatter(SlabDev d, int shift, int timed, const int32_t *list) {
+    k_radix_scatter(SlabDev d, int shift, int timed, const int32_t *list, int gen) {
   if (!d.sort_ctl[1]) return;
   const int t = tile_id(list);
   int b, lt;
@@ -159,11 +182,21 @@ __global__ void __launch_bounds__(256, kVals ? 2 : 3)
 
   uint64_t key[kTileItems];
   uint32_t val[kTileItems];
+  if (!kVals && gen) {
+    const uint8_t *T = d.rle1 + d.off[b];
+    const int m = d.m[b];
 #pragma unroll
-  for (int i = 0; i < kTileItems; i++) {
-    const int e = w * kWarpSpan + i * 32 + ln;
-    key[i] = e < valid ? K[e] : 0;
-    if (kVals) val[i] = e < valid ? V[e] : 0;
+    for (int i = 0; i < kTileItems; i++) {
+      const int e = w * kWarpSpan + i * 32 + ln;
+      key[i] = e < valid ? text_item(T, m, lt + e) : 0;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < kTileItems; i++) {
+      const int e = w * kWarpSpan + i * 32 + ln;
+      key[i] = e < valid ? K[e] : 0;
+      if (kVals) val[i] = e < valid ? V[e] : 0;
+    }
   }
   for (int i = threadIdx.x; i < kSortWarps * kRadix; i += blockDim.x) wcnt[i] = 0;
   goff[threadIdx.x] = d.tile_hist[(size_t)t * kRadix + threadIdx.x];
@@ -238,204 +271,31 @@ __global__ void k_radix_flip(SlabDev d) {
 
 // Stable sort of each block's elements by key bits [lo, hi), over `grid`
 // tiles (all tiles, or the listed ones).
+// gen: the first pass generates the packed first-sort items from the text.
 void radix_sort(const SlabDev &d, int lo, int hi, int has_vals, cudaStream_t st, int grid,
-                const int32_t *list) {
+                const int32_t *list, bool gen = false) {
   const size_t smem = has_vals ? kScatterSmem : (size_t)kTile * 8 + (size_t)kSortWarps * kRadix * 4 +
                                                     2 * kRadix * 4;
   if (grid <= 0) return;
   for (int shift = lo; shift < hi; shift += kRadixBits) {
-    k_radix_hist<<<grid, 256, 0, st>>>(d, shift, list);
+    const int g = gen && shift == lo;
+    k_radix_hist<<<grid, 256, 0, st>>>(d, shift, list, g);
     BZ_LAUNCH_CHECK();
-    k_radix_scan<<<d.nblocks, 256, 0, st>>>(d);
+    k_radix_scan<<<d.nblocks, 256, 0, st>>>(d, g);
     BZ_LAUNCH_CHECK();
     int timed = -1;
     if (d.kt_on && *d.kt_n < kMaxTimedLaunches) {
       timed = (*d.kt_n)++;
-      d.kt_bpe[timed] = has_vals ? 24 : 16;
+      d.kt_bpe[timed] = has_vals ? 24 : g ? 9 : 16;  // the generating pass reads text bytes
       BZ_CUDA(cudaEventRecord(d.kt_ev[2 * timed], st));
     }
     if (has_vals)
-      k_radix_scatter<true><<<grid, 256, smem, st>>>(d, shift, timed, list);
+      k_radix_scatter<true><<<grid, 256, smem, st>>>(d, shift, timed, list, 0);
     else
-      k_radix_scatter<false><<<grid, 256, smem, st>>>(d, shift, timed, list);
+      k_radix_scatter<false><<<grid, 256, smem, st>>>(d, shift, timed, list, g);
     BZ_LAUNCH_CHECK();
     if (timed >= 0) BZ_CUDA(cudaEventRecord(d.kt_ev[2 * timed + 1], st));
     k_radix_flip<<<1, 1, 0, st>>>(d);
-    BZ_LAUNCH_CHECK();
-  }
-}
-
-// --------------------------------------------------- first sort, by text
-// The first sort orders every rotation by its first 4 bytes with four LSD
-// passes of 8 bits, moving 4-byte rotation indices only: pass p's digit is
-// byte q = 3 - p of the rotation, read from the block's text (a few hundred
-// KB per block, served from L2), so each pass reads and writes 4 bytes per
-// rotation instead of an 8-byte (key, index) item.  Pass 0 starts from index
-// order and reads no input array; the last pass writes the packed item
-// (prefix << 32 | index) that the ranking kernels read.  Indices are below
-// 2^21 here (the packed layout), so a digit and an index share one 32-bit
-// word in shared memory.
-constexpr size_t kTextSmem =
-    (size_t)kTile * 4 + (size_t)kSortWarps * kRadix * 4 + 2 * kRadix * 4;
-
-__device__ __forceinline__ int wrap_add(int i, int q, int m) {
-  int j = i + q;
-  while (j >= m) j -= m;
-  return j;
-}
-
-// The first 4 bytes of rotation i, big-endian.
-__device__ __forceinline__ uint32_t text_prefix4(const uint8_t *T, int m, int i) {
-  uint32_t k = 0;
-#pragma unroll
-  for (int q = 0; q < 4; q++) k = (k << 8) | T[wrap_add(i, q, m)];
-  return k;
-}
-
-__global__ void __launch_bounds__(256) k_text_hist(SlabDev d, int q, int first) {
-  __shared__ uint32_t cnt[kRadix];
-  const int t = blockIdx.x;
-  int b, lt;
-  const int valid = tile_valid(d, t, d.sort_len, &b, &lt);
-  if (valid == 0) return;
-  cnt[threadIdx.x] = 0;
-  __syncthreads();
-  const int m = d.m[b];
-  const uint8_t *T = d.rle1 + d.off[b];
-  const uint32_t *V = d.vals[d.sort_ctl[0]] + d.off[b] + lt;
-  for (int e = threadIdx.x; e < valid; e += blockDim.x) {
-    const int i = first ? lt + e : (int)V[e];
-    atomicAdd(&cnt[T[wrap_add(i, q, m)]], 1u);
-  }
-  __syncthreads();
-  d.tile_hist[(size_t)t * kRadix + threadIdx.x] = cnt[threadIdx.x];
-}
-
-// One stable pass of the first sort (same tile scheme as k_radix_scatter:
-// warp-striped ranking by ballots, local order in shared memory, runs of
-// equal digits written out contiguously).
-__global__ void __launch_bounds__(256, 4)
-    k_text_scatter(SlabDev d, int q, int first, int last, int timed) {
-  const int t = blockIdx.x;
-  int b, lt;
-  const int valid = tile_valid(d, t, d.sort_len, &b, &lt);
-  if (valid == 0) return;
-  if (timed >= 0 && threadIdx.x == 0)
-    atomicAdd((unsigned long long *)&d.kt_elems[timed], (unsigned long long)valid);
-  extern __shared__ __align__(16) uint8_t smem[];
-  uint32_t *sv = reinterpret_cast<uint32_t *>(smem);        // digit << 24 | index
-  uint32_t *wcnt = sv + kTile;                               // [warp][digit]
-  uint32_t *lbase = wcnt + kSortWarps * kRadix;
-  uint32_t *goff = lbase + kRadix;
-  const int cur = d.sort_ctl[0];
-  const int64_t off = d.off[b];
-  const int m = d.m[b];
-  const uint8_t *T = d.rle1 + off;
-  const uint32_t *V = d.vals[cur] + off + lt;
-  const int w = warp_id(), ln = lane_id();
-
-  uint32_t idx[kTileItems];
-#pragma unroll
-  for (int i = 0; i < kTileItems; i++) {
-    const int e = w * kWarpSpan + i * 32 + ln;
-    idx[i] = e < valid ? (first ? (uint32_t)(lt + e) : V[e]) : 0u;
-  }
-  uint32_t dgt[kTileItems];
-#pragma unroll
-  for (int i = 0; i < kTileItems; i++) {
-    const int e = w * kWarpSpan + i * 32 + ln;
-    dgt[i] = e < valid ? T[wrap_add((int)idx[i], q, m)] : 0u;
-  }
-  for (int i = threadIdx.x; i < kSortWarps * kRadix; i += blockDim.x) wcnt[i] = 0;
-  goff[threadIdx.x] = d.tile_hist[(size_t)t * kRadix + threadIdx.x];
-  __syncthreads();
-
-  uint32_t rank2[kTileItems / 2];
-  const unsigned lt_mask = (1u << ln) - 1u;
-#pragma unroll
-  for (int i = 0; i < kTileItems; i++) {
-    const int e = w * kWarpSpan + i * 32 + ln;
-    const bool ok = e < valid;
-    const int dg = (int)dgt[i];
-    const unsigned peers = digit_peers(dg, ok);
-    const uint32_t before = ok ? wcnt[w * kRadix + dg] : 0;
-    const uint32_t r = before + __popc(peers & lt_mask);
-    if (i & 1)
-      rank2[i >> 1] |= r << 16;
-    else
-      rank2[i >> 1] = r;
-    __syncwarp();
-    if (ok && (peers & lt_mask) == 0) wcnt[w * kRadix + dg] = before + __popc(peers);
-    __syncwarp();
-  }
-  __syncthreads();
-  {
-    const int dg = threadIdx.x;
-    uint32_t run = 0;
-    for (int ww = 0; ww < kSortWarps; ww++) run += wcnt[ww * kRadix + dg];
-    __shared__ uint32_t scratch[40];
-    uint32_t tot;
-    const uint32_t lb = block_excl_sum(run, scratch, &tot);
-    uint32_t at = lb;
-    for (int ww = 0; ww < kSortWarps; ww++) {
-      const uint32_t c = wcnt[ww * kRadix + dg];
-      wcnt[ww * kRadix + dg] = at;
-      at += c;
-    }
-    goff[dg] -= lb;
-  }
-  __syncthreads();
-#pragma unroll
-  for (int i = 0; i < kTileItems; i++) {
-    const int e = w * kWarpSpan + i * 32 + ln;
-    if (e < valid) {
-      const uint32_t r = (i & 1) ? rank2[i >> 1] >> 16 : rank2[i >> 1] & 0xffffu;
-      sv[wcnt[w * kRadix + dgt[i]] + r] = (dgt[i] << 24) | idx[i];
-    }
-  }
-  __syncthreads();
-  if (!last) {
-    uint32_t *VO = d.vals[cur ^ 1];
-    for (int k = threadIdx.x; k < valid; k += blockDim.x) {
-      const uint32_t v = sv[k];
-      VO[goff[v >> 24] + (uint32_t)k] = v & 0xffffffu;
-    }
-  } else {
-    uint64_t *KO = d.keys[cur ^ 1];
-    for (int k = threadIdx.x; k < valid; k += blockDim.x) {
-      const uint32_t v = sv[k];
-      const uint32_t i = v & 0xffffffu;
-      KO[goff[v >> 24] + (uint32_t)k] = ((uint64_t)text_prefix4(T, m, (int)i) << 32) | i;
-    }
-  }
-}
-
-__global__ void k_text_flip(SlabDev d) {
-  d.sort_ctl[0] ^= 1;
-  d.sort_ctl[1] = 0;
-}
-
-// The first sort of the packed layout: four passes over rotation indices,
-// ending with packed items in keys[sort_ctl[0]].  Every pass runs (no
-// trivial-pass skip): pass 0 has no input array and the last one writes the
-// packed items.
-void text_sort(const SlabDev &d, cudaStream_t st) {
-  for (int p = 0; p < 4; p++) {
-    const int q = 3 - p;
-    k_text_hist<<<d.ntiles, 256, 0, st>>>(d, q, p == 0);
-    BZ_LAUNCH_CHECK();
-    k_radix_scan<<<d.nblocks, 256, 0, st>>>(d);
-    BZ_LAUNCH_CHECK();
-    int timed = -1;
-    if (d.kt_on && *d.kt_n < kMaxTimedLaunches) {
-      timed = (*d.kt_n)++;
-      d.kt_bpe[timed] = p == 3 ? 12 : 8;  // index read, index (or packed item) written
-      BZ_CUDA(cudaEventRecord(d.kt_ev[2 * timed], st));
-    }
-    k_text_scatter<<<d.ntiles, 256, kTextSmem, st>>>(d, q, p == 0, p == 3, timed);
-    BZ_LAUNCH_CHECK();
-    if (timed >= 0) BZ_CUDA(cudaEventRecord(d.kt_ev[2 * timed + 1], st));
-    k_text_flip<<<1, 1, 0, st>>>(d);
     BZ_LAUNCH_CHECK();
   }
 }
@@ -581,28 +441,28 @@ __global__ void __launch_bounds__(256) k_bwt_flags(SlabDev d, Layout L, int init
     sing += __shfl_xor_sync(0xffffffffu, sing, o);
   }
   if (ln == 0) {
-    red[0][w] = last;
+    const int wvalid = min(max(valid - w * kWarpSpan, 0), kWarpSpan);
+    d.warp_last[t * kSortWarps + w] = last;
+    d.warp_act[t * kSortWarps + w] = wvalid - sing;  // elements in groups of size >= 2
     red[1][w] = heads;
     red[2][w] = sing;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    int l = -1, h = 0, sg = 0;
+    int h = 0, sg = 0;
     for (int q = 0; q < kSortWarps; q++) {
-      l = max(l, red[0][q]);
       h += red[1][q];
       sg += red[2][q];
     }
-    d.tile_a[t] = l;
     d.tile_b[t] = h;
     d.tile_c[t] = sg;
-    d.tile_d[t] = valid - sg;  // elements in groups of size >= 2
   }
 }
 
-// Per block: carry of the last head into each tile, compaction offsets of
-// the active elements, and the stop test: no active element left, no group
-// split by this round (the rest are equal rotations), or prefix >= m.
+// Per block: carry of the last head into each warp span (512 elements of a
+// tile), compaction offsets of the active elements per warp span, and the
+// stop test: no active element left, no group split by this round (the rest
+// are equal rotations), or prefix >= m.
 __global__ void __launch_bounds__(256) k_bwt_rank_block(SlabDev d, int64_t prefix_len) {
   __shared__ int scratch[40];
   __shared__ int sx[256];
@@ -611,29 +471,34 @@ __global__ void __launch_bounds__(256) k_bwt_rank_block(SlabDev d, int64_t prefi
   if (len <= 0) return;
   const int nt = (len + kTile - 1) / kTile;
   const int t0 = (int)(d.off[b] / kTile);
+  const int nw = nt * kSortWarps;
+  int32_t *WL = d.warp_last + (int64_t)t0 * kSortWarps;
+  int32_t *WA = d.warp_act + (int64_t)t0 * kSortWarps;
   int carry = -1, heads = 0, singles = 0, active = 0;
-  for (int base = 0; base < nt; base += 256) {
+  for (int base = 0; base < nw; base += 256) {
     const int k = base + threadIdx.x;
-    const int v = k < nt ? d.tile_a[t0 + k] : -1;
-    const int h = k < nt ? d.tile_b[t0 + k] : 0;
-    const int sg = k < nt ? d.tile_c[t0 + k] : 0;
-    const int ac = k < nt ? d.tile_d[t0 + k] : 0;
+    const int v = k < nw ? WL[k] : -1;
+    const int ac = k < nw ? WA[k] : 0;
     const int inc = block_incl_max(v, scratch, -1);
     sx[threadIdx.x] = inc;
     __syncthreads();
     const int ex = threadIdx.x == 0 ? carry : max(carry, sx[threadIdx.x - 1]);
-    if (k < nt) d.tile_a[t0 + k] = ex;
+    if (k < nw) WL[k] = ex;
     const int c2 = max(carry, sx[255]);
     __syncthreads();
     carry = c2;
     int tot;
-    block_excl_sum(h, scratch, &tot);
-    heads += tot;
-    block_excl_sum(sg, scratch, &tot);
-    singles += tot;
     const int ao = block_excl_sum(ac, scratch, &tot);
-    if (k < nt) d.tile_d[t0 + k] = active + ao;
+    if (k < nw) WA[k] = active + ao;
     active += tot;
+  }
+  for (int base = 0; base < nt; base += 256) {
+    const int k = base + threadIdx.x;
+    int tot;
+    block_excl_sum(k < nt ? d.tile_b[t0 + k] : 0, scratch, &tot);
+    heads += tot;
+    block_excl_sum(k < nt ? d.tile_c[t0 + k] : 0, scratch, &tot);
+    singles += tot;
   }
   if (threadIdx.x == 0) {
     const int m = d.m[b];
@@ -657,8 +522,6 @@ __global__ void __launch_bounds__(256) k_bwt_rank_block(SlabDev d, int64_t prefi
 // position buffers, keyed by their new head (rank of i+h added next round).
 __global__ void __launch_bounds__(256) k_bwt_apply(SlabDev d, Layout L, int initial, int kb,
                                                    const int32_t *list) {
-  __shared__ int wlast[kSortWarps];
-  __shared__ int wact[kSortWarps];
   const int t = tile_id(list);
   int b, lt;
   const int valid = tile_valid(d, t, d.sort_len, &b, &lt);
@@ -671,42 +534,16 @@ __global__ void __launch_bounds__(256) k_bwt_apply(SlabDev d, Layout L, int init
   const int32_t *P = d.kpos[pc] + off;
   const bool compact = d.done[b] == 0;
   const int w = warp_id(), ln = lane_id();
-  // pass 1: per warp, last head and active count
-  int last = -1, act = 0;
-#pragma unroll 4
-  for (int i = 0; i < kTileItems; i++) {
-    const int e = w * kWarpSpan + i * 32 + ln;
-    if (e < valid) {
-      const int k = lt + e;
-      const uint64_t key = key_of(L, K[k]);
-      const bool hd = k == 0 || key != key_of(L, K[k - 1]);
-      const bool tl = k + 1 == len || key_of(L, K[k + 1]) != key;
-      if (hd) last = max(last, initial ? k : P[k]);
-      act += !(hd && tl);
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    last = max(last, __shfl_xor_sync(0xffffffffu, last, o));
-    act += __shfl_xor_sync(0xffffffffu, act, o);
-  }
-  if (ln == 0) {
-    wlast[w] = last;
-    wact[w] = act;
-  }
-  __syncthreads();
-  int carry = d.tile_a[t];
-  int aoff = d.tile_d[t];
-  for (int q = 0; q < w; q++) {
-    carry = max(carry, wlast[q]);
-    aoff += wact[q];
-  }
+  // this warp span's head carry and compaction offset (k_bwt_rank_block)
+  int carry = d.warp_last[t * kSortWarps + w];
+  int aoff = d.warp_act[t * kSortWarps + w];
   uint64_t *KO = d.keys[cur ^ 1] + off;
   uint32_t *VO = d.vals[cur ^ 1] + off;
   int32_t *PO = d.kpos[pc ^ 1] + off;
   int32_t *SA = d.sa + off;
   int32_t *IS = d.isa + off;
   const unsigned lt_mask = (1u << ln) - 1u;
-  // pass 2: heads by a running max, writes, compaction
+  // heads by a running max, writes, compaction
 #pragma unroll 4
   for (int i = 0; i < kTileItems; i++) {
     const int e = w * kWarpSpan + i * 32 + ln;
@@ -804,8 +641,6 @@ void stage_bwt(const SlabDev &d, int max_m, cudaStream_t st) {
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScatterSmem));
     BZ_CUDA(cudaFuncSetAttribute(k_radix_scatter<false>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScatterSmem));
-    BZ_CUDA(cudaFuncSetAttribute(k_text_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kTextSmem));
     smem_configured = true;
   }
   int kb = 1;
@@ -823,7 +658,7 @@ void stage_bwt(const SlabDev &d, int max_m, cudaStream_t st) {
   const Layout first = {packed, packed ? 32 : 0};
   const Layout round = {packed, packed ? kb : 0};
   if (packed) {
-    text_sort(d, st);
+    radix_sort(d, 32, 64, 0, st, d.ntiles, nullptr, true);
   } else {
     k_bwt_keys0<<<d.ntiles, 256, 0, st>>>(d, packed);
     BZ_LAUNCH_CHECK();

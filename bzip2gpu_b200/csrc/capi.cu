@@ -100,6 +100,7 @@ struct EngineKey {
 std::mutex g_eng_mu;
 std::map<EngineKey, std::unique_ptr<Compressor>> g_engines;
 int g_slab = 128, g_workers = 5;
+std::vector<Compressor::BatchTune> g_batch_tune;  // batched form, by block length
 bool g_timing = false;
 thread_local StageTimes g_last_stats;
 
@@ -364,8 +365,32 @@ int bz2g_compress_batch(int count, const uint8_t *const *inputs, const size_t *s
     std::vector<size_t> offs;
     g_last_stats = StageTimes();
     set_format(c);
+    {
+      std::vector<Compressor::BatchTune> tune;
+      {
+        std::lock_guard<std::mutex> g(g_eng_mu);
+        tune = g_batch_tune;
+      }
+      c.set_batch_tuning(tune);
+    }
     c.compress_batch(items.data(), count, on_device != 0, sink, offs, &g_last_stats);
     for (int i = 0; i <= count; i++) offsets[i] = offs[i];
+  });
+}
+
+int bz2g_set_batch_tuning(int n, const int *max_block_len, const int *slab_blocks,
+                          const int *workers) {
+  return guard([&] {
+    BZ_REQUIRE(n >= 0 && (n == 0 || (max_block_len && slab_blocks && workers)), kErrArg,
+               "bad arguments");
+    std::vector<Compressor::BatchTune> t(n);
+    for (int i = 0; i < n; i++) {
+      BZ_REQUIRE(max_block_len[i] > 0 && slab_blocks[i] > 0 && workers[i] > 0, kErrArg,
+                 "batch tuning entries must be positive");
+      t[i] = {max_block_len[i], slab_blocks[i], workers[i]};
+    }
+    std::lock_guard<std::mutex> g(g_eng_mu);
+    g_batch_tune = t;
   });
 }
 

@@ -34,6 +34,7 @@ struct Compressor::Worker {
   int64_t *h_act = nullptr;    // [max_blocks] A
   uint32_t *h_crc = nullptr;
   int32_t *h_err = nullptr;    // the workspace's device error word
+  int slots = 0;               // blocks a slab may hold (stride of the host arrays)
   cudaEvent_t ev[8] = {};
   cudaEvent_t kt_ev[2 * kMaxTimedLaunches] = {};
   cudaEvent_t rt_ev[2 * kMaxRounds] = {};
@@ -68,14 +69,16 @@ Compressor::Compressor(const CompressorConfig &cfg) : cfg_(cfg) {
   if (cfg_.workers < 1) cfg_.workers = 1;
   for (int i = 0; i < cfg_.workers; i++) {
     auto w = std::make_unique<Worker>();
-    w->ws = Workspace::create_for(cfg_.slab_blocks, cfg_.max_block_bytes);
+    w->ws = Workspace::create_for(cfg_.slab_blocks, cfg_.max_block_bytes, kBatchSlots);
+    w->slots = w->ws->max_blocks;
+    const int S = w->slots;
     BZ_CUDA(cudaStreamCreateWithFlags(&w->st, cudaStreamNonBlocking));
     w->h_out_cap = (size_t)w->ws->out_words * 4;
     BZ_CUDA(cudaMallocHost((void **)&w->h_out, w->h_out_cap));
-    BZ_CUDA(cudaMallocHost((void **)&w->h_sizes, sizeof(int64_t) * 2 * cfg_.slab_blocks));
-    BZ_CUDA(cudaMallocHost((void **)&w->h_crc, sizeof(uint32_t) * cfg_.slab_blocks));
-    BZ_CUDA(cudaMallocHost((void **)&w->h_cnt, sizeof(int32_t) * 5 * cfg_.slab_blocks));
-    BZ_CUDA(cudaMallocHost((void **)&w->h_act, sizeof(int64_t) * cfg_.slab_blocks));
+    BZ_CUDA(cudaMallocHost((void **)&w->h_sizes, sizeof(int64_t) * 2 * S));
+    BZ_CUDA(cudaMallocHost((void **)&w->h_crc, sizeof(uint32_t) * S));
+    BZ_CUDA(cudaMallocHost((void **)&w->h_cnt, sizeof(int32_t) * 5 * S));
+    BZ_CUDA(cudaMallocHost((void **)&w->h_act, sizeof(int64_t) * S));
     BZ_CUDA(cudaMallocHost((void **)&w->h_err, sizeof(int32_t)));
     for (auto &e : w->ev) BZ_CUDA(cudaEventCreate(&e));
     for (auto &e : w->kt_ev) BZ_CUDA(cudaEventCreate(&e));
@@ -95,6 +98,25 @@ Compressor::~Compressor() {
   for (uint32_t *c : arena_chunks_) cudaFree(c);
   if (splice_out_) cudaFree(splice_out_);
   if (splice_meta_) cudaFree(splice_meta_);
+}
+
+void Compressor::set_batch_tuning(const std::vector<BatchTune> &table) {
+  std::lock_guard<std::mutex> call_lock(call_mu_);
+  for (const BatchTune &t : table)
+    BZ_REQUIRE(t.max_len > 0 && t.slab_blocks > 0 && t.workers > 0, kErrArg,
+               "batch tuning entries must be positive");
+  tune_ = table;
+  std::sort(tune_.begin(), tune_.end(),
+            [](const BatchTune &a, const BatchTune &b) { return a.max_len < b.max_len; });
+}
+
+// The tuning entry for blocks of `len` raw bytes: the first whose max_len
+// covers it, the last one beyond, the engine's own shape without a table.
+Compressor::BatchTune Compressor::tune_for(int len) const {
+  if (tune_.empty()) return {len, cfg_.slab_blocks, (int)workers_.size()};
+  for (const BatchTune &t : tune_)
+    if (len <= t.max_len) return t;
+  return tune_.back();
 }
 
 // A run of `words` arena words for one slab (caller holds the batch lock):
@@ -341,16 +363,16 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
       if (tm) BZ_CUDA(cudaEventRecord(w.ev[6], w.st));
       BZ_CUDA(cudaMemcpyAsync(w.h_sizes, d.hdr_bits, sizeof(int64_t) * nb, cudaMemcpyDeviceToHost,
                               w.st));
-      BZ_CUDA(cudaMemcpyAsync(w.h_sizes + B, d.pay_bits, sizeof(int64_t) * nb,
+      BZ_CUDA(cudaMemcpyAsync(w.h_sizes + w.slots, d.pay_bits, sizeof(int64_t) * nb,
                               cudaMemcpyDeviceToHost, w.st));
       BZ_CUDA(cudaMemcpyAsync(w.h_crc, d.crc, sizeof(uint32_t) * nb, cudaMemcpyDeviceToHost, w.st));
       BZ_CUDA(cudaMemcpyAsync(w.h_err, d.err, sizeof(int32_t), cudaMemcpyDeviceToHost, w.st));
       if (times) {
         BZ_CUDA(cudaMemcpyAsync(w.h_cnt, d.m, 4 * nb, cudaMemcpyDeviceToHost, w.st));
-        BZ_CUDA(cudaMemcpyAsync(w.h_cnt + B, d.s, 4 * nb, cudaMemcpyDeviceToHost, w.st));
-        BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 2 * B, d.n_sel, 4 * nb, cudaMemcpyDeviceToHost, w.st));
-        BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 3 * B, d.learned, 4 * nb, cudaMemcpyDeviceToHost, w.st));
-        BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 4 * B, d.n_groups, 4 * nb, cudaMemcpyDeviceToHost, w.st));
+        BZ_CUDA(cudaMemcpyAsync(w.h_cnt + w.slots, d.s, 4 * nb, cudaMemcpyDeviceToHost, w.st));
+        BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 2 * w.slots, d.n_sel, 4 * nb, cudaMemcpyDeviceToHost, w.st));
+        BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 3 * w.slots, d.learned, 4 * nb, cudaMemcpyDeviceToHost, w.st));
+        BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 4 * w.slots, d.n_groups, 4 * nb, cudaMemcpyDeviceToHost, w.st));
         BZ_CUDA(cudaMemcpyAsync(w.h_act, d.active_sum, 8 * nb, cudaMemcpyDeviceToHost, w.st));
       }
       if (tm && w.kt_n > 0)
@@ -358,19 +380,19 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
       BZ_CUDA(cudaStreamSynchronize(w.st));
       check_err_word(w.h_err);
       int64_t total = 0;
-      for (int i = 0; i < nb; i++) total += w.h_sizes[i] + w.h_sizes[B + i];
+      for (int i = 0; i < nb; i++) total += w.h_sizes[i] + w.h_sizes[w.slots + i];
       if (times) {
         std::lock_guard<std::mutex> g(mu);
         for (int i = 0; i < nb; i++) {
           tsum.blocks++;
           tsum.n += lens[b0 + i];
           tsum.m += w.h_cnt[i];
-          tsum.s += w.h_cnt[B + i];
-          tsum.g += w.h_cnt[2 * B + i];
+          tsum.s += w.h_cnt[w.slots + i];
+          tsum.g += w.h_cnt[2 * w.slots + i];
           tsum.A += w.h_act[i];
-          tsum.bits += w.h_sizes[B + i];
-          tsum.learned_blocks += w.h_cnt[3 * B + i];
-          tsum.six_table_blocks += w.h_cnt[4 * B + i] == kMaxGroups;
+          tsum.bits += w.h_sizes[w.slots + i];
+          tsum.learned_blocks += w.h_cnt[3 * w.slots + i];
+          tsum.six_table_blocks += w.h_cnt[4 * w.slots + i] == kMaxGroups;
         }
       }
       int64_t start;
@@ -524,8 +546,47 @@ void Compressor::compress_batch(const Item *items, int count, bool on_device, By
   for (int i = 0; i < nb; i++) order[i] = i;
   std::stable_sort(order.begin(), order.end(),
                    [&](int a, int b) { return blks[a].len > blks[b].len; });
-  const int B = cfg_.slab_blocks;
-  const int nslabs = (nb + B - 1) / B;
+  // slabs over the queue: a slab takes up to the tuned block count for its
+  // longest (first) block, fewer where the workspace's capacities end
+  const Workspace &ws0 = *workers_[0]->ws;
+  std::vector<int> slab_at{0};
+  {
+    int64_t raw = 0, elems = 0;
+    int rt = 0, tiles = 0, gt = 0, cnt = 0, cap = 0;
+    for (int q = 0; q < nb; q++) {
+      const BlockNeeds bn = block_needs(blks[order[q]].len, 0);
+      if (cnt > 0 && (cnt == cap || raw + bn.raw > ws0.max_raw || elems + bn.elems > ws0.max_elems ||
+                      rt + bn.raw_tiles > ws0.max_raw_tiles || tiles + bn.tiles > ws0.max_tiles ||
+                      gt + bn.group_tiles > ws0.max_group_tiles)) {
+        slab_at.push_back(q);
+        raw = elems = 0;
+        rt = tiles = gt = cnt = 0;
+      }
+      if (cnt == 0) cap = std::min(tune_for(blks[order[q]].len).slab_blocks, ws0.max_blocks);
+      raw += bn.raw;
+      elems += bn.elems;
+      rt += bn.raw_tiles;
+      tiles += bn.tiles;
+      gt += bn.group_tiles;
+      cnt++;
+    }
+    if (nb > 0) slab_at.push_back(nb);
+  }
+  const int nslabs = (int)slab_at.size() - 1;
+  // worker streams: the tuned count for the byte-weighted median block length
+  int tuned_workers = (int)workers_.size();
+  if (nb > 0) {
+    int64_t half = 0, acc = 0;
+    for (const Blk &bk : blks) half += bk.len;
+    half /= 2;
+    for (int q = nb - 1; q >= 0; q--) {  // shortest first
+      acc += blks[order[q]].len;
+      if (acc >= half) {
+        tuned_workers = tune_for(blks[order[q]].len).workers;
+        break;
+      }
+    }
+  }
   // arena: every block's bits, word-aligned, in chunks kept by the engine
   size_t chunk = 0;
   int64_t chunk_used = 0;
@@ -538,7 +599,7 @@ void Compressor::compress_batch(const Item *items, int count, bool on_device, By
   auto work = [&](Worker &w) {
     BZ_CUDA(cudaSetDevice(device_));
     SlabPlan plan;
-    std::vector<int> lens(B);
+    std::vector<int> lens(w.slots);
     for (;;) {
       {
         std::lock_guard<std::mutex> g(mu);
@@ -546,7 +607,7 @@ void Compressor::compress_batch(const Item *items, int count, bool on_device, By
       }
       const int k = next_slab.fetch_add(1);
       if (k >= nslabs) return;
-      const int s0 = k * B, ns = std::min(B, nb - s0);
+      const int s0 = slab_at[k], ns = slab_at[k + 1] - s0;
       for (int i = 0; i < ns; i++) lens[i] = blks[order[s0 + i]].len;
       plan.build(lens.data(), ns);
       w.ws->upload_plan(plan, w.st);
@@ -574,16 +635,16 @@ void Compressor::compress_batch(const Item *items, int count, bool on_device, By
       stage_sizes(d, w.st);
       BZ_CUDA(cudaMemcpyAsync(w.h_sizes, d.hdr_bits, sizeof(int64_t) * ns, cudaMemcpyDeviceToHost,
                               w.st));
-      BZ_CUDA(cudaMemcpyAsync(w.h_sizes + B, d.pay_bits, sizeof(int64_t) * ns,
+      BZ_CUDA(cudaMemcpyAsync(w.h_sizes + w.slots, d.pay_bits, sizeof(int64_t) * ns,
                               cudaMemcpyDeviceToHost, w.st));
       BZ_CUDA(cudaMemcpyAsync(w.h_crc, d.crc, sizeof(uint32_t) * ns, cudaMemcpyDeviceToHost, w.st));
       BZ_CUDA(cudaMemcpyAsync(w.h_err, d.err, sizeof(int32_t), cudaMemcpyDeviceToHost, w.st));
       if (times) {
         BZ_CUDA(cudaMemcpyAsync(w.h_cnt, d.m, 4 * ns, cudaMemcpyDeviceToHost, w.st));
-        BZ_CUDA(cudaMemcpyAsync(w.h_cnt + B, d.s, 4 * ns, cudaMemcpyDeviceToHost, w.st));
-        BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 2 * B, d.n_sel, 4 * ns, cudaMemcpyDeviceToHost, w.st));
-        BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 3 * B, d.learned, 4 * ns, cudaMemcpyDeviceToHost, w.st));
-        BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 4 * B, d.n_groups, 4 * ns, cudaMemcpyDeviceToHost, w.st));
+        BZ_CUDA(cudaMemcpyAsync(w.h_cnt + w.slots, d.s, 4 * ns, cudaMemcpyDeviceToHost, w.st));
+        BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 2 * w.slots, d.n_sel, 4 * ns, cudaMemcpyDeviceToHost, w.st));
+        BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 3 * w.slots, d.learned, 4 * ns, cudaMemcpyDeviceToHost, w.st));
+        BZ_CUDA(cudaMemcpyAsync(w.h_cnt + 4 * w.slots, d.n_groups, 4 * ns, cudaMemcpyDeviceToHost, w.st));
         BZ_CUDA(cudaMemcpyAsync(w.h_act, d.active_sum, 8 * ns, cudaMemcpyDeviceToHost, w.st));
       }
       BZ_CUDA(cudaStreamSynchronize(w.st));
@@ -593,12 +654,12 @@ void Compressor::compress_batch(const Item *items, int count, bool on_device, By
       uint32_t *arena;
       {
         std::lock_guard<std::mutex> g(mu);
-        for (int i = 0; i < ns; i++) words += (w.h_sizes[i] + w.h_sizes[B + i] + 31) / 32;
+        for (int i = 0; i < ns; i++) words += (w.h_sizes[i] + w.h_sizes[w.slots + i] + 31) / 32;
         arena = arena_take(words, &chunk, &chunk_used, &base);
         int64_t at = base;
         for (int i = 0; i < ns; i++) {
           Blk &bk = blks[order[s0 + i]];
-          const int64_t bits = w.h_sizes[i] + w.h_sizes[B + i];
+          const int64_t bits = w.h_sizes[i] + w.h_sizes[w.slots + i];
           bk.arena_word = at;
           bk.src = arena + at;
           bk.bits = bits;
@@ -610,12 +671,12 @@ void Compressor::compress_batch(const Item *items, int count, bool on_device, By
             tsum.blocks++;
             tsum.n += lens[i];
             tsum.m += w.h_cnt[i];
-            tsum.s += w.h_cnt[B + i];
-            tsum.g += w.h_cnt[2 * B + i];
+            tsum.s += w.h_cnt[w.slots + i];
+            tsum.g += w.h_cnt[2 * w.slots + i];
             tsum.A += w.h_act[i];
-            tsum.bits += w.h_sizes[B + i];
-            tsum.learned_blocks += w.h_cnt[3 * B + i];
-            tsum.six_table_blocks += w.h_cnt[4 * B + i] == kMaxGroups;
+            tsum.bits += w.h_sizes[w.slots + i];
+            tsum.learned_blocks += w.h_cnt[3 * w.slots + i];
+            tsum.six_table_blocks += w.h_cnt[4 * w.slots + i] == kMaxGroups;
           }
       }
       // block starts (bits) in the arena, staged through the sizes buffer
@@ -628,7 +689,7 @@ void Compressor::compress_batch(const Item *items, int count, bool on_device, By
   };
 
   if (nslabs > 0) {
-    const int nw = std::min<int>((int)workers_.size(), nslabs);
+    const int nw = std::max(1, std::min({(int)workers_.size(), nslabs, tuned_workers}));
     std::vector<std::thread> th;
     auto guarded = [&](Worker &w) {
       try {

@@ -16,6 +16,10 @@ namespace mlp {
 struct SelectorTap;
 }
 
+// Block slots of every worker's workspace: the batched form packs up to this
+// many short blocks into one slab.
+constexpr int kBatchSlots = 1024;
+
 struct StageTimes {
   // milliseconds of device time summed over slabs (CUDA events on each
   // worker's stream), filled when timing is enabled
@@ -113,6 +117,16 @@ class Compressor {
   };
   void compress_batch(const Item *items, int count, bool on_device, ByteSink &out,
                       std::vector<size_t> &offsets, StageTimes *times = nullptr);
+  // Batched form tuning, by block length: a slab whose longest block has at
+  // most max_len raw bytes takes up to slab_blocks blocks (within the
+  // workspace's capacities), and a call runs on up to `workers` worker
+  // streams (chosen by its byte-weighted median block length).  Entries are
+  // kept sorted by max_len; an empty table keeps config().slab_blocks blocks
+  // per slab and every worker.
+  struct BatchTune {
+    int max_len, slab_blocks, workers;
+  };
+  void set_batch_tuning(const std::vector<BatchTune> &table);
   const CompressorConfig &config() const { return cfg_; }
   int device() const { return device_; }
 
@@ -122,11 +136,13 @@ class Compressor {
            ByteSink &out, StageTimes *times, bool part = false, int64_t *part_bits = nullptr,
            uint32_t *part_crc = nullptr);
   uint32_t *arena_take(int64_t words, size_t *chunk, int64_t *used, int64_t *base);
+  BatchTune tune_for(int len) const;
   static constexpr int64_t kArenaChunkWords = int64_t(1) << 28;  // 1 GiB
   CompressorConfig cfg_;
   int device_ = 0;
   std::vector<std::unique_ptr<Worker>> workers_;
   std::mutex call_mu_;                         // one call at a time per engine
+  std::vector<BatchTune> tune_;               // batched form: slab shapes by block length
   std::vector<uint32_t *> arena_chunks_;       // batched form: block bits
   std::vector<int64_t> arena_chunk_words_;
   uint32_t *splice_out_ = nullptr;             // batched form: spliced streams

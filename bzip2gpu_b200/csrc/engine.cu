@@ -121,6 +121,8 @@ Workspace::Workspace(int mb, int64_t mr, int64_t me, int mt, int mrt, int mgt)
     dev.tile_c = (int32_t *)alloc(T * 4);
     dev.tile_d = (int32_t *)alloc(T * 4);
     dev.tile_list = (int32_t *)alloc(T * 4);
+    dev.warp_last = (int32_t *)alloc(((int64_t)mt + 1) * (kTileThreads / 32) * 4);
+    dev.warp_act = (int32_t *)alloc(((int64_t)mt + 1) * (kTileThreads / 32) * 4);
     dev.tile_hist = (uint32_t *)alloc((int64_t)mt * 256 * 4);
     dev.tile_last = (int32_t *)alloc((int64_t)mt * 256 * 4);
     dev.gt_bits = (uint32_t *)alloc(((int64_t)mgt + 1) * 4);
@@ -212,7 +214,7 @@ void Workspace::upload_plan(const SlabPlan &p, cudaStream_t st) {
   dev.n_group_tiles = (int)p.gt_block.size();
 }
 
-Workspace *Workspace::create_for(int max_blocks, int64_t max_block_bytes) {
+Workspace *Workspace::create_for(int max_blocks, int64_t max_block_bytes, int block_slots) {
   const int64_t nb = std::max<int64_t>(max_block_bytes, 1);
   const int64_t cap = align_up(std::max<int64_t>(rle1_bound(nb), 1), kTile);
   const int64_t E = (int64_t)max_blocks * cap;
@@ -220,7 +222,7 @@ Workspace *Workspace::create_for(int max_blocks, int64_t max_block_bytes) {
   const int mt = (int)(E / kTile);
   const int mrt = (int)(max_blocks * ((nb + kRawTile - 1) / kRawTile));
   const int mgt = (int)(max_blocks * ((groups_bound(nb) + kGroupTile - 1) / kGroupTile));
-  return new Workspace(max_blocks, R, E, mt, mrt, mgt);
+  return new Workspace(std::max(max_blocks, block_slots), R, E, mt, mrt, mgt);
 }
 
 }  // namespace bz2g

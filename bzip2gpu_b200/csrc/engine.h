@@ -88,6 +88,8 @@ struct SlabDev {
   int32_t *sort_len, *done, *ngroups;  // BWT control (ngroups: groups among active rotations)
   int32_t *act_len;                    // BWT: active rotations entering the next round
   int32_t *tile_list;                  // BWT: tiles holding active rotations [ntiles]
+  int32_t *warp_last, *warp_act;       // BWT: per 512-element warp span [ntiles * 8]: last
+                                       // head, then its carry; active count, then offset
   int64_t *active_sum;                 // A: rotations in non-singleton groups, summed over rounds
   int32_t *pstat;                      // [nblocks * 8]: heads and singletons at prefix 1,2,4,8
   int64_t *hdr_bits, *pay_bits, *blk_start;
@@ -129,8 +131,11 @@ class Workspace {
   Workspace(int max_blocks, int64_t max_raw, int64_t max_elems, int max_tiles,
             int max_raw_tiles, int max_group_tiles);
   ~Workspace();
-  // Sized for slabs of up to max_blocks blocks of up to max_block_bytes each.
-  static Workspace *create_for(int max_blocks, int64_t max_block_bytes);
+  // Sized for slabs of up to max_blocks blocks of up to max_block_bytes each;
+  // per-block arrays for max(max_blocks, block_slots) blocks, so a slab of
+  // shorter blocks can hold more of them (within the same element, raw-byte
+  // and tile capacities).
+  static Workspace *create_for(int max_blocks, int64_t max_block_bytes, int block_slots = 0);
   Workspace(const Workspace &) = delete;
   Workspace &operator=(const Workspace &) = delete;
 

@@ -303,23 +303,46 @@ __global__ void k_huff_judge(SlabDev d) {
   init_tables(d, b);
 }
 
-// Canonical codes (src/compression/huffman.cu:135-146,352-362).
-__global__ void k_huff_codes(SlabDev d) {
+// Canonical codes (src/compression/huffman.cu:135-146,352-362): for each
+// length from the shortest to the longest, the symbols of that length in
+// symbol order take consecutive codes; the next length starts at twice the
+// running code.  One warp per table: lane l holds symbols l, l + 32, ...; a
+// ballot per 32 symbols gives each symbol its place among that length's.
+constexpr int kCodeSlots = (kMaxAlpha + 31) / 32;  // 9
+
+__global__ void __launch_bounds__(kMaxGroups * 32) k_huff_codes(SlabDev d) {
   const int b = blockIdx.x;
-  const int t = threadIdx.x;
+  const int t = warp_id();
+  const int ln = lane_id();
   if (t >= d.n_groups[b]) return;
   const int alpha = d.n_in_use[b] + 2;
   const uint8_t *len = d.len + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
   int32_t *code = d.code + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
+  int lv[kCodeSlots];
   int mn = 32, mx = 0;
-  for (int v = 0; v < alpha; v++) {
-    mn = min(mn, (int)len[v]);
-    mx = max(mx, (int)len[v]);
+#pragma unroll
+  for (int q = 0; q < kCodeSlots; q++) {
+    const int v = 32 * q + ln;
+    lv[q] = v < alpha ? (int)len[v] : -1;
+    if (v < alpha) {
+      mn = min(mn, lv[q]);
+      mx = max(mx, lv[q]);
+    }
   }
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  const unsigned below = (1u << ln) - 1u;
   int vec = 0;
   for (int l = mn; l <= mx; l++) {
-    for (int v = 0; v < alpha; v++)
-      if (len[v] == l) code[v] = vec++;
+#pragma unroll
+    for (int q = 0; q < kCodeSlots; q++) {
+      const bool hit = lv[q] == l;
+      const unsigned bal = __ballot_sync(0xffffffffu, hit);
+      if (hit) code[32 * q + ln] = vec + __popc(bal & below);
+      vec += __popc(bal);
+    }
     vec <<= 1;
   }
 }
@@ -375,7 +398,7 @@ void stage_huffman(const SlabDev &d, cudaStream_t st, const uint8_t *learned, in
       lengths_pass(d, kPlainRound, r, st);
     }
   }
-  k_huff_codes<<<d.nblocks, 32, 0, st>>>(d);
+  k_huff_codes<<<d.nblocks, kMaxGroups * 32, 0, st>>>(d);
   BZ_LAUNCH_CHECK();
 }
 

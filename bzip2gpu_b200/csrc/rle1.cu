@@ -182,11 +182,6 @@ __global__ void __launch_bounds__(256) k_rle1_block_carry(SlabDev d, const int *
   }
 }
 
-__device__ __forceinline__ int rle1_count_of(int j, int cut) {
-  int q = j % cut;
-  return q < 3 ? 1 : (q == 3 ? 2 : 0);
-}
-
 __global__ void __launch_bounds__(256) k_rle1_count(SlabDev d) {
   __shared__ __align__(16) uint8_t sb[kRawTile + 16];
   __shared__ int scratch[40];
@@ -207,10 +202,14 @@ __global__ void __launch_bounds__(256) k_rle1_count(SlabDev d) {
   __syncthreads();
   if (lane_id() == 0) ex = warp_id() == 0 ? -1 : wl[warp_id() - 1];
   int cur = max(ex, d.tile_b[t]);
+  // position of each byte in its run, modulo the cut, tracked incrementally
+  const int cut = d.run_cut;
+  int q = nv > 0 ? (st + p0 - cur) % cut : 0;
   int cnt = 0;
   for (int k = 0; k < nv; k++) {
-    if ((sm >> k) & 1u) cur = st + p0 + k;
-    cnt += rle1_count_of(st + p0 + k - cur, d.run_cut);
+    if ((sm >> k) & 1u) q = 0;
+    cnt += q < 3 ? 1 : (q == 3 ? 2 : 0);
+    if (++q == cut) q = 0;
   }
   int total;
   block_excl_sum(cnt, scratch, &total);
@@ -274,32 +273,47 @@ __global__ void __launch_bounds__(256) k_rle1_write(SlabDev d) {
       if ((sm >> k) & 1u) cur = st + p0 + k;
     }
   }
+  // each byte's position in its run as (chunk, position in the chunk of
+  // `cut` bytes), tracked incrementally from one division per thread
+  const int cut = d.run_cut;
+  int q0 = 0, jd0 = 0;
+  if (nv > 0) {
+    const int j0 = st + p0 - before;
+    jd0 = j0 / cut;
+    q0 = j0 - jd0 * cut;
+  }
   int cnt = 0;
   {
-    int cur = before;
+    int q = q0;
     for (int k = 0; k < nv; k++) {
-      if ((sm >> k) & 1u) cur = st + p0 + k;
-      cnt += rle1_count_of(st + p0 + k - cur, d.run_cut);
+      if ((sm >> k) & 1u) q = 0;
+      cnt += q < 3 ? 1 : (q == 3 ? 2 : 0);
+      if (++q == cut) q = 0;
     }
   }
   int tot;
   int o = block_excl_sum(cnt, scratch, &tot);
   uint8_t *out = so + o;
-  const int cut = d.run_cut;
-  int cur = before;
+  int cur = before, q = q0, jd = jd0;
 #pragma unroll
   for (int k = 0; k < kTileItems; k++) {
     if (k < nv) {
-      if ((sm >> k) & 1u) cur = st + p0 + k;
-      int j = st + p0 + k - cur;
-      int q = j % cut;
+      if ((sm >> k) & 1u) {
+        cur = st + p0 + k;
+        q = 0;
+        jd = 0;
+      }
       if (q < 3) {
         *out++ = c[k];
       } else if (q == 3) {
-        int run_len = ends[k] - cur;
-        int chunk_len = min(cut, run_len - (j / cut) * cut);
+        const int run_len = ends[k] - cur;
+        const int chunk_len = min(cut, run_len - jd * cut);
         *out++ = c[k];
         *out++ = (uint8_t)(chunk_len - 4);
+      }
+      if (++q == cut) {
+        q = 0;
+        jd++;
       }
     }
   }

@@ -103,6 +103,15 @@ size_t bz2g_compress_batch_bound(int count, const size_t *sizes, const int *leve
  * blocks per slab and worker streams (default 128 and 5; about 6.5 GB of
  * device memory per worker).  0 keeps the current value. */
 int bz2g_set_engine(int slab_blocks, int workers);
+/* Batched-form tuning (no counterpart in the reference; the table that
+ * bzip2gpu_b200/autotune.py measures and commits): entry i says that a slab
+ * whose longest block has at most max_block_len[i] raw bytes takes up to
+ * slab_blocks[i] blocks (at most 1024, and within the engine's memory per
+ * slab), and that a batch whose byte-weighted median block falls in entry i
+ * runs on up to workers[i] worker streams.  n = 0 restores the engine's own
+ * shape (bz2g_set_engine).  Outputs are identical whatever the tuning. */
+int bz2g_set_batch_tuning(int n, const int *max_block_len, const int *slab_blocks,
+                          const int *workers);
 
 /* Measurement (no counterpart in the reference, which only prints wall-clock
  * Stopwatch lines, include/stopwatch.h:12-42).  bz2g_set_timing(1) records

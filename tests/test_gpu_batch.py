@@ -44,3 +44,33 @@ def test_batch_from_device_memory(torch_cuda):
     streams = B.compress_batch(d, [lv for _, lv in items], on_device=True)
     for (a, lv), s in zip(items, streams):
         assert bytes(s) == oracle.compress(a, lv, lv * 100000)
+
+
+@pytest.mark.parametrize("table", [
+    [{"max_block_len": 300000, "slab_blocks": 3, "workers": 2},
+     {"max_block_len": 900000, "slab_blocks": 1, "workers": 5}],
+    [{"max_block_len": 900000, "slab_blocks": 1024, "workers": 1}],
+])
+def test_batch_tuning_changes_no_byte(torch_cuda, table):
+    # slab shapes from a tuning table (tiny slabs, single-block slabs, slabs as
+    # large as the workspace allows, one worker) give the same streams
+    items = _inputs()
+    data = [a for a, _ in items]
+    levels = [lv for _, lv in items]
+    ref = [bytes(s) for s in B.compress_batch(data, levels)]
+    try:
+        B.set_batch_tuning(table)
+        got = [bytes(s) for s in B.compress_batch(data, levels)]
+    finally:
+        B.set_batch_tuning([])
+        B._tuning_applied = False
+    assert got == ref
+
+
+def test_committed_tuning_table_is_well_formed():
+    import json
+    if not B.TUNING_FILE.exists():
+        pytest.skip("no tuning table committed")
+    t = json.loads(B.TUNING_FILE.read_text())["table"]
+    assert t and all(e["max_block_len"] > 0 and 1 <= e["slab_blocks"] <= 1024 and
+                     e["workers"] >= 1 for e in t)
