@@ -143,7 +143,8 @@ Workspace::Workspace(int mb, int64_t mr, int64_t me, int mt, int mrt, int mgt)
     dev.learned = (int32_t *)alloc(B * 4);
     dev.rfreq_m = (int32_t *)alloc(B * kMaxGroups * kMaxAlpha * 4);
     dev.len2 = (uint8_t *)alloc(B * kMaxGroups * kMaxAlpha);
-    dev.est_sp = (int64_t *)alloc(B * 8);
+    dev.sel2 = (uint8_t *)alloc(E / 32 + 64);
+    dev.rfreq2 = (int32_t *)alloc(B * kMaxGroups * kMaxAlpha * 4);
     dev.plain_left = (int32_t *)alloc(B * 4);
     dev.err = (int32_t *)alloc(64);
     BZ_CUDA(cudaMemset(dev.err, 0, 64));

@@ -81,8 +81,11 @@ struct SlabDev {
   int32_t *rfreq;                      // [nblocks * 6 * 258]
   int32_t *learned;                    // [nblocks]: table selection by the learned selector
   int32_t *rfreq_m;                    // [nblocks * 6 * 258]: the MLP's per-table counts
-  uint8_t *len2;                       // [nblocks * 6 * 258]: single-pass estimate's tables
-  int64_t *est_sp;                     // [nblocks]: single-pass estimate (bits)
+  uint8_t *len2;                       // [nblocks * 6 * 258]: learned form, the plain
+                                       // selector's tables of learned blocks
+  uint8_t *sel2;                       // learned form: the plain selector's second-pass
+                                       // selectors of learned blocks (sel layout)
+  int32_t *rfreq2;                     // [nblocks * 6 * 258]: their per-table counts
   int32_t *plain_left;                 // [nblocks]: plain passes still to run (learned form)
   int32_t *err;                        // device error word of the tensor-core kernels
   int32_t *sort_len, *done, *ngroups;  // BWT control (ngroups: groups among active rotations)

@@ -83,6 +83,9 @@ __global__ void k_huff_init(SlabDev d, int learned_mode) {
 // One thread per 50-symbol group.  Costs of all tables are packed in 10-bit
 // fields of one 64-bit word per symbol (50 * 17 < 1024), so a group's six
 // costs are one 64-bit sum.
+// grid.y == 2 (the learned form's second passes): y = 1 runs, for the
+// learned blocks, the plain selector's second pass over its first-pass
+// tables (len2) into sel2 / rfreq2, beside y = 0's pass over len.
 __global__ void __launch_bounds__(kGroupTile) k_huff_select(SlabDev d, int which, int round) {
   __shared__ uint16_t sy[kGroupTile * kGroupSize];
   __shared__ uint64_t plen[kMaxAlpha];
@@ -91,7 +94,12 @@ __global__ void __launch_bounds__(kGroupTile) k_huff_select(SlabDev d, int which
   const int b = d.gt_block[gt];
   const int g0 = d.gt_first[gt];
   const int nsel = d.n_sel[b];
-  if (g0 >= nsel || !serves(d, b, which, round)) return;
+  const bool second = blockIdx.y == 1;
+  if (g0 >= nsel) return;
+  if (second ? !d.learned[b] : !serves(d, b, which, round)) return;
+  const uint8_t *len_src = second ? d.len2 : d.len;
+  uint8_t *sel_dst = second ? d.sel2 : d.sel;
+  int32_t *rf_dst = second ? d.rfreq2 : d.rfreq;
   const int ng_here = min(kGroupTile, nsel - g0);
   const int s = d.s[b];
   const int ngrp = d.n_groups[b];
@@ -99,7 +107,7 @@ __global__ void __launch_bounds__(kGroupTile) k_huff_select(SlabDev d, int which
   const int64_t off = d.off[b];
   const int sym0 = g0 * kGroupSize;
   const int nsym = min(s, (g0 + ng_here) * kGroupSize) - sym0;
-  const uint8_t *len = d.len + (size_t)b * kMaxGroups * kMaxAlpha;
+  const uint8_t *len = len_src + (size_t)b * kMaxGroups * kMaxAlpha;
   for (int i = threadIdx.x; i < nsym; i += blockDim.x) sy[i] = d.rle2[off + sym0 + i];
   for (int v = threadIdx.x; v < kMaxAlpha; v += blockDim.x) {
     uint64_t p = 0;
@@ -124,11 +132,11 @@ __global__ void __launch_bounds__(kGroupTile) k_huff_select(SlabDev d, int which
         bt = t;
       }
     }
-    d.sel[off / 32 + g0 + g] = (uint8_t)bt;
+    sel_dst[off / 32 + g0 + g] = (uint8_t)bt;
     for (int i = a; i < e; i++) atomicAdd(&rf[bt * kMaxAlpha + sy[i]], 1);
   }
   __syncthreads();
-  int32_t *rfreq = d.rfreq + (size_t)b * kMaxGroups * kMaxAlpha;
+  int32_t *rfreq = rf_dst + (size_t)b * kMaxGroups * kMaxAlpha;
   for (int i = threadIdx.x; i < ngrp * kMaxAlpha; i += blockDim.x)
     if (rf[i]) atomicAdd(&rfreq[i], rf[i]);
 }
@@ -144,9 +152,11 @@ constexpr int kNodeN = kMaxAlpha * 2;
 
 __device__ __forceinline__ uint32_t hw(uint64_t e) { return (uint32_t)(e >> 32); }
 
-// split != 0 (the learned form's first table build, grid.y = 2): y = 0 builds
-// every block's tables from its counts (the MLP's counts for learned blocks),
-// y = 1 builds the single-pass estimate's tables of learned blocks into len2.
+// split (the learned form, grid.y = 2): y = 0 builds every block's tables
+// into len, y = 1 the learned blocks' plain-selector tables into len2.
+// split == 1 (first build): y = 0 from the counts of the first pass (the
+// MLP's counts for learned blocks), y = 1 from the first plain pass's counts.
+// split == 2 (second build): y = 0 from rfreq, y = 1 from rfreq2.
 __global__ void __launch_bounds__(kMaxGroups * 32) k_huff_lengths(SlabDev d, int which, int round,
                                                                   int split) {
   __shared__ __align__(16) uint64_t heap_s[kMaxGroups][kHeapN + 2];
@@ -161,10 +171,11 @@ __global__ void __launch_bounds__(kMaxGroups * 32) k_huff_lengths(SlabDev d, int
   uint8_t *len_base = d.len;
   if (split) {
     if (blockIdx.y == 0) {
-      if (d.learned[b]) rf_base = d.rfreq_m;
+      if (split == 1 && d.learned[b]) rf_base = d.rfreq_m;
     } else {
       if (!d.learned[b]) return;
       len_base = d.len2;
+      if (split == 2) rf_base = d.rfreq2;
     }
   } else if (!serves(d, b, which, round)) {
     return;
@@ -262,10 +273,11 @@ __global__ void __launch_bounds__(kMaxGroups * 32) k_huff_lengths(SlabDev d, int
 // Predicted coded size of a block's selection (bits): payload from the
 // per-table counts and lengths, plus the table headers (5-bit start, 2 bits
 // per unit of length change, 1 terminator bit per symbol).  One warp.
-__device__ int64_t predicted_bits(const SlabDev &d, int b, const uint8_t *len_base) {
+__device__ int64_t predicted_bits(const SlabDev &d, int b, const uint8_t *len_base,
+                                  const int32_t *rf_base) {
   const int ng = d.n_groups[b];
   const int alpha = d.n_in_use[b] + 2;
-  const int32_t *rf = d.rfreq + (size_t)b * kMaxGroups * kMaxAlpha;
+  const int32_t *rf = rf_base + (size_t)b * kMaxGroups * kMaxAlpha;
   const uint8_t *len = len_base + (size_t)b * kMaxGroups * kMaxAlpha;
   int64_t e = 0;
   for (int t = 0; t < ng; t++)
@@ -278,29 +290,24 @@ __device__ int64_t predicted_bits(const SlabDev &d, int b, const uint8_t *len_ba
   return e + 5 * ng;
 }
 
-// Learned form: the single-pass estimate (first plain pass over the initial
-// tables, its tables in len2).
-__global__ void k_huff_estimate(SlabDev d) {
-  const int b = blockIdx.x;
-  if (!d.learned[b]) return;
-  const int64_t e = predicted_bits(d, b, d.len2);
-  if (lane_id() == 0) d.est_sp[b] = e;
-}
-
-// Learned form, after the exact selection pass and its tables: a block whose
-// predicted size exceeds the single-pass estimate falls back to the plain
-// selector (initial tables, then 4 passes in the plain rounds).
+// Learned form, after the second passes: a learned block whose predicted
+// size exceeds that of the plain selector's first two passes takes the
+// plain two-pass selection (sel2, len2) instead.
 __global__ void k_huff_judge(SlabDev d) {
   const int b = blockIdx.x;
   if (!d.learned[b]) return;
-  const int64_t e = predicted_bits(d, b, d.len);
-  if (e <= d.est_sp[b]) return;
-  __syncwarp();
+  const int64_t el = predicted_bits(d, b, d.len, d.rfreq);
+  const int64_t ep = predicted_bits(d, b, d.len2, d.rfreq2);
+  if (el <= ep) return;
+  const size_t tb = (size_t)b * kMaxGroups * kMaxAlpha;
+  for (int i = lane_id(); i < kMaxGroups * kMaxAlpha; i += 32) d.len[tb + i] = d.len2[tb + i];
+  const int64_t s0 = d.off[b] / 32;
+  const int nsel = d.n_sel[b];
+  for (int g = lane_id(); g < nsel; g += 32) d.sel[s0 + g] = d.sel2[s0 + g];
   if (lane_id() == 0) {
     d.learned[b] = 0;
-    d.plain_left[b] = kIters;
+    d.plain_left[b] = 0;
   }
-  init_tables(d, b);
 }
 
 // Canonical codes (src/compression/huffman.cu:135-146,352-362): for each
@@ -363,12 +370,15 @@ void lengths_pass(const SlabDev &d, int which, int round, cudaStream_t st) {
 
 // Plain form (the reference's): initial tables, then 4 passes of selection
 // and code lengths.
-// Learned form, blocks with six tables: pass 1 over the initial tables gives
-// the plain single-pass estimate; the MLP's choice gives the first tables;
-// one exact selection pass and code lengths follow; if the predicted size is
-// above the single-pass estimate the block falls back to the plain selector.
-// Blocks with fewer tables run the plain passes in the same launches
-// (launches that serve none of a slab's blocks return at once).
+// Learned form, blocks with six tables: the MLP's choice gives the first
+// tables, one exact selection pass and code lengths follow.  Beside them the
+// plain selector runs its first two passes (initial tables, then its
+// first-pass tables); that is the judge: a block whose learned tables predict
+// a larger size takes the plain two-pass selection.  The judge thus costs no
+// launch of its own, and the stage runs two rounds of selection and code
+// lengths where the plain form runs four.  Blocks with fewer tables run the
+// plain passes in the same launches (launches that serve none of a slab's
+// blocks return at once).
 void stage_huffman(const SlabDev &d, cudaStream_t st, const uint8_t *learned, int plain_passes,
                    uint8_t *mlp_sel_out, size_t mlp_sel_bytes) {
   k_huff_init<<<d.nblocks, 32, 0, st>>>(d, learned ? 1 : 0);
@@ -381,19 +391,25 @@ void stage_huffman(const SlabDev &d, cudaStream_t st, const uint8_t *learned, in
   } else {
     const size_t rf_bytes = sizeof(int32_t) * kMaxGroups * kMaxAlpha * d.nblocks;
     BZ_CUDA(cudaMemsetAsync(d.rfreq_m, 0, rf_bytes, st));
-    select_pass(d, kAll, 0, st);
+    select_pass(d, kAll, 0, st);  // the plain selector's first pass, every block
     mlp::launch_select(d, learned, nullptr, nullptr, d.rfreq_m, st);
     if (mlp_sel_out)
       BZ_CUDA(cudaMemcpyAsync(mlp_sel_out, d.sel, mlp_sel_bytes, cudaMemcpyDeviceToDevice, st));
     k_huff_lengths<<<dim3(d.nblocks, 2), kMaxGroups * 32, 0, st>>>(d, kAll, 0, 1);
     BZ_LAUNCH_CHECK();
-    k_huff_estimate<<<d.nblocks, 32, 0, st>>>(d);
+    // second passes, side by side: every block over its tables (the plain
+    // blocks' second pass, the learned tables' exact pass) and, for learned
+    // blocks, the plain selector's second pass over its first-pass tables
+    BZ_CUDA(cudaMemsetAsync(d.rfreq, 0, rf_bytes, st));
+    BZ_CUDA(cudaMemsetAsync(d.rfreq2, 0, rf_bytes, st));
+    k_huff_select<<<dim3(d.n_group_tiles, 2), kGroupTile, 0, st>>>(d, kAll, 0);
     BZ_LAUNCH_CHECK();
-    select_pass(d, kAll, 0, st);
-    lengths_pass(d, kAll, 0, st);
+    k_huff_lengths<<<dim3(d.nblocks, 2), kMaxGroups * 32, 0, st>>>(d, kAll, 0, 2);
+    BZ_LAUNCH_CHECK();
     k_huff_judge<<<d.nblocks, 32, 0, st>>>(d);
     BZ_LAUNCH_CHECK();
-    for (int r = 0; r < kIters; r++) {
+    // plain blocks (fewer than six tables) finish their four passes
+    for (int r = 0; r < kIters - 2; r++) {
       select_pass(d, kPlainRound, r, st);
       lengths_pass(d, kPlainRound, r, st);
     }

@@ -280,9 +280,11 @@ int bz2g_assemble(int nparts, const uint8_t *const *d_parts, const int64_t *bits
  * group's symbol histogram predicts the table the reference's iterative
  * selector (src/compression/huffman.cu:188-243,304-323) would choose.  With
  * the learned selector on, a block with six tables takes: MLP assignment ->
- * code lengths -> one exact selection pass -> code lengths -> codes; blocks
- * with fewer tables keep the plain selector.  Streams stay valid bzip2; they
- * are no longer byte-identical to the reference's.
+ * code lengths -> one exact selection pass -> code lengths -> codes, unless
+ * the plain selector's first two passes (run beside it as the judge) predict
+ * a smaller block, in which case it takes those; blocks with fewer tables
+ * keep the plain selector.  Streams stay valid bzip2; they are no longer
+ * byte-identical to the reference's.
  *
  * Parameters: BZ2G_SELECTOR_PARAMS floats, one flat array, row-major with
  * zero padding: W1[256][272] b1[256] W2[256][256] b2[256] W3[16][256] b3[16]

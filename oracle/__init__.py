@@ -57,6 +57,7 @@ def lib():
         L.orc_rle2.argtypes = [_vp, _i, _i, _vp]
         L.orc_code_lengths.argtypes = [_vp, _vp, _i, _i]
         L.orc_huffman_build.argtypes = [_vp, _i, _i, _vp, _vp, _vp, ctypes.POINTER(_i)]
+        L.orc_huffman_build_passes.argtypes = [_vp, _i, _i, _i, _vp, _vp, _vp, ctypes.POINTER(_i)]
         L.orc_encode.restype = ctypes.c_int64
         L.orc_encode.argtypes = [_vp, _i, _vp, _vp, _vp, _vp]
         L.orc_selector_mtf.argtypes = [_vp, _i, _i, _vp]
@@ -172,15 +173,16 @@ def code_lengths(freq, alpha_size: int, max_len: int = 17) -> np.ndarray:
     return ln[:alpha_size].copy()
 
 
-def huffman_build(syms, n_in_use: int):
-    """(len[6,258], code[6,258], selectors, n_groups)"""
+def huffman_build(syms, n_in_use: int, passes: int = 4):
+    """(len[6,258], code[6,258], selectors, n_groups) of the plain selector
+    with `passes` selection passes (the reference's 4)."""
     s = np.ascontiguousarray(syms, dtype=np.uint16)
     ln = np.zeros((G, A), np.uint8)
     code = np.zeros((G, A), np.int32)
     sel = np.zeros(s.size // 50 + 2, np.uint8)
     ng = _i()
-    nsel = lib().orc_huffman_build(s.ctypes.data, s.size, n_in_use, ln.ctypes.data,
-                                   code.ctypes.data, sel.ctypes.data, ctypes.byref(ng))
+    nsel = lib().orc_huffman_build_passes(s.ctypes.data, s.size, n_in_use, passes, ln.ctypes.data,
+                                          code.ctypes.data, sel.ctypes.data, ctypes.byref(ng))
     return ln, code, sel[:nsel].copy(), ng.value
 
 

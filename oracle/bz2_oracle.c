@@ -348,11 +348,12 @@ static void canonical_codes(int ng, int alpha, uint8_t len[ORC_MAX_GROUPS][ORC_M
   }
 }
 
-/* src/compression/huffman.cu:256-364 with a zeroed histogram. */
-int orc_huffman_build(const uint16_t *syms, int s, int alphabet_size,
-                      uint8_t len[ORC_MAX_GROUPS][ORC_MAX_ALPHA],
-                      int32_t code[ORC_MAX_GROUPS][ORC_MAX_ALPHA],
-                      uint8_t *selectors, int *n_groups_out) {
+/* src/compression/huffman.cu:256-364 with a zeroed histogram, with
+ * `passes` selection passes (the reference's 4). */
+int orc_huffman_build_passes(const uint16_t *syms, int s, int alphabet_size, int passes,
+                             uint8_t len[ORC_MAX_GROUPS][ORC_MAX_ALPHA],
+                             int32_t code[ORC_MAX_GROUPS][ORC_MAX_ALPHA],
+                             uint8_t *selectors, int *n_groups_out) {
   int alpha = alphabet_size + 2;
   for (int g = 0; g < ORC_MAX_GROUPS; g++)
     for (int v = 0; v < alpha; v++) len[g][v] = 15;
@@ -362,13 +363,20 @@ int orc_huffman_build(const uint16_t *syms, int s, int alphabet_size,
   orc_initial_assignment(ng, s, alpha, freqs, len);
   int nsel = (s + 49) / 50;
   int32_t rfreq[ORC_MAX_GROUPS][ORC_MAX_ALPHA];
-  for (int iter = 0; iter < 4; iter++) {
+  for (int iter = 0; iter < passes; iter++) {
     select_pass(syms, s, ng, len, selectors, rfreq);
     for (int t = 0; t < ng; t++) orc_code_lengths(rfreq[t], len[t], alpha, 17);
   }
   canonical_codes(ng, alpha, len, code);
   *n_groups_out = ng;
   return nsel;
+}
+
+int orc_huffman_build(const uint16_t *syms, int s, int alphabet_size,
+                      uint8_t len[ORC_MAX_GROUPS][ORC_MAX_ALPHA],
+                      int32_t code[ORC_MAX_GROUPS][ORC_MAX_ALPHA],
+                      uint8_t *selectors, int *n_groups_out) {
+  return orc_huffman_build_passes(syms, s, alphabet_size, 4, len, code, selectors, n_groups_out);
 }
 
 /* The learned form's passes after its first assignment sel_in (six tables):
@@ -417,11 +425,12 @@ static int64_t predicted_bits(int ng, int alpha, int32_t rfreq[ORC_MAX_GROUPS][O
 
 /* The learned form for one block given the MLP's choices sel_mlp (written
  * from bzip2gpu_b200/csrc/huffman.cu's learned schedule): with six tables,
- * the single-pass estimate is the first plain pass over the initial tables;
  * the learned tables come from the MLP's choice, one exact selection pass and
- * code lengths; if their predicted size exceeds the estimate, the block is
- * coded with the plain selector (orc_huffman_build) and *fell_back = 1.
- * Blocks with fewer tables are plain.  Returns the selector count. */
+ * code lengths.  Beside them the plain selector runs its first two passes
+ * (initial tables, then one pass over the first pass's tables).  If the
+ * learned tables' predicted size exceeds the plain two-pass one, the block
+ * is coded with the plain two-pass selection and *fell_back = 1.  Blocks with
+ * fewer tables are plain (four passes).  Returns the selector count. */
 int orc_huffman_learned(const uint16_t *syms, int s, int alphabet_size, const uint8_t *sel_mlp,
                         uint8_t len[ORC_MAX_GROUPS][ORC_MAX_ALPHA],
                         int32_t code[ORC_MAX_GROUPS][ORC_MAX_ALPHA], uint8_t *selectors,
@@ -432,26 +441,29 @@ int orc_huffman_learned(const uint16_t *syms, int s, int alphabet_size, const ui
   if (ng != ORC_MAX_GROUPS)
     return orc_huffman_build(syms, s, alphabet_size, len, code, selectors, n_groups_out);
   static __thread int32_t rfreq[ORC_MAX_GROUPS][ORC_MAX_ALPHA];
-  static __thread uint8_t lsp[ORC_MAX_GROUPS][ORC_MAX_ALPHA];
-  uint8_t *tmp_sel = (uint8_t *)malloc((s + 49) / 50 + 1);
-  /* single-pass estimate */
-  for (int g = 0; g < ORC_MAX_GROUPS; g++)
-    for (int v = 0; v < alpha; v++) lsp[g][v] = 15;
-  int32_t freqs[ORC_MAX_ALPHA] = {0};
-  for (int i = 0; i < s; i++) freqs[syms[i]]++;
-  orc_initial_assignment(ng, s, alpha, freqs, lsp);
-  select_pass(syms, s, ng, lsp, tmp_sel, rfreq);
-  for (int t = 0; t < ng; t++) orc_code_lengths(rfreq[t], lsp[t], alpha, 17);
-  const int64_t est = predicted_bits(ng, alpha, rfreq, lsp);
-  free(tmp_sel);
+  static __thread uint8_t lp[ORC_MAX_GROUPS][ORC_MAX_ALPHA];
+  static __thread int32_t cp[ORC_MAX_GROUPS][ORC_MAX_ALPHA];
+  const int nsel = (s + 49) / 50;
+  uint8_t *sel_plain = (uint8_t *)malloc(nsel + 1);
+  /* the plain selector's first two passes, and the counts of its selection */
+  int ngp = 0;
+  orc_huffman_build_passes(syms, s, alphabet_size, 2, lp, cp, sel_plain, &ngp);
+  memset(rfreq, 0, sizeof(rfreq));
+  for (int g = 0; g < nsel; g++) {
+    const int gs = g * 50, ge = gs + 50 < s ? gs + 50 : s;
+    for (int i = gs; i < ge; i++) rfreq[sel_plain[g]][syms[i]]++;
+  }
+  const int64_t est = predicted_bits(ng, alpha, rfreq, lp);
   /* learned: MLP choice -> tables -> exact pass -> tables */
-  int nsel = orc_huffman_refine(syms, s, alphabet_size, sel_mlp, 0, len, code, selectors);
+  orc_huffman_refine(syms, s, alphabet_size, sel_mlp, 0, len, code, selectors);
   select_pass(syms, s, ng, len, selectors, rfreq);
   for (int t = 0; t < ng; t++) orc_code_lengths(rfreq[t], len[t], alpha, 17);
   if (predicted_bits(ng, alpha, rfreq, len) > est) {
     *fell_back = 1;
-    return orc_huffman_build(syms, s, alphabet_size, len, code, selectors, n_groups_out);
+    memcpy(selectors, sel_plain, nsel);
+    memcpy(len, lp, sizeof(lp));
   }
+  free(sel_plain);
   canonical_codes(ng, alpha, len, code);
   *n_groups_out = ng;
   return nsel;

@@ -86,6 +86,11 @@ void orc_code_lengths(const int32_t *freq, uint8_t *len, int alpha_size,
  * does).  selectors needs ceil(s/50) bytes.  Writes *n_groups.  Returns the
  * number of selectors.  Uses a zeroed symbol histogram.
  * src/compression/huffman.cu:126-364 */
+/* The plain selector with `passes` selection passes (the reference's 4). */
+int orc_huffman_build_passes(const uint16_t *syms, int s, int alphabet_size, int passes,
+                             uint8_t len[ORC_MAX_GROUPS][ORC_MAX_ALPHA],
+                             int32_t code[ORC_MAX_GROUPS][ORC_MAX_ALPHA],
+                             uint8_t *selectors, int *n_groups_out);
 int orc_huffman_build(const uint16_t *syms, int s, int alphabet_size,
                       uint8_t len[ORC_MAX_GROUPS][ORC_MAX_ALPHA],
                       int32_t code[ORC_MAX_GROUPS][ORC_MAX_ALPHA],

@@ -158,8 +158,8 @@ def test_learned_build_matches_oracle_given_mlp_choices(torch_cuda, seed, n):
 
 def test_learned_build_judge_both_ways(torch_cuda):
     # the shipped parameters keep the learned tables on these blocks, untrained
-    # ones lose to the single-pass estimate and fall back to the plain
-    # selector; every block equals the oracle either way
+    # ones lose to the plain selector's first two passes and fall back to
+    # them; every block equals the oracle either way
     outcomes = set()
     for P in (S.load(), _params(99)):
         d_P = torch_cuda.from_numpy(P).cuda()

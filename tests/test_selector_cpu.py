@@ -110,8 +110,8 @@ def test_selector_specs_reach_block_count():
 def test_learned_oracle_judge():
     # the MLP's choice replaced by the plain selector's own final choice:
     # one exact pass keeps (or improves) it, so no fallback; a constant
-    # choice (one table for every group) is worse than one plain pass, so the
-    # block falls back and equals the plain selector's coding
+    # choice (one table for every group) is worse than the plain selector's
+    # first two passes, so the block falls back to exactly that selection
     _, st, info = _groups(9, 600000)
     syms = st["rle2"]
     ln, code, sel, ng, fb = oracle.huffman_learned(syms, info.n_in_use, st["sel"])
@@ -121,9 +121,14 @@ def test_learned_oracle_judge():
     ln, code, sel, ng, fb = oracle.huffman_learned(syms, info.n_in_use,
                                                    np.zeros_like(st["sel"]))
     assert fb
-    assert np.array_equal(sel, st["sel"])
+    pl, pc, ps, png = oracle.huffman_build(syms, info.n_in_use, passes=2)
+    assert np.array_equal(sel, ps)
     a = info.n_in_use + 2
-    assert np.array_equal(ln[:, :a], st["len"][:, :a])
+    assert np.array_equal(ln[:, :a], pl[:, :a])
+    assert np.array_equal(code[:, :a], pc[:, :a])
+    # four passes are the reference's selector
+    fl, fc, fs, fng = oracle.huffman_build(syms, info.n_in_use)
+    assert np.array_equal(fs, st["sel"]) and np.array_equal(fl[:, :a], st["len"][:, :a])
     # fewer than six tables: plain
     _, st2, info2 = _groups(10, 1500)
     assert info2.n_groups < 6
