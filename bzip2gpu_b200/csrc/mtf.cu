@@ -74,18 +74,15 @@ __global__ void __launch_bounds__(256) k_mtf_block_scan(SlabDev d) {
 // sequential move-to-front over its own symbols with its own list.
 constexpr int kSub = kTile / 32;      // symbols per lane
 constexpr int kListStride = 264;      // bytes per lane list (8-aligned, bank spread)
-constexpr int kPartStride = kSub + 4;
 // The tile in shared memory: lane l's kSub bytes at l * (kSub + 4), so the 32
 // lanes walking their own slices hit 32 different banks.
 constexpr int kSLaneStride = kSub + 4;
 __device__ __forceinline__ int sl_at(int i) { return i + (i / kSub) * 4; }
 
 __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d) {
-  // The start keys are read before the partial lists are written, so they
-  // share storage (17.6 KB in all: 12 single-warp blocks per SM).
-  __shared__ __align__(16) uint8_t part_key[32 * kPartStride];
-  int *key = reinterpret_cast<int *>(part_key);  // [256]
-  uint8_t *part = part_key;
+  // Lane k's list at lists[k]; lane k - 1 writes its partial list straight to
+  // the front of list k, where the chain below wants it (13.5 KB of shared
+  // memory in all: 15 single-warp blocks per SM).
   __shared__ __align__(16) uint8_t sL[32 * kSLaneStride];
   __shared__ __align__(16) uint8_t lists[32 * kListStride];
   __shared__ uint32_t pmask[32][9];  // padded row: no bank conflicts across lanes
@@ -104,12 +101,6 @@ __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d) {
     pw[w] = d.present[b * 8 + w];
     nuse += __popc(pw[w]);
   }
-  // key: last position before this tile, or (-1 - c) for unseen symbols
-  for (int c = ln; c < 256; c += 32) {
-    int lp = d.tile_last[(size_t)t * 256 + c];
-    bool use = (pw[c >> 5] >> (c & 31)) & 1u;
-    key[c] = !use ? INT32_MIN : (lp >= 0 ? lp : -1 - c);
-  }
   const uint4 *src = reinterpret_cast<const uint4 *>(d.last + off + lt);
   for (int w = ln; w < (valid + 15) / 16; w += 32) {
     const uint4 v = src[w];
@@ -121,22 +112,26 @@ __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d) {
   }
 #pragma unroll
   for (int w = 0; w < 8; w++) pmask[ln][w] = 0;
-  __syncwarp();
   {
-    // Lane 0's list: the in-use symbols by key, largest first.  A bitonic
-    // sort of the 256 keys across the warp (symbol 8k+q in register q of lane
-    // k; partners 8 or more apart sit in other lanes and come by shuffle),
-    // each key packed with its symbol as (key + 257) << 8 | symbol, 0 for
-    // symbols not in use.  Keys are distinct and above -258, so the packing
-    // keeps their order.
+    // Lane 0's list: the in-use symbols by key, largest first, where a
+    // symbol's key is its last position before this tile, or -1 - c for a
+    // symbol not seen yet.  A bitonic sort of the 256 keys across the warp
+    // (symbol 8k+q in register q of lane k; partners 8 or more apart sit in
+    // other lanes and come by shuffle), each key packed with its symbol as
+    // (key + 257) << 8 | symbol, 0 for symbols not in use.  Keys are distinct
+    // and above -258, so the packing keeps their order.
     uint32_t v[8];
     {
-      const int4 *k4 = reinterpret_cast<const int4 *>(key) + 2 * ln;
+      const int4 *k4 = reinterpret_cast<const int4 *>(d.tile_last + (size_t)t * 256) + 2 * ln;
       const int4 lo = k4[0], hi = k4[1];
-      const int kk[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+      const int lp[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+      const uint32_t use = (pw[ln >> 2] >> (8 * (ln & 3))) & 0xffu;  // symbols 8 ln .. 8 ln + 7
 #pragma unroll
-      for (int q = 0; q < 8; q++)
-        v[q] = kk[q] == INT32_MIN ? 0u : ((uint32_t)(kk[q] + 257) << 8) | (uint32_t)(8 * ln + q);
+      for (int q = 0; q < 8; q++) {
+        const int c = 8 * ln + q;
+        const int key = lp[q] >= 0 ? lp[q] : -1 - c;
+        v[q] = ((use >> q) & 1u) ? ((uint32_t)(key + 257) << 8) | (uint32_t)c : 0u;
+      }
     }
 #pragma unroll
     for (int k = 2; k <= 256; k <<= 1) {
@@ -174,10 +169,10 @@ __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d) {
   const int a0 = ln * kSub;
   const int a1 = min(valid, a0 + kSub);
   uint8_t *mySL = sL + 4 * ln;  // this lane's slice: mySL[i] for i in [a0, a1)
-  __syncwarp();  // every lane has read the start keys
+  __syncwarp();  // sL and pmask are in place
   int cnt = 0;  // this lane's partial-list length
-  {
-    uint8_t *pp = part + ln * kPartStride;
+  if (ln < 31) {  // lane 31's partial list starts no list
+    uint8_t *pp = lists + (ln + 1) * kListStride;
     for (int i = a1 - 1; i >= a0; i--) {
       const int c = mySL[i];
       const uint32_t bit = 1u << (c & 31);
@@ -189,13 +184,12 @@ __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d) {
     }
   }
   __syncwarp();
-  // lane lists, in turn: list k = partial(k-1) ++ (list k-1 minus partial(k-1))
+  // lane lists, in turn: list k = partial(k-1) ++ (list k-1 minus
+  // partial(k-1)); partial(k-1) is already at the front of list k
   for (int k = 1; k < 32; k++) {
     const uint8_t *prevl = lists + (k - 1) * kListStride;
     uint8_t *cur = lists + k * kListStride;
     const int pc = __shfl_sync(0xffffffffu, cnt, k - 1);
-    const uint8_t *pp = part + (k - 1) * kPartStride;
-    for (int q = ln; q < pc; q += 32) cur[q] = pp[q];
     uint8_t keepv[8];
     int nk = 0;
 #pragma unroll
