@@ -106,9 +106,18 @@ __global__ void __launch_bounds__(256) k_radix_hist(SlabDev d, int shift, const 
   const uint64_t *K = d.keys[d.sort_ctl[0]] + d.off[b] + lt;
   const uint8_t *T = d.rle1 + d.off[b];
   const int m = d.m[b];
-  for (int e = threadIdx.x; e < valid; e += blockDim.x) {
-    const uint64_t it = gen ? text_item(T, m, lt + e) : K[e];
-    atomicAdd(&cnt[(uint32_t)(it >> shift) & (kRadix - 1)], 1u);
+  if (gen) {
+    // digit bits [shift, shift + 8) of the item are byte 3 - (shift - 32) / 8
+    // of the rotation's 4-byte prefix
+    const int q = 3 - (shift - 32) / 8;
+    for (int e = threadIdx.x; e < valid; e += blockDim.x) {
+      int j = lt + e + q;
+      while (j >= m) j -= m;
+      atomicAdd(&cnt[T[j]], 1u);
+    }
+  } else {
+    for (int e = threadIdx.x; e < valid; e += blockDim.x)
+      atomicAdd(&cnt[(uint32_t)(K[e] >> shift) & (kRadix - 1)], 1u);
   }
   __syncthreads();
   d.tile_hist[(size_t)t * kRadix + threadIdx.x] = cnt[threadIdx.x];
