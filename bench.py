@@ -183,28 +183,26 @@ def run_reference(args):
     print(json.dumps(line))
 
 
-def run_batch(args):
+def many_inputs(B, W, torch, rank: int, world: int, count: int, plain_steps: int,
+                batched_steps: int, warmup: int) -> dict:
     """Batched form vs plain form on the many-inputs workload: inputs of
     log-uniform size 1 KiB .. 8 MiB, alphabet 2..256, alpha 0.05 .. 5, level
     1..9 (blocks of level * 100,000 bytes), 1 % runs; inputs resident in HBM,
-    streams delivered to page-locked host memory."""
-    world, rank, local = dist_setup(args.gpus)
-    import torch
-
-    import bzip2gpu_b200 as B
-    import bzip2gpu_b200.workloads as W
-
-    items = W.batch_inputs(count=args.batch_count, seed=0xB2C2 + 7919 * rank)
+    streams delivered to page-locked host memory.  "plain" compresses the
+    inputs one call each; "batched" runs all their blocks through shared slabs
+    in one call (slab shapes from the committed tuning table).  The batched
+    streams are checked to be the per-input streams, byte for byte."""
+    items = W.batch_inputs(count=count, seed=0xB2C2 + 7919 * rank)
     sizes = [x.data.size for x in items]
     levels = [x.level for x in items]
     total = sum(sizes)
     flat = torch.from_numpy(np.concatenate([x.data for x in items])).cuda()
+    del items
     offs = np.concatenate([[0], np.cumsum(sizes)])
-    d_in = [flat[offs[i]:offs[i + 1]] for i in range(len(items))]
-    cap = B.lib().bz2g_compress_batch_bound(len(items), (ctypes.c_size_t * len(items))(*sizes),
-                                           (ctypes.c_int * len(items))(*levels), None)
+    d_in = [flat[offs[i]:offs[i + 1]] for i in range(len(sizes))]
+    cap = B.lib().bz2g_compress_batch_bound(len(sizes), (ctypes.c_size_t * len(sizes))(*sizes),
+                                           (ctypes.c_int * len(sizes))(*levels), None)
     h_out = torch.empty(cap, dtype=torch.uint8, pin_memory=True)
-    B.set_timing(False)
 
     def plain():
         n = 0
@@ -216,34 +214,50 @@ def run_batch(args):
         st = B.compress_batch(d_in, levels, out=h_out, on_device=True)
         return sum(len(v) for v in st)
 
-    ref = [bytes(s) for s in B.compress_batch(d_in, levels, on_device=True)]
-    for _ in range(args.warmup):
+    ref = [bytes(v) for v in B.compress_batch(d_in, levels, on_device=True)]
+    for _ in range(warmup):
         plain()
         batched()
     res = {}
-    for name, fn in (("plain", plain), ("batched", batched)):
+    for name, fn, steps in (("plain", plain, plain_steps), ("batched", batched, batched_steps)):
         barrier(world)
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(args.steps):
+        for _ in range(steps):
             nbytes = fn()
         e1.record()
         torch.cuda.synchronize()
         dt = max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
-        res[name] = {"MB/s": round(total * world * args.steps / dt / 1e6, 2),
-                     "ms_per_step": round(dt / args.steps * 1e3, 2), "stream_bytes": int(nbytes)}
+        res[name] = {"MB/s": round(total * world * steps / dt / 1e6, 2), "timed_passes": steps,
+                     "ms_per_pass": round(dt / steps * 1e3, 2), "stream_bytes": int(nbytes)}
     # the batched streams are the per-input streams
+    exact = True
     for i, (x, lv) in enumerate(zip(d_in, levels)):
         k = B.compress_device_into(x, h_out, lv, lv * 100000)
-        assert bytes(h_out[:k].numpy()) == ref[i]
+        exact = exact and bytes(h_out[:k].numpy()) == ref[i]
+    del d_in, flat, h_out
+    torch.cuda.empty_cache()
+    return {"workload": "many inputs (1 KiB..8 MiB; levels 1..9)", "inputs": len(sizes),
+            "bytes": int(total), "forms": res,
+            "batched_over_plain": round(res["batched"]["MB/s"] / res["plain"]["MB/s"], 3),
+            "bit_exact": bool(exact)}
+
+
+def run_batch(args):
+    """The many-inputs workload alone (see many_inputs)."""
+    world, rank, local = dist_setup(args.gpus)
+    import torch
+
+    import bzip2gpu_b200 as B
+    import bzip2gpu_b200.workloads as W
+    B.set_timing(False)
+    res = many_inputs(B, W, torch, rank, world, args.batch_count, args.steps, args.steps,
+                      args.warmup)
     if rank == 0:
-        print(json.dumps({"workload": "many inputs (1 KiB..8 MiB; levels 1..9)",
-                          "inputs": len(items), "bytes": int(total), "n_gpus": world,
-                          "steps": args.steps, "warmup": args.warmup, "forms": res,
-                          "batched_over_plain": round(res["batched"]["MB/s"] / res["plain"]["MB/s"], 3),
-                          "bit_exact": True}))
+        res.update({"n_gpus": world, "steps": args.steps, "warmup": args.warmup})
+        print(json.dumps(res))
 
 
 def run_stress(args):
@@ -310,6 +324,8 @@ def main():
     ap.add_argument("--size", type=int, default=10 << 30)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the many-inputs (batched form) measurement")
     ap.add_argument("--no-check", action="store_true",
                     help="skip the whole-stream parity and round-trip checks")
     ap.add_argument("--slab", type=int, default=0)
@@ -404,6 +420,13 @@ def main():
                   "ratio": round(zlen / n, 5), "size_vs_plain": round(zlen / len(out), 6)}
     dt = max_over_ranks(dt, world)
     value = n * world * args.steps / dt / 1e6
+
+    # the many-inputs workload: per-input plain calls vs the batched form
+    batch_many = None
+    if not args.no_batch:
+        B.set_timing(False)
+        batch_many = many_inputs(B, W, torch, rank, world, args.batch_count, 1, 3, 1)
+        B.set_timing(True)
 
     e2e = None
     decode = None
@@ -532,7 +555,8 @@ def main():
                        "blocks": int(stats["blocks"]), "ratio": round(ratio, 4)},
             "e2e": e2e, "roofline": roof, "pipeline_roofline": pipeline, "cpu_baseline": cpu,
             "forms": {"plain": round(value, 2), "batched": round(batched_value, 2),
-                      "learned": learned, "bzip2_format": bzip2_form},
+                      "learned": learned, "bzip2_format": bzip2_form,
+                      "batched_many_inputs": batch_many},
             "decode": decode, "checks": checks,
             "clocks": clk.summary(), "gpu_launches": int(launches),
             "stats": {k: stats[k] for k in ("n", "m", "A", "s", "g", "bits")},
