@@ -663,11 +663,17 @@ void stage_bwt(const SlabDev &d, int max_m, cudaStream_t st) {
     d.rt_act[0] = 0;
     BZ_CUDA(cudaEventRecord(d.rt_ev[0], st));
   }
+  // the tiles holding rotations (a block's workspace has room for its
+  // worst-case RLE1 output, so most of its tiles are usually empty)
+  const int nlive = live_tiles(d, st);
+  if (nlive == 0) return;
+  const int grid0 = nlive > 0 ? nlive : d.ntiles;
+  const int32_t *list0 = nlive > 0 ? d.vt_list : nullptr;
   // first sort: 4-byte prefixes in the high half of packed items, or 8-byte keys
   const Layout first = {packed, packed ? 32 : 0};
   const Layout round = {packed, packed ? kb : 0};
   if (packed) {
-    radix_sort(d, 32, 64, 0, st, d.ntiles, nullptr, true);
+    radix_sort(d, 32, 64, 0, st, grid0, list0, true);
   } else {
     k_bwt_keys0<<<d.ntiles, 256, 0, st>>>(d, packed);
     BZ_LAUNCH_CHECK();
@@ -675,8 +681,8 @@ void stage_bwt(const SlabDev &d, int max_m, cudaStream_t st) {
   }
   const int nq = packed ? 3 : 4;  // prefixes 1,2,4 (,8) bytes
   int64_t prefix = packed ? 4 : 8;
-  int grid = d.ntiles;
-  const int32_t *list = nullptr;
+  int grid = grid0;
+  const int32_t *list = list0;
   int r = 0;  // round being run (0: the first sort)
   for (int initial = 1;; initial = 0) {
     const Layout L = initial ? first : round;

@@ -121,6 +121,8 @@ Workspace::Workspace(int mb, int64_t mr, int64_t me, int mt, int mrt, int mgt)
     dev.tile_c = (int32_t *)alloc(T * 4);
     dev.tile_d = (int32_t *)alloc(T * 4);
     dev.tile_list = (int32_t *)alloc(T * 4);
+    dev.vt_list = (int32_t *)alloc(T * 4);
+    dev.vg_list = (int32_t *)alloc(((int64_t)mgt + 1) * 4);
     dev.warp_last = (int32_t *)alloc(((int64_t)mt + 1) * (kTileThreads / 32) * 4);
     dev.warp_act = (int32_t *)alloc(((int64_t)mt + 1) * (kTileThreads / 32) * 4);
     dev.tile_hist = (uint32_t *)alloc((int64_t)mt * 256 * 4);
@@ -165,11 +167,14 @@ Workspace::Workspace(int mb, int64_t mr, int64_t me, int mt, int mrt, int mgt)
     plan_dev_ = alloc(pinned_plan_bytes);
     BZ_CUDA(cudaMallocHost(&pinned_plan, pinned_plan_bytes));
     BZ_CUDA(cudaMallocHost((void **)&dev.h_flags, 64));
+    BZ_CUDA(cudaMallocHost((void **)&dev.live, 4 * sizeof(int)));
+    dev.live[0] = dev.live[1] = -1;
   } catch (...) {
     for (void *p : allocs_) cudaFree(p);
     allocs_.clear();
     if (pinned_plan) cudaFreeHost(pinned_plan);
     if (dev.h_flags) cudaFreeHost(dev.h_flags);
+    if (dev.live) cudaFreeHost(dev.live);
     throw;
   }
 }
@@ -178,9 +183,11 @@ Workspace::~Workspace() {
   for (void *p : allocs_) cudaFree(p);
   if (pinned_plan) cudaFreeHost(pinned_plan);
   if (dev.h_flags) cudaFreeHost(dev.h_flags);
+  if (dev.live) cudaFreeHost(dev.live);
 }
 
 void Workspace::upload_plan(const SlabPlan &p, cudaStream_t st) {
+  dev.live[0] = dev.live[1] = -1;  // a new slab: its tile lists are built anew
   BZ_REQUIRE(p.nblocks <= max_blocks && p.raw_total <= max_raw && p.elem_total <= max_elems &&
                  (int)p.tile_block.size() <= max_tiles && (int)p.rt_block.size() <= max_raw_tiles &&
                  (int)p.gt_block.size() <= max_group_tiles,
@@ -225,5 +232,55 @@ Workspace *Workspace::create_for(int max_blocks, int64_t max_block_bytes, int bl
   const int mgt = (int)(max_blocks * ((groups_bound(nb) + kGroupTile - 1) / kGroupTile));
   return new Workspace(std::max(max_blocks, block_slots), R, E, mt, mrt, mgt);
 }
+
+namespace {
+
+// One block of threads lists, in block order, the tiles that hold data:
+// element tiles (groups = 0) of the m[b] bytes from off[b], or group tiles
+// (groups = 1) of the ceil(s[b] / 50) groups from gt_begin[b].  The count
+// goes to sort_ctl[10 + groups].
+__global__ void __launch_bounds__(256) k_live_tiles(SlabDev d, int groups) {
+  __shared__ int scratch[40];
+  int32_t *list = groups ? d.vg_list : d.vt_list;
+  int base = 0;
+  for (int b0 = 0; b0 < d.nblocks; b0 += 256) {
+    const int b = b0 + threadIdx.x;
+    int cnt = 0, first = 0;
+    if (b < d.nblocks) {
+      if (groups) {
+        const int s = d.s[b];
+        const int nsel = s > 0 ? (s + kGroupSize - 1) / kGroupSize : 0;
+        cnt = (nsel + kGroupTile - 1) / kGroupTile;
+        first = d.gt_begin[b];
+      } else {
+        const int m = d.m[b];
+        cnt = m > 0 ? (m + kTile - 1) / kTile : 0;
+        first = (int)(d.off[b] / kTile);
+      }
+    }
+    int tot;
+    const int at = base + block_excl_sum(cnt, scratch, &tot);
+    for (int k = 0; k < cnt; k++) list[at + k] = first + k;
+    base += tot;
+  }
+  if (threadIdx.x == 0) d.sort_ctl[10 + groups] = base;
+}
+
+int live_list(const SlabDev &d, cudaStream_t st, int groups) {
+  if (!d.live) return -1;
+  if (d.live[groups] >= 0) return d.live[groups];
+  k_live_tiles<<<1, 256, 0, st>>>(d, groups);
+  BZ_LAUNCH_CHECK();
+  BZ_CUDA(cudaMemcpyAsync(d.live + 2, d.sort_ctl + 10 + groups, sizeof(int32_t),
+                          cudaMemcpyDeviceToHost, st));
+  BZ_CUDA(cudaStreamSynchronize(st));
+  d.live[groups] = d.live[2];
+  return d.live[groups];
+}
+
+}  // namespace
+
+int live_tiles(const SlabDev &d, cudaStream_t st) { return live_list(d, st, 0); }
+int live_group_tiles(const SlabDev &d, cudaStream_t st) { return live_list(d, st, 1); }
 
 }  // namespace bz2g

@@ -91,6 +91,13 @@ struct SlabDev {
   int32_t *sort_len, *done, *ngroups;  // BWT control (ngroups: groups among active rotations)
   int32_t *act_len;                    // BWT: active rotations entering the next round
   int32_t *tile_list;                  // BWT: tiles holding active rotations [ntiles]
+  // The tiles that hold data, listed in block order (a block's workspace is
+  // sized for its worst-case RLE1 output, so most of its tiles can be empty):
+  // element tiles of the m[b] RLE1 bytes, and group tiles of the
+  // ceil(s[b] / 50) groups.  live (pinned host) [0], [1]: their counts once
+  // known for this slab, -1 before (kernels then run over every tile).
+  int32_t *vt_list, *vg_list;
+  int *live;
   int32_t *warp_last, *warp_act;       // BWT: per 512-element warp span [ntiles * 8]: last
                                        // head, then its carry; active count, then offset
   int64_t *active_sum;                 // A: rotations in non-singleton groups, summed over rounds
@@ -157,6 +164,13 @@ class Workspace {
   void *plan_dev_ = nullptr;
   void *alloc(size_t bytes);
 };
+
+// The listed tiles of the slab (built on the first call after m, or s, is
+// final; the count is read back, one synchronisation of `st`): the element
+// tiles holding RLE1 bytes, and the group tiles holding 50-symbol groups.
+// Return -1 when the slab has no list (launch over every tile then).
+int live_tiles(const SlabDev &d, cudaStream_t st);
+int live_group_tiles(const SlabDev &d, cudaStream_t st);
 
 // ------------------------------------------------------------------ stages
 void stage_rle1_crc(const SlabDev &d, cudaStream_t st);

@@ -86,11 +86,13 @@ __global__ void k_huff_init(SlabDev d, int learned_mode) {
 // grid.y == 2 (the learned form's second passes): y = 1 runs, for the
 // learned blocks, the plain selector's second pass over its first-pass
 // tables (len2) into sel2 / rfreq2, beside y = 0's pass over len.
-__global__ void __launch_bounds__(kGroupTile) k_huff_select(SlabDev d, int which, int round) {
+// list: the group tiles to run (blockIdx.x-th entry), or nullptr for all.
+__global__ void __launch_bounds__(kGroupTile) k_huff_select(SlabDev d, int which, int round,
+                                                            const int32_t *list) {
   __shared__ uint16_t sy[kGroupTile * kGroupSize];
   __shared__ uint64_t plen[kMaxAlpha];
   __shared__ int rf[kMaxGroups * kMaxAlpha];
-  const int gt = blockIdx.x;
+  const int gt = list ? list[blockIdx.x] : (int)blockIdx.x;
   const int b = d.gt_block[gt];
   const int g0 = d.gt_first[gt];
   const int nsel = d.n_sel[b];
@@ -359,7 +361,10 @@ __global__ void __launch_bounds__(kMaxGroups * 32) k_huff_codes(SlabDev d) {
 namespace {
 void select_pass(const SlabDev &d, int which, int round, cudaStream_t st) {
   BZ_CUDA(cudaMemsetAsync(d.rfreq, 0, sizeof(int32_t) * kMaxGroups * kMaxAlpha * d.nblocks, st));
-  k_huff_select<<<d.n_group_tiles, kGroupTile, 0, st>>>(d, which, round);
+  const int nlive = live_group_tiles(d, st);
+  const int grid = nlive >= 0 ? nlive : d.n_group_tiles;
+  if (grid <= 0) return;
+  k_huff_select<<<grid, kGroupTile, 0, st>>>(d, which, round, nlive >= 0 ? d.vg_list : nullptr);
   BZ_LAUNCH_CHECK();
 }
 void lengths_pass(const SlabDev &d, int which, int round, cudaStream_t st) {
@@ -402,8 +407,15 @@ void stage_huffman(const SlabDev &d, cudaStream_t st, const uint8_t *learned, in
     // blocks, the plain selector's second pass over its first-pass tables
     BZ_CUDA(cudaMemsetAsync(d.rfreq, 0, rf_bytes, st));
     BZ_CUDA(cudaMemsetAsync(d.rfreq2, 0, rf_bytes, st));
-    k_huff_select<<<dim3(d.n_group_tiles, 2), kGroupTile, 0, st>>>(d, kAll, 0);
-    BZ_LAUNCH_CHECK();
+    {
+      const int nlive = live_group_tiles(d, st);
+      const int grid = nlive >= 0 ? nlive : d.n_group_tiles;
+      if (grid > 0) {
+        k_huff_select<<<dim3(grid, 2), kGroupTile, 0, st>>>(d, kAll, 0,
+                                                          nlive >= 0 ? d.vg_list : nullptr);
+        BZ_LAUNCH_CHECK();
+      }
+    }
     k_huff_lengths<<<dim3(d.nblocks, 2), kMaxGroups * 32, 0, st>>>(d, kAll, 0, 2);
     BZ_LAUNCH_CHECK();
     k_huff_judge<<<d.nblocks, 32, 0, st>>>(d);

@@ -15,10 +15,11 @@ namespace bz2g {
 
 namespace {
 
-__global__ void __launch_bounds__(256) k_mtf_last(SlabDev d) {
+// list: the tiles to run (blockIdx.x-th entry), or nullptr for every tile.
+__global__ void __launch_bounds__(256) k_mtf_last(SlabDev d, const int32_t *list) {
   __shared__ int lastpos[256];
   __shared__ uint32_t pres[8];
-  const int t = blockIdx.x;
+  const int t = list ? list[blockIdx.x] : (int)blockIdx.x;
   const int b = d.tile_block[t];
   const int64_t off = d.off[b];
   const int lt = (int)((int64_t)t * kTile - off);
@@ -79,14 +80,14 @@ constexpr int kListStride = 264;      // bytes per lane list (8-aligned, bank sp
 constexpr int kSLaneStride = kSub + 4;
 __device__ __forceinline__ int sl_at(int i) { return i + (i / kSub) * 4; }
 
-__global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d) {
+__global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d, const int32_t *list) {
   // Lane k's list at lists[k]; lane k - 1 writes its partial list straight to
   // the front of list k, where the chain below wants it (13.5 KB of shared
   // memory in all: 15 single-warp blocks per SM).
   __shared__ __align__(16) uint8_t sL[32 * kSLaneStride];
   __shared__ __align__(16) uint8_t lists[32 * kListStride];
   __shared__ uint32_t pmask[32][9];  // padded row: no bank conflicts across lanes
-  const int t = blockIdx.x;
+  const int t = list ? list[blockIdx.x] : (int)blockIdx.x;
   const int b = d.tile_block[t];
   const int64_t off = d.off[b];
   const int lt = (int)((int64_t)t * kTile - off);
@@ -260,12 +261,19 @@ __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d) {
 
 void stage_mtf(const SlabDev &d, cudaStream_t st) {
   BZ_CUDA(cudaMemsetAsync(d.present, 0, sizeof(uint32_t) * 8 * d.nblocks, st));
-  k_mtf_last<<<d.ntiles, 256, 0, st>>>(d);
-  BZ_LAUNCH_CHECK();
+  const int nlive = live_tiles(d, st);
+  const int grid = nlive >= 0 ? nlive : d.ntiles;
+  const int32_t *list = nlive >= 0 ? d.vt_list : nullptr;
+  if (grid > 0) {
+    k_mtf_last<<<grid, 256, 0, st>>>(d, list);
+    BZ_LAUNCH_CHECK();
+  }
   k_mtf_block_scan<<<d.nblocks, 256, 0, st>>>(d);
   BZ_LAUNCH_CHECK();
-  k_mtf_apply<<<d.ntiles, 32, 0, st>>>(d);
-  BZ_LAUNCH_CHECK();
+  if (grid > 0) {
+    k_mtf_apply<<<grid, 32, 0, st>>>(d, list);
+    BZ_LAUNCH_CHECK();
+  }
 }
 
 }  // namespace bz2g

@@ -148,9 +148,9 @@ __global__ void __launch_bounds__(kHdrThreads) k_sel_mtf_hdr(SlabDev d) {
 }
 
 // Payload bits per 50-symbol group; exclusive offsets within the group tile.
-__global__ void __launch_bounds__(kGroupTile) k_pay_bits(SlabDev d) {
+__global__ void __launch_bounds__(kGroupTile) k_pay_bits(SlabDev d, const int32_t *list) {
   __shared__ uint32_t scratch[8];
-  const int gt = blockIdx.x;
+  const int gt = list ? list[blockIdx.x] : (int)blockIdx.x;
   const int b = d.gt_block[gt];
   const int g0 = d.gt_first[gt];
   const int nsel = d.n_sel[b];
@@ -178,7 +178,10 @@ __global__ void __launch_bounds__(kGroupTile) k_pay_bits(SlabDev d) {
 __global__ void __launch_bounds__(256) k_pay_block(SlabDev d) {
   __shared__ uint32_t scratch[40];
   const int b = blockIdx.x;
-  const int t0 = d.gt_begin[b], nt = d.gt_begin[b + 1] - t0;
+  // the group tiles that hold groups (the others are not run)
+  const int nsel = d.n_sel[b];
+  const int t0 = d.gt_begin[b];
+  const int nt = min(d.gt_begin[b + 1] - t0, (nsel + kGroupTile - 1) / kGroupTile);
   int64_t carry = 0;
   for (int base = 0; base < nt; base += 256) {
     int k = base + threadIdx.x;
@@ -285,8 +288,8 @@ __global__ void __launch_bounds__(kHdrThreads) k_write_header(SlabDev d, int64_t
 }
 
 // Payload: one thread per 50-symbol group.
-__global__ void __launch_bounds__(kGroupTile) k_write_payload(SlabDev d, int64_t w0) {
-  const int gt = blockIdx.x;
+__global__ void __launch_bounds__(kGroupTile) k_write_payload(SlabDev d, int64_t w0, const int32_t *list) {
+  const int gt = list ? list[blockIdx.x] : (int)blockIdx.x;
   const int b = d.gt_block[gt];
   const int g0 = d.gt_first[gt];
   const int nsel = d.n_sel[b];
@@ -310,8 +313,8 @@ __global__ void __launch_bounds__(kGroupTile) k_write_payload(SlabDev d, int64_t
 
 // Payload only, in the reference's word layout (word w = stream bits
 // [32w, 32w+32), first bit in the MSB, host byte order), for one block.
-__global__ void __launch_bounds__(kGroupTile) k_pack_words(SlabDev d, uint32_t *words) {
-  const int gt = blockIdx.x;
+__global__ void __launch_bounds__(kGroupTile) k_pack_words(SlabDev d, uint32_t *words, const int32_t *list) {
+  const int gt = list ? list[blockIdx.x] : (int)blockIdx.x;
   const int b = d.gt_block[gt];
   const int g0 = d.gt_first[gt];
   const int nsel = d.n_sel[b];
@@ -343,17 +346,31 @@ __global__ void __launch_bounds__(kGroupTile) k_pack_words(SlabDev d, uint32_t *
 
 }  // namespace
 
+// A group-tile kernel over the tiles that hold groups (every tile when the
+// slab has no list).
+template <typename F>
+void launch_groups(const SlabDev &d, cudaStream_t st, F &&launch) {
+  const int nlive = live_group_tiles(d, st);
+  const int grid = nlive >= 0 ? nlive : d.n_group_tiles;
+  if (grid <= 0) return;
+  launch(grid, nlive >= 0 ? d.vg_list : nullptr);
+}
+
 void stage_sizes(const SlabDev &d, cudaStream_t st) {
   k_sel_mtf_hdr<<<d.nblocks, kHdrThreads, 0, st>>>(d);
   BZ_LAUNCH_CHECK();
-  k_pay_bits<<<d.n_group_tiles, kGroupTile, 0, st>>>(d);
+  launch_groups(d, st, [&](int grid, const int32_t *list) {
+    k_pay_bits<<<grid, kGroupTile, 0, st>>>(d, list);
+  });
   BZ_LAUNCH_CHECK();
   k_pay_block<<<d.nblocks, 256, 0, st>>>(d);
   BZ_LAUNCH_CHECK();
 }
 
 void stage_sizes_payload_only(const SlabDev &d, cudaStream_t st) {
-  k_pay_bits<<<d.n_group_tiles, kGroupTile, 0, st>>>(d);
+  launch_groups(d, st, [&](int grid, const int32_t *list) {
+    k_pay_bits<<<grid, kGroupTile, 0, st>>>(d, list);
+  });
   BZ_LAUNCH_CHECK();
   k_pay_block<<<d.nblocks, 256, 0, st>>>(d);
   BZ_LAUNCH_CHECK();
@@ -366,7 +383,9 @@ void stage_place(const SlabDev &d, int64_t slab_start_bit, int64_t w0, int64_t n
   BZ_LAUNCH_CHECK();
   k_write_header<<<d.nblocks, kHdrThreads, 0, st>>>(d, w0);
   BZ_LAUNCH_CHECK();
-  k_write_payload<<<d.n_group_tiles, kGroupTile, 0, st>>>(d, w0);
+  launch_groups(d, st, [&](int grid, const int32_t *list) {
+    k_write_payload<<<grid, kGroupTile, 0, st>>>(d, w0, list);
+  });
   BZ_LAUNCH_CHECK();
 }
 
@@ -379,7 +398,9 @@ void stage_place_arena(const SlabDev &d, uint32_t *arena, int64_t w0, int64_t nw
   a.out = arena;
   k_write_header<<<a.nblocks, kHdrThreads, 0, st>>>(a, 0);
   BZ_LAUNCH_CHECK();
-  k_write_payload<<<a.n_group_tiles, kGroupTile, 0, st>>>(a, 0);
+  launch_groups(a, st, [&](int grid, const int32_t *list) {
+    k_write_payload<<<grid, kGroupTile, 0, st>>>(a, 0, list);
+  });
   BZ_LAUNCH_CHECK();
 }
 
@@ -418,7 +439,9 @@ void launch_splice(const int64_t *src_addr, const int64_t *dst_bit, const int64_
 }
 
 void launch_pack_words(const SlabDev &d, uint32_t *words, cudaStream_t st) {
-  k_pack_words<<<d.n_group_tiles, kGroupTile, 0, st>>>(d, words);
+  launch_groups(d, st, [&](int grid, const int32_t *list) {
+    k_pack_words<<<grid, kGroupTile, 0, st>>>(d, words, list);
+  });
   BZ_LAUNCH_CHECK();
 }
 

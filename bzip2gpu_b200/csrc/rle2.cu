@@ -22,11 +22,12 @@ __device__ __forceinline__ int tile_len(const SlabDev &d, int t, int *b, int *lt
   return min(kTile, *m - *lt);
 }
 
-__global__ void __launch_bounds__(256) k_rle2_scan_tiles(SlabDev d) {
+__global__ void __launch_bounds__(256) k_rle2_scan_tiles(SlabDev d, const int32_t *list) {
+  const int t = list ? list[blockIdx.x] : (int)blockIdx.x;
   __shared__ int red[2][8];
   int b, lt, m;
   int64_t off;
-  int valid = tile_len(d, blockIdx.x, &b, &lt, &off, &m);
+  int valid = tile_len(d, t, &b, &lt, &off, &m);
   if (valid <= 0) return;
   const uint8_t *V = d.mtf + off;
   int first = INT32_MAX, last = -1;
@@ -51,8 +52,8 @@ __global__ void __launch_bounds__(256) k_rle2_scan_tiles(SlabDev d) {
       f = min(f, red[0][w]);
       l = max(l, red[1][w]);
     }
-    d.tile_a[blockIdx.x] = f;
-    d.tile_b[blockIdx.x] = l;
+    d.tile_a[t] = f;
+    d.tile_b[t] = l;
   }
 }
 
@@ -102,8 +103,8 @@ struct ZeroRuns {
   int before, after;
 };
 
-__device__ __forceinline__ ZeroRuns zero_run_bounds(const SlabDev &d, const uint8_t *V, int lt,
-                                                    int valid, int p0, int *wl, int *wf) {
+__device__ __forceinline__ ZeroRuns zero_run_bounds(const SlabDev &d, const uint8_t *V, int t,
+                                                    int lt, int valid, int p0, int *wl, int *wf) {
   int ls = -1, fs = INT32_MAX;
   for (int k = 0; k < kTileItems; k++) {
     int e = p0 + k;
@@ -125,21 +126,22 @@ __device__ __forceinline__ ZeroRuns zero_run_bounds(const SlabDev &d, const uint
   int after = lane_id() == 31 ? INT32_MAX : exm;
   for (int w = warp_id() + 1; w < (int)(blockDim.x >> 5); w++) after = min(after, wf[w]);
   ZeroRuns r;
-  r.before = max(before, d.tile_b[blockIdx.x]);
-  r.after = min(after, d.tile_a[blockIdx.x]);
+  r.before = max(before, d.tile_b[t]);
+  r.after = min(after, d.tile_a[t]);
   return r;
 }
 
-__global__ void __launch_bounds__(256) k_rle2_count(SlabDev d) {
+__global__ void __launch_bounds__(256) k_rle2_count(SlabDev d, const int32_t *list) {
+  const int t = list ? list[blockIdx.x] : (int)blockIdx.x;
   __shared__ int scratch[40];
   __shared__ int wl[8], wf[8];
   int b, lt, m;
   int64_t off;
-  int valid = tile_len(d, blockIdx.x, &b, &lt, &off, &m);
+  int valid = tile_len(d, t, &b, &lt, &off, &m);
   if (valid <= 0) return;
   const uint8_t *V = d.mtf + off;
   const int p0 = threadIdx.x * kTileItems;
-  ZeroRuns zr = zero_run_bounds(d, V, lt, valid, p0, wl, wf);
+  ZeroRuns zr = zero_run_bounds(d, V, t, lt, valid, p0, wl, wf);
   int ends[kTileItems];
   {
     int cur = zr.after;
@@ -167,7 +169,7 @@ __global__ void __launch_bounds__(256) k_rle2_count(SlabDev d) {
   }
   int tot;
   block_excl_sum(cnt, scratch, &tot);
-  if (threadIdx.x == 0) d.tile_c[blockIdx.x] = tot;
+  if (threadIdx.x == 0) d.tile_c[t] = tot;
 }
 
 __global__ void __launch_bounds__(256) k_rle2_block_offsets(SlabDev d) {
@@ -193,18 +195,19 @@ __global__ void __launch_bounds__(256) k_rle2_block_offsets(SlabDev d) {
   }
 }
 
-__global__ void __launch_bounds__(256) k_rle2_write(SlabDev d) {
+__global__ void __launch_bounds__(256) k_rle2_write(SlabDev d, const int32_t *list) {
+  const int t = list ? list[blockIdx.x] : (int)blockIdx.x;
   __shared__ int scratch[40];
   __shared__ int wl[8], wf[8];
   __shared__ int hist[kMaxAlpha];
   int b, lt, m;
   int64_t off;
-  int valid = tile_len(d, blockIdx.x, &b, &lt, &off, &m);
+  int valid = tile_len(d, t, &b, &lt, &off, &m);
   if (valid <= 0) return;
   for (int i = threadIdx.x; i < kMaxAlpha; i += blockDim.x) hist[i] = 0;
   const uint8_t *V = d.mtf + off;
   const int p0 = threadIdx.x * kTileItems;
-  ZeroRuns zr = zero_run_bounds(d, V, lt, valid, p0, wl, wf);
+  ZeroRuns zr = zero_run_bounds(d, V, t, lt, valid, p0, wl, wf);
   int ends[kTileItems];
   {
     int cur = zr.after;
@@ -234,7 +237,7 @@ __global__ void __launch_bounds__(256) k_rle2_write(SlabDev d) {
   }
   int tot;
   int o = block_excl_sum(cnt, scratch, &tot);
-  uint16_t *out = d.rle2 + off + d.tile_c[blockIdx.x] + o;
+  uint16_t *out = d.rle2 + off + d.tile_c[t] + o;
   int prev_nz = zr.before;
 #pragma unroll
   for (int k = 0; k < kTileItems; k++) {
@@ -271,16 +274,25 @@ __global__ void __launch_bounds__(256) k_rle2_write(SlabDev d) {
 
 void stage_rle2(const SlabDev &d, cudaStream_t st) {
   BZ_CUDA(cudaMemsetAsync(d.freq, 0, sizeof(int32_t) * kMaxAlpha * d.nblocks, st));
-  k_rle2_scan_tiles<<<d.ntiles, 256, 0, st>>>(d);
-  BZ_LAUNCH_CHECK();
+  const int nlive = live_tiles(d, st);
+  const int grid = nlive >= 0 ? nlive : d.ntiles;
+  const int32_t *list = nlive >= 0 ? d.vt_list : nullptr;
+  if (grid > 0) {
+    k_rle2_scan_tiles<<<grid, 256, 0, st>>>(d, list);
+    BZ_LAUNCH_CHECK();
+  }
   k_rle2_block_carry<<<d.nblocks, 256, 0, st>>>(d);
   BZ_LAUNCH_CHECK();
-  k_rle2_count<<<d.ntiles, 256, 0, st>>>(d);
-  BZ_LAUNCH_CHECK();
+  if (grid > 0) {
+    k_rle2_count<<<grid, 256, 0, st>>>(d, list);
+    BZ_LAUNCH_CHECK();
+  }
   k_rle2_block_offsets<<<d.nblocks, 256, 0, st>>>(d);
   BZ_LAUNCH_CHECK();
-  k_rle2_write<<<d.ntiles, 256, 0, st>>>(d);
-  BZ_LAUNCH_CHECK();
+  if (grid > 0) {
+    k_rle2_write<<<grid, 256, 0, st>>>(d, list);
+    BZ_LAUNCH_CHECK();
+  }
 }
 
 }  // namespace bz2g
