@@ -311,9 +311,10 @@ def run_stress(args):
                           "bwt_rounds": rows}))
 
 
-# DRAM bytes per algorithmic byte of k_radix_scatter: (127.4 + 76.6) MB / 256 MB
-# in an ncu capture of its first-sort pass over a 64-block slab
-TRAFFIC_PER_ALGO_BYTE = 204.0 / 256.0
+# DRAM bytes per algorithmic byte of k_radix_scatter: (255.06 + 203.20) MB /
+# 494.13 MB in an ncu capture of the second pass of the first sort over a
+# 128-block slab (profiles/k_radix_scatter_ncu_full_256MiB.md)
+TRAFFIC_PER_ALGO_BYTE = (255.06 + 203.20) / 494.13
 
 
 def main():
@@ -510,16 +511,15 @@ def main():
     # durations of its launches on their worker streams in the last timed step
     sc_ms = stats["scatter_ms"]
     sc_gbs = stats["scatter_bytes"] / (sc_ms / 1e3) / 1e9 if sc_ms > 0 else 0.0
-    # DRAM traffic per launch, scaled from one ncu capture of the scatter's
-    # first-sort pass (128 MiB stream, one worker: 127.4 MB read + 76.6 MB
-    # written for 256 MB of algorithmic bytes) by this launch's algorithmic
-    # bytes
+    # DRAM traffic per launch, scaled from one ncu capture of the scatter
+    # (profiles/k_radix_scatter_ncu_full_256MiB.md: 0.927 DRAM bytes per
+    # algorithmic byte) by this launch's algorithmic bytes
     per_launch = stats["scatter_bytes"] / max(stats["scatter_launches"], 1)
     traffic = int(per_launch * TRAFFIC_PER_ALGO_BYTE)
     roof = {"bound": "hbm", "achieved": round(sc_gbs, 1), "peak": peak, "unit": "GB/s",
             "frac": round(sc_gbs / peak, 4), "traffic": traffic,
-            "traffic_source": "ncu dram bytes of the first-sort scatter pass (128 MiB stream), "
-                              "0.797 per algorithmic byte, scaled to this launch",
+            "traffic_source": "ncu dram bytes of a first-sort scatter pass (256 MiB stream, "
+                              "128-block slab), 0.927 per algorithmic byte, scaled to this launch",
             "kernel": "k_radix_scatter (BWT radix sort scatter)",
             "launches_per_step": int(stats["scatter_launches"]),
             "avg_launch_us": round(1e3 * sc_ms / max(stats["scatter_launches"], 1), 1),
