@@ -325,6 +325,8 @@ def main():
     ap.add_argument("--size", type=int, default=10 << 30)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-isolated", action="store_true",
+                    help="skip the one-worker timing of the scatter kernel")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the many-inputs (batched form) measurement")
     ap.add_argument("--no-check", action="store_true",
@@ -530,6 +532,29 @@ def main():
                 "achieved_gbs": round(mb / step_s / 1e9, 1),
                 "frac_of_hbm": round(mb / step_s / 1e9 / peak, 4)}
 
+    # The same scatter kernel with the GPU to itself: one worker stream over
+    # the first 2 GiB of the stream (in the timed region above five worker
+    # streams share the GPU, so each launch's event time includes the other
+    # streams' kernels).  Outside the timed region; an explanation of the
+    # roofline figure, not the metric.
+    iso = None
+    if not args.no_isolated:
+        k = min(n, 2 << 30)
+        d_part = h_in[:k].cuda() if not args.no_e2e else d_in[:k]
+        B.set_engine(args.slab or 128, 1)
+        B.compress_device(d_part, 9)
+        B.compress_device(d_part, 9)
+        torch.cuda.synchronize()
+        st1 = B.last_stats()
+        B.set_engine(args.slab or 128, args.workers or 5)
+        del d_part
+        if st1["scatter_ms"] > 0:
+            g1 = st1["scatter_bytes"] / (st1["scatter_ms"] / 1e3) / 1e9
+            iso = {"achieved": round(g1, 1), "frac": round(g1 / peak, 4), "workers": 1,
+                   "bytes": int(k), "launches": int(st1["scatter_launches"]),
+                   "avg_launch_us": round(1e3 * st1["scatter_ms"] /
+                                          max(st1["scatter_launches"], 1), 1)}
+
     cpu = None
     if rank == 0 and world == 1:
         import oracle
@@ -553,7 +578,8 @@ def main():
             "config": {"workload": WORKLOAD, "bytes_per_rank": n, "block_bytes": 900000,
                        "level": 9, "form": "plain", "l2": "input larger than L2",
                        "blocks": int(stats["blocks"]), "ratio": round(ratio, 4)},
-            "e2e": e2e, "roofline": roof, "pipeline_roofline": pipeline, "cpu_baseline": cpu,
+            "e2e": e2e, "roofline": roof, "roofline_isolated": iso,
+            "pipeline_roofline": pipeline, "cpu_baseline": cpu,
             "forms": {"plain": round(value, 2), "batched": round(batched_value, 2),
                       "learned": learned, "bzip2_format": bzip2_form,
                       "batched_many_inputs": batch_many},
