@@ -221,54 +221,30 @@ __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d, const int32_t *list
   // The list is handled eight entries at a time: entry 8i+q is byte q of
   // little-endian word i.  A word without the symbol shifts up one byte (its
   // top byte carries into the next word); in the word holding it, the bytes
-  // below it shift up and it leaves.  Word 0 (the eight most recent
-  // symbols, where most symbols are found) stays in a register; the symbols
-  // are read and their indices written four at a time.
+  // below it shift up and it leaves.
   {
     uint64_t *lw = reinterpret_cast<uint64_t *>(lists + ln * kListStride);
     const uint64_t ones = 0x0101010101010101ull, highs = 0x8080808080808080ull;
-    uint64_t r0 = lw[0];
-    const int n = a1 - a0;
-    uint32_t *s32 = reinterpret_cast<uint32_t *>(mySL + a0);  // 4-byte aligned
-    for (int i4 = 0; i4 < n; i4 += 4) {
-      const uint32_t in4 = s32[i4 >> 2];
-      uint32_t out4 = in4;
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        if (i4 + k < n) {
-          const uint32_t c = (in4 >> (8 * k)) & 0xffu;
-          const uint64_t bc = ones * c;
-          const uint64_t x0 = r0 ^ bc;
-          const uint64_t z0 = (x0 - ones) & ~x0 & highs;  // lowest set bit: the first match
-          int q;
-          if (z0) {
-            const int j = (__ffsll((long long)z0) - 1) >> 3;
-            const uint64_t low = j == 7 ? ~0ull : ((1ull << (8 * (j + 1))) - 1);
-            r0 = (r0 & ~low) | (((r0 << 8) | c) & low);
-            q = j;
-          } else {
-            uint64_t carry = r0 >> 56;
-            r0 = (r0 << 8) | c;
-            q = 0;
-            for (int wi = 1; wi < 32; wi++) {
-              const uint64_t wv = lw[wi];
-              const uint64_t x = wv ^ bc;
-              const uint64_t z = (x - ones) & ~x & highs;
-              if (z) {
-                const int j = (__ffsll((long long)z) - 1) >> 3;
-                const uint64_t low = j == 7 ? ~0ull : ((1ull << (8 * (j + 1))) - 1);
-                lw[wi] = (wv & ~low) | (((wv << 8) | carry) & low);
-                q = wi * 8 + j;
-                break;
-              }
-              lw[wi] = (wv << 8) | carry;
-              carry = wv >> 56;
-            }
-          }
-          out4 = (out4 & ~(0xffu << (8 * k))) | ((uint32_t)q << (8 * k));
+    for (int i = a0; i < a1; i++) {
+      const uint32_t c = mySL[i];
+      const uint64_t bc = ones * c;
+      uint64_t carry = c;
+      int q = 0;
+      for (int wi = 0; wi < 32; wi++) {
+        const uint64_t wv = lw[wi];
+        const uint64_t x = wv ^ bc;
+        const uint64_t z = (x - ones) & ~x & highs;  // lowest set bit marks the first match
+        if (z) {
+          const int j = (__ffsll((long long)z) - 1) >> 3;
+          const uint64_t low = j == 7 ? ~0ull : ((1ull << (8 * (j + 1))) - 1);
+          lw[wi] = (wv & ~low) | (((wv << 8) | carry) & low);
+          q = wi * 8 + j;
+          break;
         }
+        lw[wi] = (wv << 8) | carry;
+        carry = wv >> 56;
       }
-      s32[i4 >> 2] = out4;
+      mySL[i] = (uint8_t)q;
     }
   }
   __syncwarp();
