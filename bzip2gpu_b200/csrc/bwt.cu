@@ -652,21 +652,24 @@ void stage_bwt(const SlabDev &d, int max_m, cudaStream_t st) {
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScatterSmem));
     smem_configured = true;
   }
-  int kb = 1;
-  while ((1ll << kb) <= (int64_t)max_m) kb++;
-  const int packed = 3 * kb <= 64;
   k_bwt_init<<<(d.nblocks + 127) / 128, 128, 0, st>>>(d);
   BZ_LAUNCH_CHECK();
   if (max_m <= 1) return;
+  // the tiles holding rotations (a block's workspace has room for its
+  // worst-case RLE1 output, so most of its tiles are usually empty), and the
+  // slab's largest m, which sets the width of the rank fields
+  const int nlive = live_tiles(d, st);
+  if (nlive == 0) return;
+  if (nlive > 0 && d.live[2] >= 0) max_m = std::min(max_m, std::max(d.live[2], 1));
+  if (max_m <= 1) return;
+  int kb = 1;
+  while ((1ll << kb) <= (int64_t)max_m) kb++;
+  const int packed = 3 * kb <= 64;
   bool rounds_timed = d.kt_on && d.rt_ev != nullptr;
   if (rounds_timed) {
     d.rt_act[0] = 0;
     BZ_CUDA(cudaEventRecord(d.rt_ev[0], st));
   }
-  // the tiles holding rotations (a block's workspace has room for its
-  // worst-case RLE1 output, so most of its tiles are usually empty)
-  const int nlive = live_tiles(d, st);
-  if (nlive == 0) return;
   const int grid0 = nlive > 0 ? nlive : d.ntiles;
   const int32_t *list0 = nlive > 0 ? d.vt_list : nullptr;
   // first sort: 4-byte prefixes in the high half of packed items, or 8-byte keys

@@ -167,8 +167,8 @@ Workspace::Workspace(int mb, int64_t mr, int64_t me, int mt, int mrt, int mgt)
     plan_dev_ = alloc(pinned_plan_bytes);
     BZ_CUDA(cudaMallocHost(&pinned_plan, pinned_plan_bytes));
     BZ_CUDA(cudaMallocHost((void **)&dev.h_flags, 64));
-    BZ_CUDA(cudaMallocHost((void **)&dev.live, 4 * sizeof(int)));
-    dev.live[0] = dev.live[1] = -1;
+    BZ_CUDA(cudaMallocHost((void **)&dev.live, 8 * sizeof(int)));
+    dev.live[0] = dev.live[1] = dev.live[2] = -1;
   } catch (...) {
     for (void *p : allocs_) cudaFree(p);
     allocs_.clear();
@@ -187,7 +187,7 @@ Workspace::~Workspace() {
 }
 
 void Workspace::upload_plan(const SlabPlan &p, cudaStream_t st) {
-  dev.live[0] = dev.live[1] = -1;  // a new slab: its tile lists are built anew
+  dev.live[0] = dev.live[1] = dev.live[2] = -1;  // a new slab: its lists are built anew
   BZ_REQUIRE(p.nblocks <= max_blocks && p.raw_total <= max_raw && p.elem_total <= max_elems &&
                  (int)p.tile_block.size() <= max_tiles && (int)p.rt_block.size() <= max_raw_tiles &&
                  (int)p.gt_block.size() <= max_group_tiles,
@@ -242,7 +242,7 @@ namespace {
 __global__ void __launch_bounds__(256) k_live_tiles(SlabDev d, int groups) {
   __shared__ int scratch[40];
   int32_t *list = groups ? d.vg_list : d.vt_list;
-  int base = 0;
+  int base = 0, mmax = 0;
   for (int b0 = 0; b0 < d.nblocks; b0 += 256) {
     const int b = b0 + threadIdx.x;
     int cnt = 0, first = 0;
@@ -256,6 +256,7 @@ __global__ void __launch_bounds__(256) k_live_tiles(SlabDev d, int groups) {
         const int m = d.m[b];
         cnt = m > 0 ? (m + kTile - 1) / kTile : 0;
         first = (int)(d.off[b] / kTile);
+        mmax = max(mmax, m);
       }
     }
     int tot;
@@ -263,18 +264,24 @@ __global__ void __launch_bounds__(256) k_live_tiles(SlabDev d, int groups) {
     for (int k = 0; k < cnt; k++) list[at + k] = first + k;
     base += tot;
   }
+  if (!groups) {
+    for (int o = 16; o > 0; o >>= 1) mmax = max(mmax, __shfl_xor_sync(0xffffffffu, mmax, o));
+    if (lane_id() == 0) atomicMax(&d.sort_ctl[12], mmax);
+  }
   if (threadIdx.x == 0) d.sort_ctl[10 + groups] = base;
 }
 
 int live_list(const SlabDev &d, cudaStream_t st, int groups) {
   if (!d.live) return -1;
   if (d.live[groups] >= 0) return d.live[groups];
+  if (!groups) BZ_CUDA(cudaMemsetAsync(d.sort_ctl + 12, 0, sizeof(int32_t), st));
   k_live_tiles<<<1, 256, 0, st>>>(d, groups);
   BZ_LAUNCH_CHECK();
-  BZ_CUDA(cudaMemcpyAsync(d.live + 2, d.sort_ctl + 10 + groups, sizeof(int32_t),
+  BZ_CUDA(cudaMemcpyAsync(d.live + 4, d.sort_ctl + 10, 3 * sizeof(int32_t),
                           cudaMemcpyDeviceToHost, st));
   BZ_CUDA(cudaStreamSynchronize(st));
-  d.live[groups] = d.live[2];
+  d.live[groups] = d.live[4 + groups];
+  if (!groups) d.live[2] = d.live[6];  // the largest m of the slab
   return d.live[groups];
 }
 

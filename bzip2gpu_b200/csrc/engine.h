@@ -95,7 +95,8 @@ struct SlabDev {
   // sized for its worst-case RLE1 output, so most of its tiles can be empty):
   // element tiles of the m[b] RLE1 bytes, and group tiles of the
   // ceil(s[b] / 50) groups.  live (pinned host) [0], [1]: their counts once
-  // known for this slab, -1 before (kernels then run over every tile).
+  // known for this slab, -1 before (kernels then run over every tile); [2]:
+  // the slab's largest m, known with [0]; [4..6]: staging.
   int32_t *vt_list, *vg_list;
   int *live;
   int32_t *warp_last, *warp_act;       // BWT: per 512-element warp span [ntiles * 8]: last
@@ -109,6 +110,7 @@ struct SlabDev {
                                        // [4]=tiles of the next round, [5]=tile list fill,
                                        // [6]=rotations entering the next round,
                                        // [8..9]=u64 rotations the first sort's model charges
+                                       // [10], [11]=tile-list counts, [12]=largest m
   int32_t *h_flags;                    // pinned host mirror of small counters
   // stream state: [0] = bit offset (u64), [1] = stream crc, [2] = slab first word,
   // [3] = slab word count
