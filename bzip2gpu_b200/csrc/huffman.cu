@@ -135,7 +135,24 @@ __global__ void __launch_bounds__(kGroupTile) k_huff_select(SlabDev d, int which
       }
     }
     sel_dst[off / 32 + g0 + g] = (uint8_t)bt;
-    for (int i = a; i < e; i++) atomicAdd(&rf[bt * kMaxAlpha + sy[i]], 1);
+    // RUNA, RUNB and MTF index 1 (symbols 0, 1, 2) make up most of a block's
+    // symbols: count them in registers, so that the threads of a warp do not
+    // all add to the same few counters one symbol at a time
+    int c0 = 0, c1 = 0, c2 = 0;
+    int *rft = rf + bt * kMaxAlpha;
+    for (int i = a; i < e; i++) {
+      const int v = sy[i];
+      if (v < 3) {
+        c0 += v == 0;
+        c1 += v == 1;
+        c2 += v == 2;
+      } else {
+        atomicAdd(&rft[v], 1);
+      }
+    }
+    if (c0) atomicAdd(&rft[0], c0);
+    if (c1) atomicAdd(&rft[1], c1);
+    if (c2) atomicAdd(&rft[2], c2);
   }
   __syncthreads();
   int32_t *rfreq = rf_dst + (size_t)b * kMaxGroups * kMaxAlpha;

@@ -18,7 +18,6 @@ namespace {
 // list: the tiles to run (blockIdx.x-th entry), or nullptr for every tile.
 __global__ void __launch_bounds__(256) k_mtf_last(SlabDev d, const int32_t *list) {
   __shared__ int lastpos[256];
-  __shared__ uint32_t pres[8];
   const int t = list ? list[blockIdx.x] : (int)blockIdx.x;
   const int b = d.tile_block[t];
   const int64_t off = d.off[b];
@@ -27,7 +26,6 @@ __global__ void __launch_bounds__(256) k_mtf_last(SlabDev d, const int32_t *list
   const int valid = min(kTile, m - lt);
   if (valid <= 0) return;
   lastpos[threadIdx.x] = -1;
-  if (threadIdx.x < 8) pres[threadIdx.x] = 0;
   __syncthreads();
   const uint8_t *T = d.rle1 + off;
   const int32_t *SA = d.sa + off;
@@ -39,11 +37,14 @@ __global__ void __launch_bounds__(256) k_mtf_last(SlabDev d, const int32_t *list
     uint8_t c = T[i == 0 ? m - 1 : i - 1];
     L[j] = c;
     atomicMax(&lastpos[c], j);
-    atomicOr(&pres[c >> 5], 1u << (c & 31));
   }
   __syncthreads();
-  d.tile_last[(size_t)t * 256 + threadIdx.x] = lastpos[threadIdx.x];
-  if (threadIdx.x < 8 && pres[threadIdx.x]) atomicOr(&d.present[b * 8 + threadIdx.x], pres[threadIdx.x]);
+  // thread k stands for symbol k: the symbols present in the tile are those
+  // with a last position, one ballot per 32 symbols
+  const int lp = lastpos[threadIdx.x];
+  d.tile_last[(size_t)t * 256 + threadIdx.x] = lp;
+  const unsigned pb = __ballot_sync(0xffffffffu, lp >= 0);
+  if (lane_id() == 0 && pb) atomicOr(&d.present[b * 8 + warp_id()], pb);
 }
 
 // Per block, per symbol: exclusive prefix max of last positions over tiles.

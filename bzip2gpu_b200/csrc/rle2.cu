@@ -239,6 +239,9 @@ __global__ void __launch_bounds__(256) k_rle2_write(SlabDev d, const int32_t *li
   int o = block_excl_sum(cnt, scratch, &tot);
   uint16_t *out = d.rle2 + off + d.tile_c[t] + o;
   int prev_nz = zr.before;
+  // RUNA, RUNB and symbol 2 (MTF index 1) are most of the symbols: counted
+  // in registers, added to the tile's histogram once per thread
+  int h0 = 0, h1 = 0, h2 = 0;
 #pragma unroll
   for (int k = 0; k < kTileItems; k++) {
     int e = p0 + k;
@@ -246,7 +249,10 @@ __global__ void __launch_bounds__(256) k_rle2_write(SlabDev d, const int32_t *li
       int v = V[lt + e];
       if (v != 0) {
         *out++ = (uint16_t)(v + 1);
-        atomicAdd(&hist[v + 1], 1);
+        if (v == 1)
+          h2++;
+        else
+          atomicAdd(&hist[v + 1], 1);
         prev_nz = lt + e;
       } else {
         int zs = prev_nz + 1;
@@ -260,11 +266,15 @@ __global__ void __launch_bounds__(256) k_rle2_write(SlabDev d, const int32_t *li
             k2 >>= 1;
           }
           *out++ = (uint16_t)dgt;
-          atomicAdd(&hist[dgt], 1);
+          h0 += dgt == 0;
+          h1 += dgt == 1;
         }
       }
     }
   }
+  if (h0) atomicAdd(&hist[0], h0);
+  if (h1) atomicAdd(&hist[1], h1);
+  if (h2) atomicAdd(&hist[2], h2);
   __syncthreads();
   for (int i = threadIdx.x; i < kMaxAlpha; i += blockDim.x)
     if (hist[i]) atomicAdd(&d.freq[b * kMaxAlpha + i], hist[i]);
