@@ -565,6 +565,20 @@ def main():
                "kind": "port",
                "sample": f"{sample.size} bytes: {CPU_SAMPLE_NOTE}; oracle port of the "
                          f"reference path, {threads} threads"}
+        # A familiar yardstick, not bit-comparable: bzip2 -9 (libbz2 1.0.8, through
+        # Python's bz2 module, which releases the GIL) on independent 900,000-byte
+        # pieces of the same sample, one piece per task on all host threads.
+        import bz2
+        from concurrent.futures import ThreadPoolExecutor
+        pieces = [sample[i:i + 900000].tobytes() for i in range(0, sample.size, 900000)]
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(threads) as ex:
+            zbytes = sum(len(z) for z in ex.map(lambda x: bz2.compress(x, 9), pieces))
+        zdt = time.perf_counter() - t0
+        cpu["libbz2_yardstick"] = {"MB/s": round(sample.size / zdt / 1e6, 2), "threads": threads,
+                                   "ratio": round(zbytes / sample.size, 4),
+                                   "what": "bzip2 -9 (libbz2 1.0.8) on independent 900,000-byte "
+                                           "pieces of the same sample"}
 
     if rank == 0:
         stage_ms = {k[3:]: round(v / args.steps if False else v, 1)
