@@ -533,7 +533,7 @@ def main():
                 "frac_of_hbm": round(mb / step_s / 1e9 / peak, 4)}
 
     # The same scatter kernel with the GPU to itself: one worker stream over
-    # the first 2 GiB of the stream (in the timed region above five worker
+    # the first 2 GiB of the stream (in the timed region above the worker
     # streams share the GPU, so each launch's event time includes the other
     # streams' kernels).  Outside the timed region; an explanation of the
     # roofline figure, not the metric.
@@ -541,12 +541,13 @@ def main():
     if not args.no_isolated:
         k = min(n, 2 << 30)
         d_part = h_in[:k].cuda() if not args.no_e2e else d_in[:k]
-        B.set_engine(args.slab or 128, 1)
+        shape = B.get_engine()
+        B.set_engine(shape[0], 1)
         B.compress_device(d_part, 9)
         B.compress_device(d_part, 9)
         torch.cuda.synchronize()
         st1 = B.last_stats()
-        B.set_engine(args.slab or 128, args.workers or 5)
+        B.set_engine(*shape)
         del d_part
         if st1["scatter_ms"] > 0:
             g1 = st1["scatter_bytes"] / (st1["scatter_ms"] / 1e3) / 1e9

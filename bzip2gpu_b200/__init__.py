@@ -20,7 +20,7 @@ import numpy as np
 
 __all__ = [
     "Bz2gError", "lib", "lib_path", "compress", "compress_device", "compress_bound",
-    "set_engine", "compress_into", "compress_device_into", "compress_batch", "rle1", "crc32", "bwt", "mtf", "symbols_table", "rle2", "huffman_build",
+    "set_engine", "get_engine", "compress_into", "compress_device_into", "compress_batch", "rle1", "crc32", "bwt", "mtf", "symbols_table", "rle2", "huffman_build",
     "huffman_encode", "count_frequencies", "gen_markov", "gen_uniform", "MAX_GROUPS",
     "MAX_ALPHA", "SELECTOR_PARAMS", "selector_load", "set_selector", "get_selector",
     "selector_logits", "huffman_build_learned", "selector_dataset", "compress_part",
@@ -52,6 +52,7 @@ _SIGS = {
     "bz2g_compress_batch_bound": (_sz, [_i, _vp, _vp, _vp]),
     "bz2g_free": (None, [_vp]),
     "bz2g_set_engine": (_i, [_i, _i]),
+    "bz2g_get_engine": (_i, [_c.POINTER(_i), _c.POINTER(_i)]),
     "bz2g_set_batch_tuning": (_i, [_i, _vp, _vp, _vp]),
     "bz2g_set_timing": (_i, [_i]),
     "bz2g_last_stats": (_i, [_c.POINTER(_c.c_double), _i]),
@@ -344,6 +345,13 @@ def compress_bound(n: int, block_bytes: int = 900000) -> int:
 
 def set_engine(slab_blocks: int = 0, workers: int = 0) -> None:
     _check(lib().bz2g_set_engine(slab_blocks, workers))
+
+
+def get_engine() -> tuple[int, int]:
+    """The engine shape of the whole-stream calls: (slab_blocks, workers)."""
+    sb, nw = _c.c_int(0), _c.c_int(0)
+    _check(lib().bz2g_get_engine(_c.byref(sb), _c.byref(nw)))
+    return sb.value, nw.value
 
 
 def set_timing(on: bool) -> None:

@@ -99,7 +99,7 @@ struct EngineKey {
 };
 std::mutex g_eng_mu;
 std::map<EngineKey, std::unique_ptr<Compressor>> g_engines;
-int g_slab = 128, g_workers = 5;
+int g_slab = 384, g_workers = 4;
 std::vector<Compressor::BatchTune> g_batch_tune;  // batched form, by block length
 bool g_timing = false;
 thread_local StageTimes g_last_stats;
@@ -272,6 +272,15 @@ int bz2g_set_engine(int slab_blocks, int workers) {
     std::lock_guard<std::mutex> g(g_eng_mu);
     if (slab_blocks > 0) g_slab = slab_blocks;
     if (workers > 0) g_workers = workers;
+  });
+}
+
+int bz2g_get_engine(int *slab_blocks, int *workers) {
+  return guard([&] {
+    BZ_REQUIRE(slab_blocks && workers, kErrArg, "null output pointer");
+    std::lock_guard<std::mutex> g(g_eng_mu);
+    *slab_blocks = g_slab;
+    *workers = g_workers;
   });
 }
 

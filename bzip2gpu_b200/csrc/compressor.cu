@@ -43,6 +43,43 @@ struct Compressor::Worker {
   int kt_n = 0;
   int kt_bpe[kMaxTimedLaunches] = {};
   uint64_t *h_kt = nullptr;
+  // The slab workspace and the host arrays strided by its block slots.
+  void release_slab() {
+    delete ws;
+    ws = nullptr;
+    for (void *p : {(void *)h_out, (void *)h_sizes, (void *)h_crc, (void *)h_cnt,
+                    (void *)h_act, (void *)h_err})
+      if (p) cudaFreeHost(p);
+    h_out = nullptr;
+    h_sizes = nullptr;
+    h_crc = nullptr;
+    h_cnt = nullptr;
+    h_act = nullptr;
+    h_err = nullptr;
+    h_out_cap = 0;
+    slots = 0;
+  }
+  // (Re)creates them for slabs of up to `blocks` blocks of max_block_bytes.
+  void size_slab(int blocks, int64_t max_block_bytes) {
+    BZ_CUDA(cudaStreamSynchronize(st));
+    release_slab();
+    ws = Workspace::create_for(blocks, max_block_bytes, kBatchSlots);
+    slots = ws->max_blocks;
+    const int S = slots;
+    h_out_cap = (size_t)ws->out_words * 4;
+    BZ_CUDA(cudaMallocHost((void **)&h_out, h_out_cap));
+    BZ_CUDA(cudaMallocHost((void **)&h_sizes, sizeof(int64_t) * 2 * S));
+    BZ_CUDA(cudaMallocHost((void **)&h_crc, sizeof(uint32_t) * S));
+    BZ_CUDA(cudaMallocHost((void **)&h_cnt, sizeof(int32_t) * 5 * S));
+    BZ_CUDA(cudaMallocHost((void **)&h_act, sizeof(int64_t) * S));
+    BZ_CUDA(cudaMallocHost((void **)&h_err, sizeof(int32_t)));
+    ws->dev.rt_ev = rt_ev;
+    ws->dev.rt_n = &rt_n;
+    ws->dev.rt_act = rt_act;
+    ws->dev.kt_ev = kt_ev;
+    ws->dev.kt_n = &kt_n;
+    ws->dev.kt_bpe = kt_bpe;
+  }
   ~Worker() {
     if (st) cudaStreamSynchronize(st);
     for (auto &e : ev)
@@ -52,13 +89,7 @@ struct Compressor::Worker {
     for (auto &e : rt_ev)
       if (e) cudaEventDestroy(e);
     if (h_kt) cudaFreeHost(h_kt);
-    delete ws;
-    if (h_out) cudaFreeHost(h_out);
-    if (h_sizes) cudaFreeHost(h_sizes);
-    if (h_crc) cudaFreeHost(h_crc);
-    if (h_cnt) cudaFreeHost(h_cnt);
-    if (h_act) cudaFreeHost(h_act);
-    if (h_err) cudaFreeHost(h_err);
+    release_slab();
     if (st) cudaStreamDestroy(st);
   }
 };
@@ -69,29 +100,28 @@ Compressor::Compressor(const CompressorConfig &cfg) : cfg_(cfg) {
   if (cfg_.workers < 1) cfg_.workers = 1;
   for (int i = 0; i < cfg_.workers; i++) {
     auto w = std::make_unique<Worker>();
-    w->ws = Workspace::create_for(cfg_.slab_blocks, cfg_.max_block_bytes, kBatchSlots);
-    w->slots = w->ws->max_blocks;
-    const int S = w->slots;
     BZ_CUDA(cudaStreamCreateWithFlags(&w->st, cudaStreamNonBlocking));
-    w->h_out_cap = (size_t)w->ws->out_words * 4;
-    BZ_CUDA(cudaMallocHost((void **)&w->h_out, w->h_out_cap));
-    BZ_CUDA(cudaMallocHost((void **)&w->h_sizes, sizeof(int64_t) * 2 * S));
-    BZ_CUDA(cudaMallocHost((void **)&w->h_crc, sizeof(uint32_t) * S));
-    BZ_CUDA(cudaMallocHost((void **)&w->h_cnt, sizeof(int32_t) * 5 * S));
-    BZ_CUDA(cudaMallocHost((void **)&w->h_act, sizeof(int64_t) * S));
-    BZ_CUDA(cudaMallocHost((void **)&w->h_err, sizeof(int32_t)));
     for (auto &e : w->ev) BZ_CUDA(cudaEventCreate(&e));
     for (auto &e : w->kt_ev) BZ_CUDA(cudaEventCreate(&e));
     for (auto &e : w->rt_ev) BZ_CUDA(cudaEventCreate(&e));
-    w->ws->dev.rt_ev = w->rt_ev;
-    w->ws->dev.rt_n = &w->rt_n;
-    w->ws->dev.rt_act = w->rt_act;
     BZ_CUDA(cudaMallocHost((void **)&w->h_kt, 8 * kMaxTimedLaunches));
-    w->ws->dev.kt_ev = w->kt_ev;
-    w->ws->dev.kt_n = &w->kt_n;
-    w->ws->dev.kt_bpe = w->kt_bpe;
     workers_.push_back(std::move(w));
   }
+}
+
+// Slab workspaces are sized on demand (caller holds the call lock): a call
+// of `blocks` blocks needs slabs of at most min(blocks, slab_blocks) blocks,
+// so small calls take little device memory.  A call that needs more than
+// the workers hold grows every worker's workspace, at least doubling it and
+// at most to slab_blocks blocks; the workspaces are then kept for later
+// calls.
+void Compressor::reserve(int blocks) {
+  const int want = std::max(1, std::min(blocks, cfg_.slab_blocks));
+  if (slab_capacity_ >= want) return;
+  const int nb = std::min(cfg_.slab_blocks, std::max(want, 2 * slab_capacity_));
+  slab_capacity_ = 0;  // stays 0 if a (re)allocation fails part way
+  for (auto &w : workers_) w->size_slab(nb, cfg_.max_block_bytes);
+  slab_capacity_ = nb;
 }
 
 Compressor::~Compressor() {
@@ -248,6 +278,17 @@ void Compressor::run(const uint8_t *const *ptrs, const int *lens, int nblocks, i
                      bool on_device, ByteSink &out, StageTimes *times, bool part,
                      int64_t *part_bits, uint32_t *part_crc) {
   std::lock_guard<std::mutex> call_lock(call_mu_);
+  {
+    // room for min(nblocks, slab_blocks) blocks; with an RLE1 cap a block's
+    // raw bytes may exceed max_block_bytes and take the raw room of several
+    int want = nblocks;
+    if (cfg_.m_cap > 0) {
+      const int64_t per = align_up(std::max<int64_t>(cfg_.max_block_bytes, 1), 16);
+      for (int b = 0; b < nblocks; b++)
+        want = (int)std::max<int64_t>(want, (lens[b] + per - 1) / per);
+    }
+    reserve(want);
+  }
   const Workspace &ws0 = *workers_[0]->ws;
   const int64_t raw_max = cfg_.m_cap > 0 ? ws0.max_raw : cfg_.max_block_bytes;
   BZ_REQUIRE(cfg_.m_cap <= rle1_bound(cfg_.max_block_bytes), kErrArg,
@@ -548,6 +589,7 @@ void Compressor::compress_batch(const Item *items, int count, bool on_device, By
                    [&](int a, int b) { return blks[a].len > blks[b].len; });
   // slabs over the queue: a slab takes up to the tuned block count for its
   // longest (first) block, fewer where the workspace's capacities end
+  reserve(nb);
   const Workspace &ws0 = *workers_[0]->ws;
   std::vector<int> slab_at{0};
   {

@@ -43,8 +43,8 @@ struct StageTimes {
 };
 
 struct CompressorConfig {
-  int slab_blocks = 128;
-  int workers = 5;
+  int slab_blocks = 384;
+  int workers = 4;
   int64_t max_block_bytes = 900000;
   bool time_stages = false;
   // Learned table selector: packed weights on this engine's device
@@ -137,10 +137,12 @@ class Compressor {
            uint32_t *part_crc = nullptr);
   uint32_t *arena_take(int64_t words, size_t *chunk, int64_t *used, int64_t *base);
   BatchTune tune_for(int len) const;
+  void reserve(int blocks);
   static constexpr int64_t kArenaChunkWords = int64_t(1) << 28;  // 1 GiB
   CompressorConfig cfg_;
   int device_ = 0;
   std::vector<std::unique_ptr<Worker>> workers_;
+  int slab_capacity_ = 0;                      // blocks the workers' workspaces hold
   std::mutex call_mu_;                         // one call at a time per engine
   std::vector<BatchTune> tune_;               // batched form: slab shapes by block length
   std::vector<uint32_t *> arena_chunks_;       // batched form: block bits

@@ -100,9 +100,15 @@ size_t bz2g_compress_batch_bound(int count, const size_t *sizes, const int *leve
                                  const int *block_bytes);
 
 /* Engine shape used by the whole-stream calls on this thread's device:
- * blocks per slab and worker streams (default 128 and 5; about 6.5 GB of
- * device memory per worker).  0 keeps the current value. */
+ * blocks per slab and worker streams (default 384 and 4).  0 keeps the
+ * current value.  Each worker's workspace takes about 55 MB of device memory
+ * per 900,000-byte block it holds (21 GB at 384 blocks) and is allocated when
+ * a call first needs it: a call of k blocks takes room for min(k,
+ * slab_blocks) blocks per worker, and a later, larger call grows it (at least
+ * doubling, at most to slab_blocks); it is kept until the shape changes.
+ * bz2g_get_engine: the current shape. */
 int bz2g_set_engine(int slab_blocks, int workers);
+int bz2g_get_engine(int *slab_blocks, int *workers);
 /* Batched-form tuning (no counterpart in the reference; the table that
  * bzip2gpu_b200/autotune.py measures and commits): entry i says that a slab
  * whose longest block has at most max_block_len[i] raw bytes takes up to
