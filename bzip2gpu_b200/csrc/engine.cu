@@ -227,6 +227,8 @@ Workspace *Workspace::create_for(int max_blocks, int64_t max_block_bytes, int bl
   const int64_t cap = align_up(std::max<int64_t>(rle1_bound(nb), 1), kTile);
   const int64_t E = (int64_t)max_blocks * cap;
   const int64_t R = (int64_t)max_blocks * align_up(nb, 16);
+  BZ_REQUIRE(E + kTile < (int64_t(1) << 32), kErrArg,
+             "slab too large: its element offsets must fit 32 bits (use fewer slab blocks)");
   const int mt = (int)(E / kTile);
   const int mrt = (int)(max_blocks * ((nb + kRawTile - 1) / kRawTile));
   const int mgt = (int)(max_blocks * ((groups_bound(nb) + kGroupTile - 1) / kGroupTile));

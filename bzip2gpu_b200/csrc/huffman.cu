@@ -161,11 +161,14 @@ __global__ void __launch_bounds__(kGroupTile) k_huff_select(SlabDev d, int which
 }
 
 // bzip2's length-limited Huffman lengths (src/compression/huffman.cu:13-124),
-// one warp per table.  Lane 0 runs the heap: its entries carry their node's
-// weight in the high half (weight << 32 | node), so a sift step reads a
-// sibling pair with one 16-byte shared load; comparisons use the weight half
-// only, with the reference's strict '<', so ties resolve exactly as there.
-// All lanes then walk the parent links for the code lengths.
+// one warp per block: lane t runs table t's heap (a block's tables share
+// its alphabet size, so the lanes' heaps have equal sizes at every step and
+// stay in step), so the warp issues about one heap's instructions for all
+// six.  Heap entries carry their node's weight in the high half (weight << 32
+// | node), so a sift step reads a sibling pair with one 16-byte shared load;
+// comparisons use the weight half only, with the reference's strict '<', so
+// ties resolve exactly as there.  All lanes then walk the parent links for
+// the code lengths, table by table.
 constexpr int kHeapN = kMaxAlpha + 2;
 constexpr int kNodeN = kMaxAlpha * 2;
 
@@ -176,16 +179,13 @@ __device__ __forceinline__ uint32_t hw(uint64_t e) { return (uint32_t)(e >> 32);
 // split == 1 (first build): y = 0 from the counts of the first pass (the
 // MLP's counts for learned blocks), y = 1 from the first plain pass's counts.
 // split == 2 (second build): y = 0 from rfreq, y = 1 from rfreq2.
-__global__ void __launch_bounds__(kMaxGroups * 32) k_huff_lengths(SlabDev d, int which, int round,
-                                                                  int split) {
+__global__ void __launch_bounds__(32) k_huff_lengths(SlabDev d, int which, int round, int split) {
   __shared__ __align__(16) uint64_t heap_s[kMaxGroups][kHeapN + 2];
   __shared__ int32_t leafw_s[kMaxGroups][kMaxAlpha + 1];
   __shared__ int16_t parent_s[kMaxGroups][kNodeN];
   const int b = blockIdx.x;
-  const int t = warp_id();
   const int ln = lane_id();
   const int ngrp = d.n_groups[b];
-  if (t >= ngrp) return;
   const int32_t *rf_base = d.rfreq;
   uint8_t *len_base = d.len;
   if (split) {
@@ -200,18 +200,20 @@ __global__ void __launch_bounds__(kMaxGroups * 32) k_huff_lengths(SlabDev d, int
     return;
   }
   const int alpha = d.n_in_use[b] + 2;
-  uint64_t *heap = heap_s[t];
-  int32_t *leafw = leafw_s[t];
-  int16_t *parent = parent_s[t];
-  const int32_t *freq = rf_base + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
-  uint8_t *len = len_base + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
-  for (int i = ln; i < alpha; i += 32) {
-    int f = freq[i];
-    leafw[i + 1] = (f == 0 ? 1 : f) << 8;
+  for (int t = 0; t < ngrp; t++) {
+    const int32_t *freq = rf_base + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
+    for (int i = ln; i < alpha; i += 32) {
+      const int f = freq[i];
+      leafw_s[t][i + 1] = (f == 0 ? 1 : f) << 8;
+    }
   }
   __syncwarp();
-  for (;;) {
-    if (ln == 0) {
+  unsigned pending = (1u << ngrp) - 1u;  // tables whose lengths are not final yet
+  while (pending) {
+    if ((pending >> ln) & 1u) {
+      uint64_t *heap = heap_s[ln];
+      const int32_t *leafw = leafw_s[ln];
+      int16_t *parent = parent_s[ln];
       int n_nodes = alpha, n_heap = 0;
       heap[0] = 0;  // sentinel: weight 0
       for (int i = 1; i <= alpha; i++) {
@@ -269,23 +271,32 @@ __global__ void __launch_bounds__(kMaxGroups * 32) k_huff_lengths(SlabDev d, int
       }
     }
     __syncwarp();
-    bool too_long = false;
-    for (int i = ln + 1; i <= alpha; i += 32) {
-      int j = 0, k = i;
-      while (parent[k] >= 0) {
-        k = parent[k];
-        j++;
+    unsigned redo = 0;
+    for (int t = 0; t < ngrp; t++) {
+      if (!((pending >> t) & 1u)) continue;
+      const int16_t *parent = parent_s[t];
+      uint8_t *len = len_base + ((size_t)b * kMaxGroups + t) * kMaxAlpha;
+      bool too_long = false;
+      for (int i = ln + 1; i <= alpha; i += 32) {
+        int j = 0, k = i;
+        while (parent[k] >= 0) {
+          k = parent[k];
+          j++;
+        }
+        len[i - 1] = (uint8_t)j;
+        too_long |= j > kMaxCodeLen;
       }
-      len[i - 1] = (uint8_t)j;
-      too_long |= j > kMaxCodeLen;
-    }
-    if (!__any_sync(0xffffffffu, too_long)) break;
-    for (int i = ln + 1; i <= alpha; i += 32) {
-      int j = leafw[i] >> 8;
-      j = 1 + (j / 2);
-      leafw[i] = j << 8;
+      if (__any_sync(0xffffffffu, too_long)) {
+        redo |= 1u << t;
+        for (int i = ln + 1; i <= alpha; i += 32) {
+          int j = leafw_s[t][i] >> 8;
+          j = 1 + (j / 2);
+          leafw_s[t][i] = j << 8;
+        }
+      }
     }
     __syncwarp();
+    pending = redo;
   }
 }
 
@@ -385,7 +396,7 @@ void select_pass(const SlabDev &d, int which, int round, cudaStream_t st) {
   BZ_LAUNCH_CHECK();
 }
 void lengths_pass(const SlabDev &d, int which, int round, cudaStream_t st) {
-  k_huff_lengths<<<d.nblocks, kMaxGroups * 32, 0, st>>>(d, which, round, 0);
+  k_huff_lengths<<<d.nblocks, 32, 0, st>>>(d, which, round, 0);
   BZ_LAUNCH_CHECK();
 }
 }  // namespace
@@ -417,7 +428,7 @@ void stage_huffman(const SlabDev &d, cudaStream_t st, const uint8_t *learned, in
     mlp::launch_select(d, learned, nullptr, nullptr, d.rfreq_m, st);
     if (mlp_sel_out)
       BZ_CUDA(cudaMemcpyAsync(mlp_sel_out, d.sel, mlp_sel_bytes, cudaMemcpyDeviceToDevice, st));
-    k_huff_lengths<<<dim3(d.nblocks, 2), kMaxGroups * 32, 0, st>>>(d, kAll, 0, 1);
+    k_huff_lengths<<<dim3(d.nblocks, 2), 32, 0, st>>>(d, kAll, 0, 1);
     BZ_LAUNCH_CHECK();
     // second passes, side by side: every block over its tables (the plain
     // blocks' second pass, the learned tables' exact pass) and, for learned
@@ -433,7 +444,7 @@ void stage_huffman(const SlabDev &d, cudaStream_t st, const uint8_t *learned, in
         BZ_LAUNCH_CHECK();
       }
     }
-    k_huff_lengths<<<dim3(d.nblocks, 2), kMaxGroups * 32, 0, st>>>(d, kAll, 0, 2);
+    k_huff_lengths<<<dim3(d.nblocks, 2), 32, 0, st>>>(d, kAll, 0, 2);
     BZ_LAUNCH_CHECK();
     k_huff_judge<<<d.nblocks, 32, 0, st>>>(d);
     BZ_LAUNCH_CHECK();
