@@ -68,26 +68,54 @@ __global__ void __launch_bounds__(256) k_mtf_block_scan(SlabDev d) {
   }
 }
 
-// One warp per tile.  The tile's starting list comes from the
-// last-occurrence table.  Lane k owns the 128 symbols [128k, 128k+128): it
-// records their distinct values most recent first (its "partial list"); the
-// warp then derives each lane's starting list in turn (list k = partial k-1
-// followed by list k-1 without those symbols), and every lane runs the
-// sequential move-to-front over its own symbols with its own list.
+// One warp per tile; lane l owns the kSub symbols [kSub*l, kSub*l + kSub)
+// of the tile (its chunk).  Move-to-front is computed from occurrences, not
+// by moving list entries: the index of symbol c at position i is
+//   - if c occurred earlier in the chunk, last at p: the number of distinct
+//     symbols in (p, i), i.e. of chunk positions in (p, i) that are the last
+//     occurrence so far of their symbol (a 128-bit mask L, in registers);
+//   - otherwise: the distinct symbols seen in the chunk so far, plus the
+//     symbols ahead of c in the lane's starting list not seen yet: r - s,
+//     r = c's rank in that list, s = seen symbols of lower rank (a 256-bit
+//     mask S of their ranks, in registers).
+// So each step is a fixed handful of bit operations, whatever the depth of
+// the symbol in the list.  Lane l's starting list, as a rank per symbol,
+// follows from lane l-1's: symbols seen in chunk l-1 come first, most
+// recent first (their recency rank from a backward scan of the chunk), then
+// the others in their previous order.  The tile's starting list (lane 0)
+// comes from the last-occurrence table.
 constexpr int kSub = kTile / 32;      // symbols per lane
-constexpr int kListStride = 264;      // bytes per lane list (8-aligned, bank spread)
+constexpr int kRow = 260;             // bytes per lane row of a per-symbol table (bank spread)
 // The tile in shared memory: lane l's kSub bytes at l * (kSub + 4), so the 32
 // lanes walking their own slices hit 32 different banks.
 constexpr int kSLaneStride = kSub + 4;
 __device__ __forceinline__ int sl_at(int i) { return i + (i / kSub) * 4; }
 
+// Set bits of the 128-bit mask (w0..w3) at positions 0..p.
+__device__ __forceinline__ int popc_upto128(uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3,
+                                            int p) {
+  const int w = p >> 5;
+  const uint32_t m = (2u << (p & 31)) - 1u;
+  const uint32_t ww = w == 0 ? w0 : w == 1 ? w1 : w == 2 ? w2 : w3;
+  return (w > 0 ? __popc(w0) : 0) + (w > 1 ? __popc(w1) : 0) + (w > 2 ? __popc(w2) : 0) +
+         __popc(ww & m);
+}
+
+// Set bits of the 256-bit mask s[0..7] below position r.
+__device__ __forceinline__ int popc_below256(const uint32_t (&s)[8], int r) {
+  const int w = r >> 5;
+  const uint32_t m = (1u << (r & 31)) - 1u;
+  int n = 0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) n += k < w ? __popc(s[k]) : (k == w ? __popc(s[k] & m) : 0);
+  return n;
+}
+
 __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d, const int32_t *list) {
-  // Lane k's list at lists[k]; lane k - 1 writes its partial list straight to
-  // the front of list k, where the chain below wants it (13.5 KB of shared
-  // memory in all: 15 single-warp blocks per SM).
   __shared__ __align__(16) uint8_t sL[32 * kSLaneStride];
-  __shared__ __align__(16) uint8_t lists[32 * kListStride];
-  __shared__ uint32_t pmask[32][9];  // padded row: no bank conflicts across lanes
+  __shared__ __align__(16) uint8_t rk[32 * kRow];   // lane l's starting list: rank of each symbol
+  __shared__ __align__(16) uint8_t tab[32 * kRow];  // per lane: recency ranks, then last positions
+  __shared__ __align__(16) uint8_t mark[256];       // chain: ranks held by seen symbols
   const int t = list ? list[blockIdx.x] : (int)blockIdx.x;
   const int b = d.tile_block[t];
   const int64_t off = d.off[b];
@@ -103,6 +131,7 @@ __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d, const int32_t *list
     pw[w] = d.present[b * 8 + w];
     nuse += __popc(pw[w]);
   }
+  const uint32_t use = (pw[ln >> 2] >> (8 * (ln & 3))) & 0xffu;  // symbols 8 ln .. 8 ln + 7
   const uint4 *src = reinterpret_cast<const uint4 *>(d.last + off + lt);
   for (int w = ln; w < (valid + 15) / 16; w += 32) {
     const uint4 v = src[w];
@@ -112,8 +141,10 @@ __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d, const int32_t *list
     d4[2] = v.z;
     d4[3] = v.w;
   }
-#pragma unroll
-  for (int w = 0; w < 8; w++) pmask[ln][w] = 0;
+  uint32_t *myTw = reinterpret_cast<uint32_t *>(tab + ln * kRow);
+#pragma unroll 8
+  for (int w = 0; w < 64; w++) myTw[w] = ~0u;
+  reinterpret_cast<uint64_t *>(mark)[ln] = 0;
   {
     // Lane 0's list: the in-use symbols by key, largest first, where a
     // symbol's key is its last position before this tile, or -1 - c for a
@@ -127,7 +158,6 @@ __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d, const int32_t *list
       const int4 *k4 = reinterpret_cast<const int4 *>(d.tile_last + (size_t)t * 256) + 2 * ln;
       const int4 lo = k4[0], hi = k4[1];
       const int lp[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
-      const uint32_t use = (pw[ln >> 2] >> (8 * (ln & 3))) & 0xffu;  // symbols 8 ln .. 8 ln + 7
 #pragma unroll
       for (int q = 0; q < 8; q++) {
         const int c = 8 * ln + q;
@@ -163,89 +193,101 @@ __global__ void __launch_bounds__(32) k_mtf_apply(SlabDev d, const int32_t *list
         }
       }
     }
+    // position j of the sorted order (register q of lane j / 8) is rank j
 #pragma unroll
     for (int q = 0; q < 8; q++)
-      if (8 * ln + q < nuse) lists[8 * ln + q] = (uint8_t)(v[q] & 0xffu);
+      if (8 * ln + q < nuse) rk[v[q] & 0xffu] = (uint8_t)(8 * ln + q);
   }
-  // partial lists
   const int a0 = ln * kSub;
   const int a1 = min(valid, a0 + kSub);
   uint8_t *mySL = sL + 4 * ln;  // this lane's slice: mySL[i] for i in [a0, a1)
-  __syncwarp();  // sL and pmask are in place
-  int cnt = 0;  // this lane's partial-list length
-  if (ln < 31) {  // lane 31's partial list starts no list
-    uint8_t *pp = lists + (ln + 1) * kListStride;
-    for (int i = a1 - 1; i >= a0; i--) {
-      const int c = mySL[i];
-      const uint32_t bit = 1u << (c & 31);
-      const uint32_t mw = pmask[ln][c >> 5];
-      if (!(mw & bit)) {
-        pmask[ln][c >> 5] = mw | bit;
-        pp[cnt++] = (uint8_t)c;
-      }
-    }
+  uint8_t *myT = tab + ln * kRow;
+  __syncwarp();  // sL, lane 0's ranks and the cleared tables are in place
+  // recency ranks in this lane's chunk (0 = the symbol occurring last) and
+  // the chunk's distinct symbol count
+  int dist = 0;
+  for (int i = a1 - 1; i >= a0; i--) {
+    const int c = mySL[i];
+    if (myT[c] == 0xffu) myT[c] = (uint8_t)dist++;
   }
   __syncwarp();
-  // lane lists, in turn: list k = partial(k-1) ++ (list k-1 minus
-  // partial(k-1)); partial(k-1) is already at the front of list k
+  // starting lists, lane by lane: rank in list k of symbol c =
+  //   its recency rank in chunk k-1 if seen there, else
+  //   dist(k-1) + its rank r in list k-1 - (seen symbols of rank below r);
+  // the seen ranks are marked in `mark` and counted by a warp scan (lane j
+  // holds ranks 8j .. 8j+7)
   for (int k = 1; k < 32; k++) {
-    const uint8_t *prevl = lists + (k - 1) * kListStride;
-    uint8_t *cur = lists + k * kListStride;
-    const int pc = __shfl_sync(0xffffffffu, cnt, k - 1);
-    uint8_t keepv[8];
-    int nk = 0;
+    const uint8_t *rp = rk + (k - 1) * kRow;
+    const uint8_t *tp = tab + (k - 1) * kRow;
+    uint8_t *rn = rk + k * kRow;
+    const int dk = __shfl_sync(0xffffffffu, dist, k - 1);
+    int rq[8], sq[8];
 #pragma unroll
     for (int q = 0; q < 8; q++) {
-      const int j = ln * 8 + q;
-      uint8_t c = 0;
-      bool keep = false;
-      if (j < nuse) {
-        c = prevl[j];
-        keep = !((pmask[k - 1][c >> 5] >> (c & 31)) & 1u);
-      }
-      keepv[q] = c;
-      nk += keep;
+      const int c = 8 * ln + q;
+      const bool in = (use >> q) & 1u;
+      sq[q] = in ? tp[c] : 0xff;
+      rq[q] = in ? rp[c] : 0;
+      if (in) mark[rq[q]] = sq[q] != 0xff;
     }
-    int inc = warp_incl_sum(nk);
-    int o = pc + inc - nk;
+    __syncwarp();
+    const uint2 mw = reinterpret_cast<const uint2 *>(mark)[ln];
+    const uint32_t bits = (mw.x & 1u) | ((mw.x >> 7) & 2u) | ((mw.x >> 14) & 4u) |
+                          ((mw.x >> 21) & 8u) | ((mw.y & 1u) << 4) | ((mw.y >> 3) & 0x20u) |
+                          ((mw.y >> 10) & 0x40u) | ((mw.y >> 17) & 0x80u);
+    const int cnt = __popc(bits);
+    const int excl = warp_incl_sum(cnt) - cnt;
+    const uint32_t packed = ((uint32_t)excl << 8) | bits;
 #pragma unroll
     for (int q = 0; q < 8; q++) {
-      const int j = ln * 8 + q;
-      if (j < nuse) {
-        const uint8_t c = keepv[q];
-        if (!((pmask[k - 1][c >> 5] >> (c & 31)) & 1u)) cur[o++] = c;
-      }
+      const uint32_t x = __shfl_sync(0xffffffffu, packed, rq[q] >> 3);
+      const int below = (int)(x >> 8) + __popc(x & ((1u << (rq[q] & 7)) - 1u));
+      if ((use >> q) & 1u)
+        rn[8 * ln + q] = (uint8_t)(sq[q] != 0xff ? sq[q] : dk + rq[q] - below);
     }
     __syncwarp();
   }
-  // each lane: sequential move-to-front over its symbols, in place in sL.
-  // The list is handled eight entries at a time: entry 8i+q is byte q of
-  // little-endian word i.  A word without the symbol shifts up one byte (its
-  // top byte carries into the next word); in the word holding it, the bytes
-  // below it shift up and it leaves.
+  // each lane: the move-to-front indices of its chunk, in place in sL;
+  // myT now holds each symbol's last position in the chunk so far
+#pragma unroll 8
+  for (int w = 0; w < 64; w++) myTw[w] = ~0u;
+  __syncwarp();
   {
-    uint64_t *lw = reinterpret_cast<uint64_t *>(lists + ln * kListStride);
-    const uint64_t ones = 0x0101010101010101ull, highs = 0x8080808080808080ull;
-    for (int i = a0; i < a1; i++) {
-      const uint32_t c = mySL[i];
-      const uint64_t bc = ones * c;
-      uint64_t carry = c;
-      int q = 0;
-      for (int wi = 0; wi < 32; wi++) {
-        const uint64_t wv = lw[wi];
-        const uint64_t x = wv ^ bc;
-        const uint64_t z = (x - ones) & ~x & highs;  // lowest set bit marks the first match
-        if (z) {
-          const int j = (__ffsll((long long)z) - 1) >> 3;
-          const uint64_t low = j == 7 ? ~0ull : ((1ull << (8 * (j + 1))) - 1);
-          lw[wi] = (wv & ~low) | (((wv << 8) | carry) & low);
-          q = wi * 8 + j;
-          break;
+    const uint8_t *myR = rk + ln * kRow;
+    uint32_t L0 = 0, L1 = 0, L2 = 0, L3 = 0;  // last occurrences so far, by chunk position
+    uint32_t S[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // starting-list ranks of the symbols seen
+    int dc = 0;                                // distinct symbols seen (set bits of L)
+    const int n = a1 - a0;
+#pragma unroll
+    for (int wq = 0; wq < 4; wq++) {
+      const int e = min(n, 32 * wq + 32);
+      for (int li = 32 * wq; li < e; li++) {
+        const int c = mySL[a0 + li];
+        const int pp = myT[c];
+        myT[c] = (uint8_t)li;
+        int idx;
+        if (pp != 0xff) {
+          idx = dc - popc_upto128(L0, L1, L2, L3, pp);
+          const uint32_t bit = 1u << (pp & 31);
+          const int w = pp >> 5;
+          L0 ^= w == 0 ? bit : 0u;
+          L1 ^= w == 1 ? bit : 0u;
+          L2 ^= w == 2 ? bit : 0u;
+          L3 ^= w == 3 ? bit : 0u;
+        } else {
+          const int r = myR[c];
+          idx = dc + r - popc_below256(S, r);
+#pragma unroll
+          for (int k = 0; k < 8; k++) S[k] |= (r >> 5) == k ? 1u << (r & 31) : 0u;
+          dc++;
         }
-        lw[wi] = (wv << 8) | carry;
-        carry = wv >> 56;
+        const uint32_t me = 1u << (li & 31);
+        if (wq == 0) L0 |= me;
+        if (wq == 1) L1 |= me;
+        if (wq == 2) L2 |= me;
+        if (wq == 3) L3 |= me;
+        mySL[a0 + li] = (uint8_t)idx;
       }
-      mySL[i] = (uint8_t)q;
     }
   }
   __syncwarp();
