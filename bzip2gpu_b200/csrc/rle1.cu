@@ -64,10 +64,55 @@ __device__ __forceinline__ uint32_t tile_bytes(const uint8_t *sb, int p0, int le
   return starts;
 }
 
+// Output bytes of the positions [0, n) of a run (the per-position counts
+// summed: 5 per chunk of `cut`, and 1, 1, 1, 2 for its first four).
+__device__ __forceinline__ int rle1_out_upto(int n, int cut) {
+  const int f = n / cut, r = n - f * cut;
+  return 5 * f + (r < 4 ? r : 5);
+}
+
+// Which of a thread's 16 bytes (bit k: byte k) emit output: positions 0..3
+// of a run chunk emit their byte (e), position 3 also a length byte (e3).
+// sm: the run starts among the bytes; nv: bytes in the tile.  With carry,
+// byte 0 continues a run at position q0 of its chunk; the chunk starts are
+// then the run starts, the carried chunk's start (byte -q0) and, while the
+// carried run lasts, its next chunk start (byte cut - q0; a run beginning
+// among these bytes reaches no chunk end within them, as cut > 16).
+// Without carry the bytes before the first run start emit nothing here.
+// A byte emits when a chunk starts within the 4 bytes up to it; it emits a
+// length too when that start is exactly 3 before it.
+__device__ __forceinline__ void rle1_emit_masks(uint32_t sm, int q0, int nv, int cut, bool carry,
+                                                uint32_t *e, uint32_t *e3) {
+  uint32_t s4 = sm << 4;  // bit k + 4: byte k
+  if (carry) {
+    if (q0 <= 3) {
+      s4 |= 1u << (4 - q0);
+    } else {
+      const int pw = cut - q0;
+      if (pw < kTileItems && (sm & ((1u << pw) - 1u)) == 0) s4 |= 1u << (pw + 4);
+    }
+  }
+  const uint32_t nvm = (1u << nv) - 1u;
+  uint32_t em = ((s4 | (s4 << 1) | (s4 << 2) | (s4 << 3)) >> 4) & nvm;
+  uint32_t em3 = (((s4 << 3) & ~(s4 << 2) & ~(s4 << 1) & ~s4) >> 4) & nvm;
+  if (!carry) {
+    const uint32_t keep = sm ? ~((sm & (0u - sm)) - 1u) : 0u;
+    em &= keep;
+    em3 &= keep;
+  }
+  *e = em;
+  *e3 = em3;
+}
+
+// Per raw tile: its first and last run start, its crc0, and its RLE1 output
+// bytes from its first run start on (the bytes before it continue a run from
+// an earlier tile; the per-block kernel adds their count in closed form).
 __global__ void __launch_bounds__(256) k_rle1_scan_tiles(SlabDev d) {
   __shared__ __align__(16) uint8_t sb[kRawTile + 16];
   __shared__ uint32_t tbl[256];
   __shared__ int red[2][9];
+  __shared__ int scratch[40];
+  __shared__ int wl[8];
   const int t = blockIdx.x;
   int b, st, n, prev;
   crc_table_fill(tbl);
@@ -88,6 +133,25 @@ __global__ void __launch_bounds__(256) k_rle1_scan_tiles(SlabDev d) {
   if (lane_id() == 0) {
     red[0][warp_id()] = first;
     red[1][warp_id()] = last;
+  }
+  {
+    // output bytes: each thread's bytes from the last run start before them
+    // in this tile (positions in the run modulo the cut); bytes before the
+    // tile's first run start are left to the per-block kernel
+    const int nv = min(kTileItems, max(0, len - p0));
+    const int ls = sm ? st + p0 + 31 - __clz(sm) : -1;
+    const int inc = block_incl_max(ls, scratch, -1);
+    int ex = __shfl_up_sync(0xffffffffu, inc, 1);
+    if (lane_id() == 31) wl[warp_id()] = inc;
+    __syncthreads();
+    if (lane_id() == 0) ex = warp_id() == 0 ? -1 : wl[warp_id() - 1];
+    const int cut = d.run_cut;
+    uint32_t em, em3;
+    rle1_emit_masks(sm, ex >= 0 ? (st + p0 - ex) % cut : 0, nv, cut, ex >= 0, &em, &em3);
+    const int cnt = __popc(em) + __popc(em3);
+    int total;
+    block_excl_sum(cnt, scratch, &total);
+    if (threadIdx.x == 0) d.tile_c[t] = total;
   }
 
   // crc0 of the tile, right-aligned into a virtual 4096-byte tile (leading
@@ -137,7 +201,8 @@ __global__ void __launch_bounds__(256) k_rle1_block_carry(SlabDev d, const int *
   const int b = blockIdx.x;
   const int t0 = rt_first[b], nt = rt_first[b + 1] - t0;
   const int n = d.raw_len[b];
-  int carry = -1;
+  int carry = -1, out_carry = 0;
+  const int cut = d.run_cut;
   for (int base = 0; base < nt; base += 256) {
     int k = base + threadIdx.x;
     int v = k < nt ? d.tile_b[t0 + k] : -1;
@@ -145,11 +210,27 @@ __global__ void __launch_bounds__(256) k_rle1_block_carry(SlabDev d, const int *
     sx[threadIdx.x] = inc;
     __syncthreads();
     int ex = threadIdx.x == 0 ? carry : max(carry, sx[threadIdx.x - 1]);
-    if (k < nt) d.tile_b[t0 + k] = ex;
+    int cnt = 0;
+    if (k < nt) {
+      d.tile_b[t0 + k] = ex;
+      // the tile's output: its own count plus that of its bytes before its
+      // first run start, positions j0 .. j0 + pre - 1 of the run begun at ex
+      const int st = d.rt_start[t0 + k];
+      const int len = min(kRawTile, n - st);
+      const int fs = d.tile_a[t0 + k];
+      const int pre = (fs == INT32_MAX ? st + len : fs) - st;
+      const int j0 = st - ex;
+      cnt = d.tile_c[t0 + k] + (pre > 0 ? rle1_out_upto(j0 + pre, cut) - rle1_out_upto(j0, cut) : 0);
+    }
     int c2 = max(carry, sx[255]);
     __syncthreads();
     carry = c2;
+    int tot;
+    const int o = block_excl_sum(cnt, scratch, &tot);
+    if (k < nt) d.tile_c[t0 + k] = out_carry + o;
+    out_carry += tot;
   }
+  if (threadIdx.x == 0) d.m[b] = out_carry;
   int carry_min = n;
   // walk backwards for the suffix minimum
   for (int base = ((nt - 1) / 256) * 256; base >= 0; base -= 256) {
@@ -180,57 +261,6 @@ __global__ void __launch_bounds__(256) k_rle1_block_carry(SlabDev d, const int *
     for (int w = 0; w < (int)(blockDim.x >> 5); w++) a ^= (uint32_t)scratch[w];
     d.crc[b] = ~(gf_mul(0xFFFFFFFFu, xpow8((uint64_t)n)) ^ a);
   }
-}
-
-__global__ void __launch_bounds__(256) k_rle1_count(SlabDev d) {
-  __shared__ __align__(16) uint8_t sb[kRawTile + 16];
-  __shared__ int scratch[40];
-  const int t = blockIdx.x;
-  int b, st, n, prev;
-  int len = load_raw_tile(d, t, sb, &b, &st, &n, &prev);
-  __syncthreads();
-  const int p0 = threadIdx.x * kTileItems;
-  uint8_t c[kTileItems];
-  const uint32_t sm = tile_bytes(sb, p0, len, prev, c);
-  const int nv = min(kTileItems, max(0, len - p0));  // bytes of this thread in the tile
-  int ls = sm ? st + p0 + 31 - __clz(sm) : -1;
-  int inc = block_incl_max(ls, scratch, -1);
-  // exclusive: max over earlier threads, with the tile carry
-  int ex = __shfl_up_sync(0xffffffffu, inc, 1);
-  __shared__ int wl[8];
-  if (lane_id() == 31) wl[warp_id()] = inc;
-  __syncthreads();
-  if (lane_id() == 0) ex = warp_id() == 0 ? -1 : wl[warp_id() - 1];
-  int cur = max(ex, d.tile_b[t]);
-  // position of each byte in its run, modulo the cut, tracked incrementally
-  const int cut = d.run_cut;
-  int q = nv > 0 ? (st + p0 - cur) % cut : 0;
-  int cnt = 0;
-  for (int k = 0; k < nv; k++) {
-    if ((sm >> k) & 1u) q = 0;
-    cnt += q < 3 ? 1 : (q == 3 ? 2 : 0);
-    if (++q == cut) q = 0;
-  }
-  int total;
-  block_excl_sum(cnt, scratch, &total);
-  if (threadIdx.x == 0) d.tile_c[t] = total;
-}
-
-// Per block: exclusive sum of tile output counts; m[b] = RLE1 length.
-__global__ void __launch_bounds__(256) k_rle1_block_offsets(SlabDev d, const int *rt_first) {
-  __shared__ int scratch[40];
-  const int b = blockIdx.x;
-  const int t0 = rt_first[b], nt = rt_first[b + 1] - t0;
-  int carry = 0;
-  for (int base = 0; base < nt; base += 256) {
-    int k = base + threadIdx.x;
-    int v = k < nt ? d.tile_c[t0 + k] : 0;
-    int tot;
-    int ex = block_excl_sum(v, scratch, &tot);
-    if (k < nt) d.tile_c[t0 + k] = carry + ex;
-    carry += tot;
-  }
-  if (threadIdx.x == 0) d.m[b] = carry;
 }
 
 __global__ void __launch_bounds__(256) k_rle1_write(SlabDev d) {
@@ -264,56 +294,28 @@ __global__ void __launch_bounds__(256) k_rle1_write(SlabDev d) {
   before = max(before, d.tile_b[t]);
   after = min(after, d.tile_a[t]);  // next start after the tile (or n)
 
-  int ends[kTileItems];
-  {
-    int cur = after;
-#pragma unroll
-    for (int k = kTileItems - 1; k >= 0; k--) {
-      ends[k] = cur;
-      if ((sm >> k) & 1u) cur = st + p0 + k;
-    }
-  }
-  // each byte's position in its run as (chunk, position in the chunk of
-  // `cut` bytes), tracked incrementally from one division per thread
+  // each byte's emits: its position in its chunk from the run start before
+  // the thread (one division per thread), then bit masks
   const int cut = d.run_cut;
-  int q0 = 0, jd0 = 0;
-  if (nv > 0) {
-    const int j0 = st + p0 - before;
-    jd0 = j0 / cut;
-    q0 = j0 - jd0 * cut;
-  }
-  int cnt = 0;
-  {
-    int q = q0;
-    for (int k = 0; k < nv; k++) {
-      if ((sm >> k) & 1u) q = 0;
-      cnt += q < 3 ? 1 : (q == 3 ? 2 : 0);
-      if (++q == cut) q = 0;
-    }
-  }
+  const int pbase = st + p0;  // block-local position of byte 0
+  uint32_t em = 0, em3 = 0;
+  if (nv > 0)
+    rle1_emit_masks(sm, before >= 0 ? (pbase - before) % cut : 0, nv, cut, before >= 0, &em, &em3);
   int tot;
-  int o = block_excl_sum(cnt, scratch, &tot);
+  const int o = block_excl_sum(__popc(em) + __popc(em3), scratch, &tot);
   uint8_t *out = so + o;
-  int cur = before, q = q0, jd = jd0;
 #pragma unroll
   for (int k = 0; k < kTileItems; k++) {
-    if (k < nv) {
-      if ((sm >> k) & 1u) {
-        cur = st + p0 + k;
-        q = 0;
-        jd = 0;
-      }
-      if (q < 3) {
-        *out++ = c[k];
-      } else if (q == 3) {
-        const int run_len = ends[k] - cur;
-        const int chunk_len = min(cut, run_len - jd * cut);
-        *out++ = c[k];
-        *out++ = (uint8_t)(chunk_len - 4);
-      }
-      if (++q == cut) {
-        q = 0;
-        jd++;
+    if ((em >> k) & 1u) {
+      const uint32_t below = (1u << k) - 1u;
+      const int at = __popc(em & below) + __popc(em3 & below);
+      out[at] = c[k];
+      if ((em3 >> k) & 1u) {
+        // the chunk's length: from its start (3 bytes back) to the run's end
+        // or the cut, whichever comes first
+        const uint32_t rest = k + 1 < kTileItems ? sm >> (k + 1) : 0u;
+        const int run_end = rest ? pbase + k + __ffs(rest) : after;
+        out[at + 1] = (uint8_t)(min(cut, run_end - (pbase + k - 3)) - 4);
       }
     }
   }
@@ -332,12 +334,6 @@ void stage_rle1_crc(const SlabDev &d, cudaStream_t st) {
     BZ_LAUNCH_CHECK();
   }
   k_rle1_block_carry<<<d.nblocks, 256, 0, st>>>(d, rt_first);
-  BZ_LAUNCH_CHECK();
-  if (d.n_raw_tiles > 0) {
-    k_rle1_count<<<d.n_raw_tiles, 256, 0, st>>>(d);
-    BZ_LAUNCH_CHECK();
-  }
-  k_rle1_block_offsets<<<d.nblocks, 256, 0, st>>>(d, rt_first);
   BZ_LAUNCH_CHECK();
   if (d.n_raw_tiles > 0) {
     k_rle1_write<<<d.n_raw_tiles, 256, 0, st>>>(d);
