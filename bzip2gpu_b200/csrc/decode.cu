@@ -835,9 +835,11 @@ __global__ void __launch_bounds__(32 * kUnrleWarps)
 __global__ void __launch_bounds__(256) k_dec_crc(const int64_t *lens, const int64_t *off,
                                                  const uint8_t *out, uint32_t *crcs) {
   __shared__ uint32_t tbl[256];
+  __shared__ uint32_t red4[16];
   __shared__ __align__(16) uint8_t chunk[4096];
   __shared__ uint32_t part[2][8];
   crc_table_fill(tbl);
+  red4_fill(red4);
   const int k = blockIdx.x;
   const int64_t n = lens[k];
   const uint8_t *src = out + off[k];
@@ -854,7 +856,7 @@ __global__ void __launch_bounds__(256) k_dec_crc(const int64_t *lens, const int6
     const uint32_t w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
     for (int q = 0; q < 16; q++) r = crc_byte(r, (w[q >> 2] >> (8 * (q & 3))) & 0xFFu, tbl);
-    r = r ? gf_mul(r, c_klane.v[threadIdx.x]) : 0u;
+    r = gf_mul_lane(r, threadIdx.x, red4);
     for (int o = 16; o; o >>= 1) r ^= __shfl_xor_sync(0xffffffffu, r, o);
     if ((threadIdx.x & 31) == 0) part[it & 1][threadIdx.x >> 5] = r;
     __syncthreads();

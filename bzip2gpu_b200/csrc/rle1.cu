@@ -110,12 +110,14 @@ __device__ __forceinline__ void rle1_emit_masks(uint32_t sm, int q0, int nv, int
 __global__ void __launch_bounds__(256) k_rle1_scan_tiles(SlabDev d) {
   __shared__ __align__(16) uint8_t sb[kRawTile + 16];
   __shared__ uint32_t tbl[256];
+  __shared__ uint32_t red4[16];
   __shared__ int red[2][9];
   __shared__ int scratch[40];
   __shared__ int wl[8];
   const int t = blockIdx.x;
   int b, st, n, prev;
   crc_table_fill(tbl);
+  red4_fill(red4);
   int len = load_raw_tile(d, t, sb, &b, &st, &n, &prev);
   __syncthreads();
 
@@ -171,7 +173,7 @@ __global__ void __launch_bounds__(256) k_rle1_scan_tiles(SlabDev d) {
         r = (r << 8) ^ tbl[(r >> 24) ^ byte];
       }
     }
-    r = r ? gf_mul(r, c_klane.v[threadIdx.x]) : 0u;
+    r = gf_mul_lane(r, threadIdx.x, red4);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) r ^= __shfl_xor_sync(0xffffffffu, r, o);
     if (lane_id() == 0) wcrc[warp_id()] = r;
