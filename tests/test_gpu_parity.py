@@ -26,10 +26,30 @@ def test_rle1_reference_vectors(torch_cuda, R):
     assert np.array_equal(got, oracle.rle1(a))
 
 
+def _runs(seed, n, max_run, alphabet):
+    rng = np.random.default_rng(seed)
+    parts, tot = [], 0
+    while tot < n:
+        k = int(rng.integers(1, max_run + 1))
+        parts.append(np.full(k, rng.integers(0, alphabet), np.uint8))
+        tot += k
+    return np.concatenate(parts)[:n]
+
+
 @pytest.mark.parametrize("case", ["one", "four", "259", "260", "263", "518", "long", "alt",
-                                  "tile_edge", "markov"])
+                                  "tile_edge", "markov", "runs_random", "runs_span_tiles",
+                                  "runs_at_thread_edges"])
 def test_rle1_edges(torch_cuda, case):
     a = {
+        # random runs of 1..700 bytes over 6 symbols: runs start and end at
+        # every offset of a thread's 16 bytes and of a 4096-byte tile
+        "runs_random": _runs(21, 600000, 700, 6),
+        # runs of 1..20000: chunk ends and carried runs across several tiles
+        "runs_span_tiles": _runs(22, 900000, 20000, 3),
+        # run boundaries on 16-byte thread spans and 4096-byte tiles
+        "runs_at_thread_edges": np.concatenate(
+            [np.full(k, i % 2, np.uint8) for i, k in
+             enumerate([16, 4096, 4080, 16, 259 * 16, 4, 3, 4097, 255, 260, 12288, 1, 15, 17])]),
         "one": np.array([5], np.uint8),
         "four": np.full(4, 9, np.uint8),
         "259": np.full(259, 1, np.uint8),
@@ -98,6 +118,25 @@ def test_mtf_reference_vectors(torch_cuda, A):
     assert (op, nu) == (op2, nu2) and np.array_equal(pres, pres2)
 
 
+@pytest.mark.parametrize("case", ["uniform256", "sparse3", "one_symbol", "skewed", "partial_tile"])
+def test_mtf_symbol_patterns(torch_cuda, case):
+    # the occurrence-based move-to-front: first-seen and repeated symbols in
+    # every lane of a tile, alphabets of 1 to 256 symbols, a short last tile
+    rng = np.random.default_rng(31)
+    a = {
+        "uniform256": rng.integers(0, 256, 70000).astype(np.uint8),
+        "sparse3": np.array([0, 127, 255], np.uint8)[rng.integers(0, 3, 50000)],
+        "one_symbol": np.full(9000, 77, np.uint8),
+        "skewed": np.minimum(rng.geometric(0.2, 80000), 255).astype(np.uint8),
+        "partial_tile": rng.integers(0, 200, 4096 * 3 + 129).astype(np.uint8),
+    }[case]
+    sa = rng.permutation(a.size).astype(np.int32)
+    got, op, pres, nu = B.mtf(dev(torch_cuda, a), dev(torch_cuda, sa))
+    ref, op2, pres2, nu2 = oracle.mtf(a, sa)
+    assert np.array_equal(got.cpu().numpy(), ref)
+    assert (op, nu) == (op2, nu2) and np.array_equal(pres, pres2)
+
+
 def test_mtf_real_sa_and_symbols_table(torch_cuda):
     r1 = oracle.rle1(W.small_markov(900000, seed=5))
     sa = oracle.bwt(r1)
@@ -118,9 +157,20 @@ def test_symbols_table_reference_vector(torch_cuda):
 
 # ------------------------------------------------------------------- RLE2
 @pytest.mark.parametrize("case", ["R20", "R10000", "incompressible", "zeros", "single_zero",
-                                  "one_nonzero", "tile_runs"])
+                                  "one_nonzero", "tile_runs", "zero_runs_random",
+                                  "zero_runs_span_tiles", "leading_trailing_zeros"])
 def test_rle2(torch_cuda, case):
+    rng = np.random.default_rng(23)
+    zr = np.where(rng.random(400000) < 0.7, 0, rng.integers(1, 40, 400000)).astype(np.uint8)
     a = {
+        # zero runs of every length up to a few dozen, at every tile offset
+        "zero_runs_random": zr,
+        # zero runs of up to 20000 across several tiles
+        "zero_runs_span_tiles": np.where(_runs(24, 500000, 20000, 3) == 0, 0,
+                                         rng.integers(1, 9, 500000)).astype(np.uint8),
+        # zeros before the first and after the last non-zero, tiles without one
+        "leading_trailing_zeros": np.concatenate(
+            [np.zeros(9000), [3], np.zeros(5), [1, 2], np.zeros(12289)]).astype(np.uint8),
         "R20": C.ref_rle2_input(20),
         "R10000": C.ref_rle2_input(10000),
         "incompressible": C.ref_rle2_incompressible(),
