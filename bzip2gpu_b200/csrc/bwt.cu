@@ -123,7 +123,8 @@ __global__ void __launch_bounds__(256) k_radix_hist(SlabDev d, int shift, const 
   d.tile_hist[(size_t)t * kRadix + threadIdx.x] = cnt[threadIdx.x];
 }
 
-// Per block: turn tile digit counts into global scatter bases.
+// Per block: turn tile digit counts into each tile's count of the digit in
+// the block's earlier tiles (one pass), and the digit's base in the block.
 // force != 0 (the generating pass): the pass runs even if every tile holds one
 // digit only, since it writes the items the later passes read.
 __global__ void __launch_bounds__(256) k_radix_scan(SlabDev d, int force) {
@@ -148,19 +149,13 @@ __global__ void __launch_bounds__(256) k_radix_scan(SlabDev d, int force) {
       run += h[j];
     }
   }
+  // the digit's base in the block (exclusive sum over digits of the block's
+  // counts), added by the scatter to each tile's count before it
   uint32_t tot;
   uint32_t base = block_excl_sum(run, scratch, &tot);
   int trivial = __syncthreads_or(run == (uint32_t)len);
   if ((!trivial || force) && threadIdx.x == 0) atomicOr(&d.sort_ctl[1], 1);
-  const uint32_t add = (uint32_t)d.off[b] + base;
-  for (int k0 = 0; k0 < nt; k0 += kU) {
-    uint32_t h[kU];
-#pragma unroll
-    for (int j = 0; j < kU; j++) h[j] = k0 + j < nt ? H[(size_t)(k0 + j) * kRadix] : 0u;
-#pragma unroll
-    for (int j = 0; j < kU; j++)
-      if (k0 + j < nt) H[(size_t)(k0 + j) * kRadix] = h[j] + add;
-  }
+  d.sort_base[(size_t)b * kRadix + dg] = (uint32_t)d.off[b] + base;
 }
 
 // Stable scatter of one tile by one 8-bit digit.  Elements are warp-striped
@@ -208,7 +203,8 @@ __global__ void __launch_bounds__(256, kVals ? 2 : 3)
     }
   }
   for (int i = threadIdx.x; i < kSortWarps * kRadix; i += blockDim.x) wcnt[i] = 0;
-  goff[threadIdx.x] = d.tile_hist[(size_t)t * kRadix + threadIdx.x];
+  goff[threadIdx.x] = d.tile_hist[(size_t)t * kRadix + threadIdx.x] +
+                     d.sort_base[(size_t)b * kRadix + threadIdx.x];
   __syncthreads();
 
   uint32_t rank2[kTileItems / 2];  // two 16-bit ranks per register (ranks < 512)

@@ -160,6 +160,7 @@ Workspace::Workspace(int mb, int64_t mr, int64_t me, int mt, int mrt, int mgt)
     dev.pay_bits = (int64_t *)alloc(B * 8);
     dev.blk_start = (int64_t *)alloc(B * 8);
     dev.sort_ctl = (int32_t *)alloc(64);
+    dev.sort_base = (uint32_t *)alloc(B * 256 * 4);
     dev.stream = (uint64_t *)alloc(64);
     dev.kt_elems = (uint64_t *)alloc(8 * kMaxTimedLaunches);
     // plan arrays: 3 int64 per block + ints

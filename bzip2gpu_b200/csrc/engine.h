@@ -69,6 +69,7 @@ struct SlabDev {
   // per-tile scratch
   int32_t *tile_a, *tile_b, *tile_c, *tile_d;  // [ntiles] or [n_raw_tiles]
   uint32_t *tile_hist;                 // [ntiles * 256]
+  uint32_t *sort_base;                 // [nblocks * 256]: radix sort digit bases
   int32_t *tile_last;                  // [ntiles * 256]
   uint32_t *gt_bits;                   // [n_group_tiles]
   uint32_t *grp_bits;                  // per group, at sel layout
