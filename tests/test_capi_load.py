@@ -52,3 +52,42 @@ def test_cli_help_runs_without_gpu():
     cli = B.lib_path().parent / "bzip2gpu"
     r = subprocess.run([str(cli), "-h"], capture_output=True, text=True)
     assert r.returncode == 0 and "--best" in r.stdout
+
+
+def test_engine_shape_host_logic():
+    # bz2g_set_engine / bz2g_get_engine only touch host state (no CUDA call)
+    shape = B.get_engine()
+    assert shape == (384, 4)
+    try:
+        B.set_engine(16, 2)
+        assert B.get_engine() == (16, 2)
+        B.set_engine(0, 3)  # 0 keeps the current value
+        assert B.get_engine() == (16, 3)
+        B.set_engine(32, 0)
+        assert B.get_engine() == (32, 3)
+        try:
+            B.set_engine(-1, 1)
+        except Exception:
+            pass
+        else:
+            raise AssertionError("a negative engine shape was accepted")
+        assert B.get_engine() == (32, 3)
+    finally:
+        B.set_engine(*shape)
+    assert B.get_engine() == shape
+
+
+def test_batch_tuning_table_validation():
+    # the committed table is well formed and accepted; bad entries are refused
+    import json
+    table = json.loads(B.TUNING_FILE.read_text())["table"]
+    assert [t["max_block_len"] for t in table] == sorted(t["max_block_len"] for t in table)
+    assert all(t["slab_blocks"] > 0 and t["workers"] > 0 for t in table)
+    B.set_batch_tuning(table)
+    try:
+        B.set_batch_tuning([{"max_block_len": 900000, "slab_blocks": 0, "workers": 4}])
+    except Exception:
+        pass
+    else:
+        raise AssertionError("a zero slab size was accepted")
+    B.set_batch_tuning(table)  # the committed table stays in force
