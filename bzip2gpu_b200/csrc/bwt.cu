@@ -31,12 +31,20 @@ namespace bz2g {
 
 namespace {
 
-constexpr int kRadixBits = 8;
-constexpr int kRadix = 1 << kRadixBits;
 constexpr int kSortWarps = kTileThreads / 32;  // 8
 constexpr int kWarpSpan = kTile / kSortWarps;   // elements per warp in a tile (512)
-constexpr size_t kScatterSmem =
-    (size_t)kTile * 8 + (size_t)kTile * 4 + (size_t)kSortWarps * kRadix * 4 + 2 * kRadix * 4;
+// Digits of the doubling rounds' sorts may be 9 or 10 bits wide (fewer
+// passes over the 2kb key bits); the tile and block digit tables (tile_hist,
+// sort_base) are sized for kMaxRadix digits.  Shared memory of the scatter: the tile's
+// keys (and values), per-warp digit counts, two digit tables.
+template <int RB>
+constexpr size_t scatter_smem_keys() {
+  return (size_t)kTile * 8 + (size_t)kSortWarps * (1 << RB) * 4 + 2 * (1 << RB) * 4;
+}
+template <int RB>
+constexpr size_t scatter_smem_vals() {
+  return scatter_smem_keys<RB>() + (size_t)kTile * 4;
+}
 
 // How a sorted element is stored: packed (one item: key << low | rotation)
 // or as separate keys[] and vals[].
@@ -65,12 +73,13 @@ __device__ __forceinline__ int tile_valid(const SlabDev &d, int t, const int32_t
   return v < 0 ? 0 : (v > kTile ? kTile : v);
 }
 
-// The valid lanes of the warp whose 8-bit digit equals this lane's: one
+// The valid lanes of the warp whose RB-bit digit equals this lane's: one
 // ballot per digit bit (cheaper here than __match_any_sync).
+template <int RB>
 __device__ __forceinline__ unsigned digit_peers(int dg, bool ok) {
   unsigned peers = __ballot_sync(0xffffffffu, ok);
 #pragma unroll
-  for (int bit = 0; bit < kRadixBits; bit++) {
+  for (int bit = 0; bit < RB; bit++) {
     const bool on = (dg >> bit) & 1;
     const unsigned bb = __ballot_sync(0xffffffffu, on);
     peers &= on ? bb : ~bb;
@@ -93,15 +102,18 @@ __device__ __forceinline__ uint64_t text_item(const uint8_t *T, int m, int i) {
   return ((uint64_t)k << 32) | (uint32_t)i;
 }
 
-// gen != 0: the generating first pass (items from the text, see text_item).
+// gen != 0: the generating first pass (items from the text, see text_item;
+// 8-bit digits).  RB: digit width, tile_hist holds 2^RB counts per tile.
+template <int RB>
 __global__ void __launch_bounds__(256) k_radix_hist(SlabDev d, int shift, const int32_t *list,
                                                     int gen) {
-  __shared__ uint32_t cnt[kRadix];
+  constexpr int kN = 1 << RB;
+  __shared__ uint32_t cnt[kN];
   const int t = tile_id(list);
   int b, lt;
   int valid = tile_valid(d, t, d.sort_len, &b, &lt);
   if (valid == 0) return;
-  cnt[threadIdx.x] = 0;
+  for (int i = threadIdx.x; i < kN; i += blockDim.x) cnt[i] = 0;
   __syncthreads();
   const uint64_t *K = d.keys[d.sort_ctl[0]] + d.off[b] + lt;
   const uint8_t *T = d.rle1 + d.off[b];
@@ -117,45 +129,63 @@ __global__ void __launch_bounds__(256) k_radix_hist(SlabDev d, int shift, const 
     }
   } else {
     for (int e = threadIdx.x; e < valid; e += blockDim.x)
-      atomicAdd(&cnt[(uint32_t)(K[e] >> shift) & (kRadix - 1)], 1u);
+      atomicAdd(&cnt[(uint32_t)(K[e] >> shift) & (kN - 1)], 1u);
   }
   __syncthreads();
-  d.tile_hist[(size_t)t * kRadix + threadIdx.x] = cnt[threadIdx.x];
+  for (int i = threadIdx.x; i < kN; i += blockDim.x) d.tile_hist[(size_t)t * kN + i] = cnt[i];
 }
 
 // Per block: turn tile digit counts into each tile's count of the digit in
 // the block's earlier tiles (one pass), and the digit's base in the block.
 // force != 0 (the generating pass): the pass runs even if every tile holds one
 // digit only, since it writes the items the later passes read.
+// Thread i handles the kD = 2^RB / 256 consecutive digits kD*i .. kD*i+kD-1.
+template <int RB>
 __global__ void __launch_bounds__(256) k_radix_scan(SlabDev d, int force) {
+  constexpr int kN = 1 << RB, kD = kN / 256;
   __shared__ uint32_t scratch[40];
   const int b = blockIdx.x;
   const int len = d.sort_len[b];
   if (len <= 0) return;
   const int nt = (len + kTile - 1) / kTile;
   const int t0 = (int)(d.off[b] / kTile);
-  const int dg = threadIdx.x;
-  uint32_t *H = d.tile_hist + (size_t)t0 * kRadix + dg;
+  uint32_t *H = d.tile_hist + (size_t)t0 * kN + kD * threadIdx.x;
   // eight tiles' counts in flight at a time (the loads are independent)
   constexpr int kU = 8;
-  uint32_t run = 0;
+  uint32_t run[kD];
+#pragma unroll
+  for (int q = 0; q < kD; q++) run[q] = 0;
   for (int k0 = 0; k0 < nt; k0 += kU) {
-    uint32_t h[kU];
 #pragma unroll
-    for (int j = 0; j < kU; j++) h[j] = k0 + j < nt ? H[(size_t)(k0 + j) * kRadix] : 0u;
+    for (int q = 0; q < kD; q++) {
+      uint32_t h[kU];
 #pragma unroll
-    for (int j = 0; j < kU; j++) {
-      if (k0 + j < nt) H[(size_t)(k0 + j) * kRadix] = run;
-      run += h[j];
+      for (int j = 0; j < kU; j++) h[j] = k0 + j < nt ? H[(size_t)(k0 + j) * kN + q] : 0u;
+#pragma unroll
+      for (int j = 0; j < kU; j++) {
+        if (k0 + j < nt) H[(size_t)(k0 + j) * kN + q] = run[q];
+        run[q] += h[j];
+      }
     }
   }
   // the digit's base in the block (exclusive sum over digits of the block's
   // counts), added by the scatter to each tile's count before it
+  uint32_t sum = 0;
+  bool one = false;
+#pragma unroll
+  for (int q = 0; q < kD; q++) {
+    sum += run[q];
+    one |= run[q] == (uint32_t)len;
+  }
   uint32_t tot;
-  uint32_t base = block_excl_sum(run, scratch, &tot);
-  int trivial = __syncthreads_or(run == (uint32_t)len);
+  uint32_t base = block_excl_sum(sum, scratch, &tot);
+  int trivial = __syncthreads_or(one);
   if ((!trivial || force) && threadIdx.x == 0) atomicOr(&d.sort_ctl[1], 1);
-  d.sort_base[(size_t)b * kRadix + dg] = (uint32_t)d.off[b] + base;
+#pragma unroll
+  for (int q = 0; q < kD; q++) {
+    d.sort_base[(size_t)b * kN + kD * threadIdx.x + q] = (uint32_t)d.off[b] + base;
+    base += run[q];
+  }
 }
 
 // Stable scatter of one tile by one 8-bit digit.  Elements are warp-striped
@@ -163,9 +193,10 @@ __global__ void __launch_bounds__(256) k_radix_scan(SlabDev d, int force) {
 // over the lanes with equal digits keeps the original order; the tile is sorted locally
 // in shared memory, then written so that equal digits go out contiguously.
 // All of a thread's loads are issued before the ranking starts.
-template <bool kVals>
+template <bool kVals, int RB>
 __global__ void __launch_bounds__(256, kVals ? 2 : 3)
     k_radix_scatter(SlabDev d, int shift, int timed, const int32_t *list, int gen) {
+  constexpr int kN = 1 << RB, kD = kN / 256;
   if (!d.sort_ctl[1]) return;
   const int t = tile_id(list);
   int b, lt;
@@ -177,8 +208,7 @@ __global__ void __launch_bounds__(256, kVals ? 2 : 3)
   uint64_t *sk = reinterpret_cast<uint64_t *>(smem);
   uint32_t *sv = reinterpret_cast<uint32_t *>(sk + kTile);
   uint32_t *wcnt = kVals ? sv + kTile : reinterpret_cast<uint32_t *>(sk + kTile);  // [warp][digit]
-  uint32_t *lbase = wcnt + kSortWarps * kRadix;  // local digit base
-  uint32_t *goff = lbase + kRadix;               // global digit base for this tile
+  uint32_t *goff = wcnt + kSortWarps * kN + kN;  // global digit base for this tile
   const int cur = d.sort_ctl[0];
   const uint64_t *K = d.keys[cur] + d.off[b] + lt;
   const uint32_t *V = d.vals[cur] + d.off[b] + lt;
@@ -202,9 +232,9 @@ __global__ void __launch_bounds__(256, kVals ? 2 : 3)
       if (kVals) val[i] = e < valid ? V[e] : 0;
     }
   }
-  for (int i = threadIdx.x; i < kSortWarps * kRadix; i += blockDim.x) wcnt[i] = 0;
-  goff[threadIdx.x] = d.tile_hist[(size_t)t * kRadix + threadIdx.x] +
-                     d.sort_base[(size_t)b * kRadix + threadIdx.x];
+#pragma unroll
+  for (int q = 0; q < kSortWarps * kD; q++) wcnt[q * 256 + threadIdx.x] = 0;
+
   __syncthreads();
 
   uint32_t rank2[kTileItems / 2];  // two 16-bit ranks per register (ranks < 512)
@@ -213,16 +243,16 @@ __global__ void __launch_bounds__(256, kVals ? 2 : 3)
   for (int i = 0; i < kTileItems; i++) {
     const int e = w * kWarpSpan + i * 32 + ln;
     const bool ok = e < valid;
-    const int dg = ok ? (int)((key[i] >> shift) & (kRadix - 1)) : 0;
-    const unsigned peers = digit_peers(dg, ok);
-    const uint32_t before = ok ? wcnt[w * kRadix + dg] : 0;
+    const int dg = ok ? (int)((key[i] >> shift) & (kN - 1)) : 0;
+    const unsigned peers = digit_peers<RB>(dg, ok);
+    const uint32_t before = ok ? wcnt[w * kN + dg] : 0;
     const uint32_t r = before + __popc(peers & lt_mask);
     if (i & 1)
       rank2[i >> 1] |= r << 16;
     else
       rank2[i >> 1] = r;
     __syncwarp();
-    if (ok && (peers & lt_mask) == 0) wcnt[w * kRadix + dg] = before + __popc(peers);
+    if (ok && (peers & lt_mask) == 0) wcnt[w * kN + dg] = before + __popc(peers);
     __syncwarp();
   }
   __syncthreads();
@@ -231,28 +261,53 @@ __global__ void __launch_bounds__(256, kVals ? 2 : 3)
     // counts); each warp's count becomes that warp's local start for the
     // digit, and the digit's global base becomes (global - local) base, so
     // the placement and the write below read one table entry each
-    const int dg = threadIdx.x;
-    uint32_t run = 0;
-    for (int ww = 0; ww < kSortWarps; ww++) run += wcnt[ww * kRadix + dg];
     __shared__ uint32_t scratch[40];
     uint32_t tot;
-    const uint32_t lb = block_excl_sum(run, scratch, &tot);
-    uint32_t at = lb;
-    for (int ww = 0; ww < kSortWarps; ww++) {
-      const uint32_t c = wcnt[ww * kRadix + dg];
-      wcnt[ww * kRadix + dg] = at;
-      at += c;
+    if constexpr (kD == 1) {
+      const int dg = threadIdx.x;
+      uint32_t run = 0;
+      for (int ww = 0; ww < kSortWarps; ww++) run += wcnt[ww * kN + dg];
+      const uint32_t lb = block_excl_sum(run, scratch, &tot);
+      uint32_t at = lb;
+      for (int ww = 0; ww < kSortWarps; ww++) {
+        const uint32_t c = wcnt[ww * kN + dg];
+        wcnt[ww * kN + dg] = at;
+        at += c;
+      }
+      goff[dg] = d.tile_hist[(size_t)t * kN + dg] + d.sort_base[(size_t)b * kN + dg] - lb;
+    } else {
+      // thread i: the kD consecutive digits kD*i ..
+      uint32_t run[kD], sum = 0;
+#pragma unroll
+      for (int q = 0; q < kD; q++) {
+        const int dg = kD * threadIdx.x + q;
+        run[q] = 0;
+        for (int ww = 0; ww < kSortWarps; ww++) run[q] += wcnt[ww * kN + dg];
+        sum += run[q];
+      }
+      uint32_t lb = block_excl_sum(sum, scratch, &tot);
+#pragma unroll
+      for (int q = 0; q < kD; q++) {
+        const int dg = kD * threadIdx.x + q;
+        uint32_t at = lb;
+        for (int ww = 0; ww < kSortWarps; ww++) {
+          const uint32_t c = wcnt[ww * kN + dg];
+          wcnt[ww * kN + dg] = at;
+          at += c;
+        }
+        goff[dg] = d.tile_hist[(size_t)t * kN + dg] + d.sort_base[(size_t)b * kN + dg] - lb;
+        lb += run[q];
+      }
     }
-    goff[dg] -= lb;
   }
   __syncthreads();
 #pragma unroll
   for (int i = 0; i < kTileItems; i++) {
     const int e = w * kWarpSpan + i * 32 + ln;
     if (e < valid) {
-      const int dg = (int)((key[i] >> shift) & (kRadix - 1));
+      const int dg = (int)((key[i] >> shift) & (kN - 1));
       const uint32_t r = (i & 1) ? rank2[i >> 1] >> 16 : rank2[i >> 1] & 0xffffu;
-      const uint32_t pos = wcnt[w * kRadix + dg] + r;
+      const uint32_t pos = wcnt[w * kN + dg] + r;
       sk[pos] = key[i];
       if (kVals) sv[pos] = val[i];
     }
@@ -262,7 +317,7 @@ __global__ void __launch_bounds__(256, kVals ? 2 : 3)
   uint32_t *VO = d.vals[cur ^ 1];
   for (int k = threadIdx.x; k < valid; k += blockDim.x) {
     const uint64_t kk = sk[k];
-    const int dg = (int)((kk >> shift) & (kRadix - 1));
+    const int dg = (int)((kk >> shift) & (kN - 1));
     const uint32_t g = goff[dg] + (uint32_t)k;
     KO[g] = kk;
     if (kVals) VO[g] = sv[k];
@@ -277,16 +332,18 @@ __global__ void k_radix_flip(SlabDev d) {
 // Stable sort of each block's elements by key bits [lo, hi), over `grid`
 // tiles (all tiles, or the listed ones).
 // gen: the first pass generates the packed first-sort items from the text.
-void radix_sort(const SlabDev &d, int lo, int hi, int has_vals, cudaStream_t st, int grid,
-                const int32_t *list, bool gen = false) {
-  const size_t smem = has_vals ? kScatterSmem : (size_t)kTile * 8 + (size_t)kSortWarps * kRadix * 4 +
-                                                    2 * kRadix * 4;
-  if (grid <= 0) return;
-  for (int shift = lo; shift < hi; shift += kRadixBits) {
+// RB: digit width (8; 9 or 10 for packed items of the doubling rounds where
+// that takes fewer passes).
+template <int RB>
+void radix_passes(const SlabDev &d, int lo, int hi, int has_vals, cudaStream_t st, int grid,
+                  const int32_t *list, bool gen) {
+  BZ_REQUIRE(RB == 8 || (!has_vals && !gen), kErrInternal, "wide digits are for packed rounds");
+  const size_t smem = has_vals ? scatter_smem_vals<RB>() : scatter_smem_keys<RB>();
+  for (int shift = lo; shift < hi; shift += RB) {
     const int g = gen && shift == lo;
-    k_radix_hist<<<grid, 256, 0, st>>>(d, shift, list, g);
+    k_radix_hist<RB><<<grid, 256, 0, st>>>(d, shift, list, g);
     BZ_LAUNCH_CHECK();
-    k_radix_scan<<<d.nblocks, 256, 0, st>>>(d, g);
+    k_radix_scan<RB><<<d.nblocks, 256, 0, st>>>(d, g);
     BZ_LAUNCH_CHECK();
     int timed = -1;
     if (d.kt_on && *d.kt_n < kMaxTimedLaunches) {
@@ -294,15 +351,33 @@ void radix_sort(const SlabDev &d, int lo, int hi, int has_vals, cudaStream_t st,
       d.kt_bpe[timed] = has_vals ? 24 : g ? 9 : 16;  // the generating pass reads text bytes
       BZ_CUDA(cudaEventRecord(d.kt_ev[2 * timed], st));
     }
-    if (has_vals)
-      k_radix_scatter<true><<<grid, 256, smem, st>>>(d, shift, timed, list, 0);
-    else
-      k_radix_scatter<false><<<grid, 256, smem, st>>>(d, shift, timed, list, g);
+    if constexpr (RB == 8) {
+      if (has_vals)
+        k_radix_scatter<true, 8><<<grid, 256, smem, st>>>(d, shift, timed, list, 0);
+      else
+        k_radix_scatter<false, 8><<<grid, 256, smem, st>>>(d, shift, timed, list, g);
+    } else {
+      k_radix_scatter<false, RB><<<grid, 256, smem, st>>>(d, shift, timed, list, 0);
+    }
     BZ_LAUNCH_CHECK();
     if (timed >= 0) BZ_CUDA(cudaEventRecord(d.kt_ev[2 * timed + 1], st));
     k_radix_flip<<<1, 1, 0, st>>>(d);
     BZ_LAUNCH_CHECK();
   }
+}
+
+void radix_sort(const SlabDev &d, int lo, int hi, int has_vals, cudaStream_t st, int grid,
+                const int32_t *list, bool gen = false) {
+  if (grid <= 0) return;
+  // the narrowest digit that takes the fewest passes
+  const int bits = hi - lo;
+  const int p8 = (bits + 7) / 8, p9 = (bits + 8) / 9, p10 = (bits + 9) / 10;
+  if (has_vals || gen || (p9 >= p8 && p10 >= p8))
+    radix_passes<8>(d, lo, hi, has_vals, st, grid, list, gen);
+  else if (p9 <= p10)
+    radix_passes<9>(d, lo, hi, has_vals, st, grid, list, gen);
+  else
+    radix_passes<10>(d, lo, hi, has_vals, st, grid, list, gen);
 }
 
 // ------------------------------------------------------------------- BWT
@@ -642,10 +717,18 @@ bool smem_configured = false;
 
 void stage_bwt(const SlabDev &d, int max_m, cudaStream_t st) {
   if (!smem_configured) {
-    BZ_CUDA(cudaFuncSetAttribute(k_radix_scatter<true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScatterSmem));
-    BZ_CUDA(cudaFuncSetAttribute(k_radix_scatter<false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScatterSmem));
+    BZ_CUDA(cudaFuncSetAttribute(k_radix_scatter<true, 8>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)scatter_smem_vals<8>()));
+    BZ_CUDA(cudaFuncSetAttribute(k_radix_scatter<false, 8>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)scatter_smem_keys<8>()));
+    BZ_CUDA(cudaFuncSetAttribute(k_radix_scatter<false, 9>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)scatter_smem_keys<9>()));
+    BZ_CUDA(cudaFuncSetAttribute(k_radix_scatter<false, 10>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)scatter_smem_keys<10>()));
     smem_configured = true;
   }
   k_bwt_init<<<(d.nblocks + 127) / 128, 128, 0, st>>>(d);

@@ -125,7 +125,7 @@ Workspace::Workspace(int mb, int64_t mr, int64_t me, int mt, int mrt, int mgt)
     dev.vg_list = (int32_t *)alloc(((int64_t)mgt + 1) * 4);
     dev.warp_last = (int32_t *)alloc(((int64_t)mt + 1) * (kTileThreads / 32) * 4);
     dev.warp_act = (int32_t *)alloc(((int64_t)mt + 1) * (kTileThreads / 32) * 4);
-    dev.tile_hist = (uint32_t *)alloc((int64_t)mt * 256 * 4);
+    dev.tile_hist = (uint32_t *)alloc((int64_t)mt * kMaxRadix * 4);
     dev.tile_last = (int32_t *)alloc((int64_t)mt * 256 * 4);
     dev.gt_bits = (uint32_t *)alloc(((int64_t)mgt + 1) * 4);
     const int64_t B = mb + 1;
@@ -160,7 +160,7 @@ Workspace::Workspace(int mb, int64_t mr, int64_t me, int mt, int mrt, int mgt)
     dev.pay_bits = (int64_t *)alloc(B * 8);
     dev.blk_start = (int64_t *)alloc(B * 8);
     dev.sort_ctl = (int32_t *)alloc(64);
-    dev.sort_base = (uint32_t *)alloc(B * 256 * 4);
+    dev.sort_base = (uint32_t *)alloc(B * kMaxRadix * 4);
     dev.stream = (uint64_t *)alloc(64);
     dev.kt_elems = (uint64_t *)alloc(8 * kMaxTimedLaunches);
     // plan arrays: 3 int64 per block + ints

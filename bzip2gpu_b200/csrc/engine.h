@@ -49,6 +49,7 @@ struct SlabPlan {
 };
 
 constexpr int kGroupTile = 128;  // 50-symbol groups per group tile
+constexpr int kMaxRadix = 1024;  // widest radix sort digit (10 bits)
 
 // Device pointers of one slab, passed to kernels by value.
 struct SlabDev {
@@ -68,8 +69,8 @@ struct SlabDev {
   uint32_t *out;
   // per-tile scratch
   int32_t *tile_a, *tile_b, *tile_c, *tile_d;  // [ntiles] or [n_raw_tiles]
-  uint32_t *tile_hist;                 // [ntiles * 256]
-  uint32_t *sort_base;                 // [nblocks * 256]: radix sort digit bases
+  uint32_t *tile_hist;                 // [ntiles * kMaxRadix]: radix sort tile digit counts
+  uint32_t *sort_base;                 // [nblocks * kMaxRadix]: radix sort digit bases
   int32_t *tile_last;                  // [ntiles * 256]
   uint32_t *gt_bits;                   // [n_group_tiles]
   uint32_t *grp_bits;                  // per group, at sel layout
