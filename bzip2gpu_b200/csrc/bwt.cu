@@ -102,8 +102,15 @@ __device__ __forceinline__ uint64_t text_item(const uint8_t *T, int m, int i) {
   return ((uint64_t)k << 32) | (uint32_t)i;
 }
 
+template <int RB>
+__device__ __forceinline__ void block_digit_scan(const SlabDev &d, int b, int force,
+                                                 uint32_t *scratch);
+
 // gen != 0: the generating first pass (items from the text, see text_item;
 // 8-bit digits).  RB: digit width, tile_hist holds 2^RB counts per tile.
+// The last tile of a block to finish its counts (a per-block counter, after
+// a fence that publishes the counts) runs the block's scan over its tiles'
+// counts, so the pass needs no scan launch of its own.
 template <int RB>
 __global__ void __launch_bounds__(256) k_radix_hist(SlabDev d, int shift, const int32_t *list,
                                                     int gen) {
@@ -133,6 +140,19 @@ __global__ void __launch_bounds__(256) k_radix_hist(SlabDev d, int shift, const 
   }
   __syncthreads();
   for (int i = threadIdx.x; i < kN; i += blockDim.x) d.tile_hist[(size_t)t * kN + i] = cnt[i];
+  __threadfence();
+  __syncthreads();
+  __shared__ int s_last;
+  __shared__ uint32_t scratch[40];
+  if (threadIdx.x == 0) {
+    const int nt = (d.sort_len[b] + kTile - 1) / kTile;
+    s_last = atomicAdd(&d.blk_count[b], 1) == nt - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  block_digit_scan<RB>(d, b, gen, scratch);
+  if (threadIdx.x == 0) d.blk_count[b] = 0;
 }
 
 // Per block: turn tile digit counts into each tile's count of the digit in
@@ -141,12 +161,10 @@ __global__ void __launch_bounds__(256) k_radix_hist(SlabDev d, int shift, const 
 // digit only, since it writes the items the later passes read.
 // Thread i handles the kD = 2^RB / 256 consecutive digits kD*i .. kD*i+kD-1.
 template <int RB>
-__global__ void __launch_bounds__(256) k_radix_scan(SlabDev d, int force) {
+__device__ __forceinline__ void block_digit_scan(const SlabDev &d, int b, int force,
+                                                 uint32_t *scratch) {
   constexpr int kN = 1 << RB, kD = kN / 256;
-  __shared__ uint32_t scratch[40];
-  const int b = blockIdx.x;
   const int len = d.sort_len[b];
-  if (len <= 0) return;
   const int nt = (len + kTile - 1) / kTile;
   const int t0 = (int)(d.off[b] / kTile);
   uint32_t *H = d.tile_hist + (size_t)t0 * kN + kD * threadIdx.x;
@@ -160,7 +178,7 @@ __global__ void __launch_bounds__(256) k_radix_scan(SlabDev d, int force) {
     for (int q = 0; q < kD; q++) {
       uint32_t h[kU];
 #pragma unroll
-      for (int j = 0; j < kU; j++) h[j] = k0 + j < nt ? H[(size_t)(k0 + j) * kN + q] : 0u;
+      for (int j = 0; j < kU; j++) h[j] = k0 + j < nt ? __ldcg(&H[(size_t)(k0 + j) * kN + q]) : 0u;
 #pragma unroll
       for (int j = 0; j < kU; j++) {
         if (k0 + j < nt) H[(size_t)(k0 + j) * kN + q] = run[q];
@@ -342,8 +360,6 @@ void radix_passes(const SlabDev &d, int lo, int hi, int has_vals, cudaStream_t s
   for (int shift = lo; shift < hi; shift += RB) {
     const int g = gen && shift == lo;
     k_radix_hist<RB><<<grid, 256, 0, st>>>(d, shift, list, g);
-    BZ_LAUNCH_CHECK();
-    k_radix_scan<RB><<<d.nblocks, 256, 0, st>>>(d, g);
     BZ_LAUNCH_CHECK();
     int timed = -1;
     if (d.kt_on && *d.kt_n < kMaxTimedLaunches) {

@@ -161,6 +161,8 @@ Workspace::Workspace(int mb, int64_t mr, int64_t me, int mt, int mrt, int mgt)
     dev.blk_start = (int64_t *)alloc(B * 8);
     dev.sort_ctl = (int32_t *)alloc(64);
     dev.sort_base = (uint32_t *)alloc(B * kMaxRadix * 4);
+    dev.blk_count = (int32_t *)alloc(B * 4);
+    BZ_CUDA(cudaMemset(dev.blk_count, 0, B * 4));
     dev.stream = (uint64_t *)alloc(64);
     dev.kt_elems = (uint64_t *)alloc(8 * kMaxTimedLaunches);
     // plan arrays: 3 int64 per block + ints

@@ -71,6 +71,7 @@ struct SlabDev {
   int32_t *tile_a, *tile_b, *tile_c, *tile_d;  // [ntiles] or [n_raw_tiles]
   uint32_t *tile_hist;                 // [ntiles * kMaxRadix]: radix sort tile digit counts
   uint32_t *sort_base;                 // [nblocks * kMaxRadix]: radix sort digit bases
+  int32_t *blk_count;                  // [nblocks]: radix sort tiles counted (reset by the last)
   int32_t *tile_last;                  // [ntiles * 256]
   uint32_t *gt_bits;                   // [n_group_tiles]
   uint32_t *grp_bits;                  // per group, at sel layout
