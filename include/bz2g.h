@@ -101,8 +101,8 @@ size_t bz2g_compress_batch_bound(int count, const size_t *sizes, const int *leve
 
 /* Engine shape used by the whole-stream calls on this thread's device:
  * blocks per slab and worker streams (default 384 and 4).  0 keeps the
- * current value.  Each worker's workspace takes about 55 MB of device memory
- * per 900,000-byte block it holds (21 GB at 384 blocks) and is allocated when
+ * current value.  Each worker's workspace takes about 56 MB of device memory
+ * per 900,000-byte block it holds (21.5 GB at 384 blocks) and is allocated when
  * a call first needs it: a call of k blocks takes room for min(k,
  * slab_blocks) blocks per worker, and a later, larger call grows it (at least
  * doubling, at most to slab_blocks); it is kept until the shape changes.
