@@ -408,6 +408,7 @@ __global__ void k_bwt_init(SlabDev d) {
   d.ngroups[b] = -1;
   d.act_len[b] = 0;
   d.active_sum[b] = 0;
+  d.blk_count[b] = 0;  // the histogram tile counter: each pass resets it, and so does this
   for (int k = 0; k < 8; k++) d.pstat[b * 8 + k] = 0;
   if (m == 1) d.sa[d.off[b]] = 0;
 }
