@@ -33,9 +33,9 @@ namespace {
 
 constexpr int kSortWarps = kTileThreads / 32;  // 8
 constexpr int kWarpSpan = kTile / kSortWarps;   // elements per warp in a tile (512)
-// Digits of the doubling rounds' sorts may be 9 or 10 bits wide (fewer
-// passes over the 2kb key bits); the tile and block digit tables (tile_hist,
-// sort_base) are sized for kMaxRadix digits.  Shared memory of the scatter: the tile's
+// Digits of the doubling rounds' sorts may be 9 bits wide (fewer passes over
+// the 2kb key bits); the tile and block digit tables (tile_hist, sort_base)
+// are sized for kMaxRadix digits.  Shared memory of the scatter: the tile's
 // keys (and values), per-warp digit counts, two digit tables.
 template <int RB>
 constexpr size_t scatter_smem_keys() {
@@ -350,8 +350,8 @@ __global__ void k_radix_flip(SlabDev d) {
 // Stable sort of each block's elements by key bits [lo, hi), over `grid`
 // tiles (all tiles, or the listed ones).
 // gen: the first pass generates the packed first-sort items from the text.
-// RB: digit width (8; 9 or 10 for packed items of the doubling rounds where
-// that takes fewer passes).
+// RB: digit width (8; 9 for packed items of the doubling rounds where that
+// takes fewer passes).
 template <int RB>
 void radix_passes(const SlabDev &d, int lo, int hi, int has_vals, cudaStream_t st, int grid,
                   const int32_t *list, bool gen) {
@@ -385,15 +385,14 @@ void radix_passes(const SlabDev &d, int lo, int hi, int has_vals, cudaStream_t s
 void radix_sort(const SlabDev &d, int lo, int hi, int has_vals, cudaStream_t st, int grid,
                 const int32_t *list, bool gen = false) {
   if (grid <= 0) return;
-  // the narrowest digit that takes the fewest passes
+  // 9-bit digits where they take fewer passes than 8-bit ones (10-bit
+  // digits also save a pass for 19- and 20-bit rank fields, but their
+  // 4x digit tables made the deep rounds of long blocks slower)
   const int bits = hi - lo;
-  const int p8 = (bits + 7) / 8, p9 = (bits + 8) / 9, p10 = (bits + 9) / 10;
-  if (has_vals || gen || (p9 >= p8 && p10 >= p8))
-    radix_passes<8>(d, lo, hi, has_vals, st, grid, list, gen);
-  else if (p9 <= p10)
+  if (!has_vals && !gen && (bits + 8) / 9 < (bits + 7) / 8)
     radix_passes<9>(d, lo, hi, has_vals, st, grid, list, gen);
   else
-    radix_passes<10>(d, lo, hi, has_vals, st, grid, list, gen);
+    radix_passes<8>(d, lo, hi, has_vals, st, grid, list, gen);
 }
 
 // ------------------------------------------------------------------- BWT
@@ -743,9 +742,6 @@ void stage_bwt(const SlabDev &d, int max_m, cudaStream_t st) {
     BZ_CUDA(cudaFuncSetAttribute(k_radix_scatter<false, 9>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)scatter_smem_keys<9>()));
-    BZ_CUDA(cudaFuncSetAttribute(k_radix_scatter<false, 10>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)scatter_smem_keys<10>()));
     smem_configured = true;
   }
   k_bwt_init<<<(d.nblocks + 127) / 128, 128, 0, st>>>(d);

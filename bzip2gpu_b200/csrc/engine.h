@@ -49,7 +49,7 @@ struct SlabPlan {
 };
 
 constexpr int kGroupTile = 128;  // 50-symbol groups per group tile
-constexpr int kMaxRadix = 1024;  // widest radix sort digit (10 bits)
+constexpr int kMaxRadix = 512;   // widest radix sort digit (9 bits)
 
 // Device pointers of one slab, passed to kernels by value.
 struct SlabDev {
